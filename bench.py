@@ -1,0 +1,313 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 dycore: cell-steps/s of the order-9 WENO SSPRK3
+dynamical core on the neutral boundary-layer workload (256x256x128, dx=10 m,
+tracers water_vapor + TKE), one JSON line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+* value: K SSPRK3 steps of the resident FP32 state, timed with CUDA events
+  on the dycore's stream between a barrier and a device synchronize on both
+  sides, max over ranks; the state (>= 0.9 GB) is larger than L2.
+* e2e: the reference-facing call (pu_dycore_time_step, dt_phys = 10 dycore
+  steps as the reference's drivers use, abl_neutral.cpp:25) with the coupler
+  arrays in pinned host memory: host->device copy, conversion, 10 SSPRK3
+  steps, conversion back and device->host copy inside every timed call.
+* roofline: the x/y flux kernel (the larger share of the step), its
+  algorithmic bytes per launch over its CUDA-event duration in the timed
+  region; traffic from the committed ncu capture (profiles/).
+* cpu_baseline: the reference's own dycore code (oracle/_ref, built from the
+  reference's headers with a single-rank shim) on all host cores, on a
+  bounded sample of the same workload.
+* Multi-GPU: the dycore is not domain-decomposed here; N ranks run N
+  independent replicas (ensemble members) with no collective in the data
+  path (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
+WORKLOAD = dict(nx=256, ny=256, nz=128, dx=10.0)
+DYN_CYCLE = 10
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        d["source"] = "measured"
+        return d
+    return dict(PEAKS_FALLBACK)
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_case(seed=0):
+    from porturb_b200 import cases
+    return cases.abl_neutral(nx=WORKLOAD["nx"], ny=WORKLOAD["ny"], nz=WORKLOAD["nz"], dx=WORKLOAD["dx"], seed=seed)
+
+
+def workload_name():
+    w = WORKLOAD
+    return "abl_neutral %dx%dx%d dx=%gm, water_vapor+TKE tracers, WENO order 9, SSPRK3" % (
+        w["nx"], w["ny"], w["nz"], w["dx"])
+
+
+def cpu_sample_case():
+    """The bounded CPU sample: the same boundary-layer configuration on a
+    64x64 column block of the full 128 levels (same spacing and profile)."""
+    from porturb_b200 import cases
+    return cases.abl_neutral(nx=64, ny=64, nz=WORKLOAD["nz"], dx=WORKLOAD["dx"], seed=0)
+
+
+def cpu_reference_rate(steps=1, warmup=1):
+    """Cell-steps/s of the reference's own dycore code on the host cores
+    (oracle/_ref); falls back to this project's REF restatement if the
+    reference library was not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    kind = "reference" if pyoracle.have_ref() else "ref"
+    case = cpu_sample_case()
+    d = pyoracle.Dycore(case, kind)
+    d.init_case()
+    d.load_coupler(list(case.coupler_arrays(perturbed=True)))
+    dt = d.compute_time_step()
+    for _ in range(warmup):
+        d.advance(dt, 1)
+    t0 = time.perf_counter()
+    d.advance(dt, steps)
+    el = time.perf_counter() - t0
+    import ctypes
+    lib = pyoracle._lib(pyoracle.ORACLE_SO, "orc_")
+    threads = int(lib.orc_num_threads())
+    return {"value": case.ncells * steps / el, "unit": "cell-steps/s", "cores": threads,
+            "kind": "reference" if kind == "reference" else "port",
+            "sample": "%d SSPRK3 step(s) of abl_neutral on a %dx%dx%d block (same dx and profile), "
+                      "after %d warm-up step(s), %.1f s" % (steps, case.nx, case.ny, case.nz, warmup, el)}
+
+
+def setup_dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    base = cpu_reference_rate(steps=max(1, args.steps // 10), warmup=1)
+    line = {"impl": "reference", "metric": "cell-steps/s", "value": base["value"], "unit": "cell-steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64-state/f32-stencil", "data": "synthetic",
+            "config": {"workload": workload_name(), "sample": base["sample"]},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-calls", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = setup_dist()
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from porturb_b200 import Dycore, build
+    build.build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    case = build_case(seed=rank)
+    stream = torch.cuda.Stream(device=local)
+    g = Dycore.from_case(case, precision="f32", device=local, stream=stream.cuda_stream)
+    rd, u, v, w, T, trc = [np.ascontiguousarray(a) for a in case.coupler_arrays(perturbed=False)]
+    g.init(rd, u, v, w, T, list(trc), None)
+    rd, u, v, w, T, trc = [np.ascontiguousarray(a) for a in case.coupler_arrays(perturbed=True)]
+    g.load_state(rd, u, v, w, T, list(trc))
+    dt = g.compute_time_step()
+    N = case.ncells
+    S = 5 + len(case.tracers)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # Warm-up, then the timed region.
+    for _ in range(args.warmup):
+        g.advance(dt, 1)
+    g.synchronize()
+    clocks = ClockSampler(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    g.profile(True)
+    launches0 = g.kernel_launches()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        g.advance(dt, 1)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = g.kernel_launches() - launches0
+    prof = g.profile_read()
+    g.profile(False)
+    clk = clocks.stop()
+    barrier()
+    g.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = world * N * args.steps / (ms / 1e3)
+
+    # e2e through the C-ABI with pinned host coupler arrays.
+    shp = (case.nz, case.ny, case.nx)
+    pinned = [torch.empty(shp, dtype=torch.float64).pin_memory() for _ in range(5)]
+    ptrc = [torch.empty(shp, dtype=torch.float64).pin_memory() for _ in range(len(case.tracers))]
+    g.store_state(*pinned, ptrc)
+    dt_phys = DYN_CYCLE * dt
+    g.time_step(*pinned, ptrc, dt_phys)   # warm-up call
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ncyc = 0
+    for _ in range(args.e2e_calls):
+        ncyc += g.time_step(*pinned, ptrc, dt_phys)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * N * ncyc / e2e_s
+    bytes_io = (5 + len(case.tracers)) * N * 8
+
+    if rank == 0:
+        peaks = measured_peaks()
+        hbm_peak = peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+        xy_ms, xy_n = prof["xy"]
+        z_ms, z_n = prof["z"]
+        # Algorithmic bytes: 32*S B per cell-step (8 passes over the S-field
+        # FP32 state).  The x/y kernel owns 1 of the 8 passes per stage
+        # (reading the stage input), i.e. 4*S B per cell per launch.
+        alg_xy = 4.0 * S * N
+        xy_avg_s = xy_ms / 1e3 / max(xy_n, 1)
+        achieved = alg_xy / xy_avg_s / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                traffic = json.load(f).get("k_xy_bytes_per_launch")
+        cpu = None
+        if not args.no_cpu_baseline:
+            try:
+                cpu = cpu_reference_rate(steps=1, warmup=1)
+            except Exception as e:  # the baseline is a report, not the product
+                cpu = {"error": str(e)}
+        line = {
+            "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": workload_name(), "cells": N, "prognostics": S, "weno": "plain",
+                       "l2": "state and stage buffers (%.2f GB) exceed L2" % (4 * S * N * 4 / 1e9),
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "hbm_gbs_step": 32.0 * S * N * args.steps / (ms / 1e3) / 1e9,
+            "roofline": {"kernel": "k_xy (x/y WENO + Riemann + divergence)", "bound": "hbm",
+                         "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                         "traffic": traffic, "peak_source": peaks.get("source"),
+                         "note": "FP32-pipe bound; see profiles/ for FP32 pipe utilisation"},
+            "kernel_ms": {"k_xy": xy_ms / max(xy_n, 1), "k_z": z_ms / max(z_n, 1),
+                          "share_xy": xy_ms / max(xy_ms + z_ms, 1e-12)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": bytes_io,
+                    "d2h_bytes_per_step": bytes_io, "calls": args.e2e_calls, "dycore_steps_per_call": ncyc // max(1, args.e2e_calls)},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,189 @@
+/* pu_dycore: C-ABI of the B200 dynamical core.
+ *
+ * A drop-in for the reference's compressible, hydrostatically stratified
+ * WENO finite-volume dycore, modules::Dynamics_Euler_Stratified_WenoFV
+ * (model/modules/dynamics_rk.h:25-1355), at WENO order 9 on one GPU.
+ *
+ * The reference module is stateless and keeps everything in the coupler's
+ * DataManager; its three entry points are
+ *     void init(core::Coupler &)                      dynamics_rk.h:917-1246
+ *     void time_step(core::Coupler &, real dt_phys)   dynamics_rk.h:103-137
+ *     real compute_time_step(core::Coupler const &)   dynamics_rk.h:57-64
+ * Here a handle (pu_dycore) holds the grid, options and device-resident
+ * state; the coupler's arrays are passed in as a pu_state_view (host or
+ * device pointers).  A host-side C++ wrapper with the reference's exact
+ * module API is in porturb_b200/cpp/dynamics_rk.h.
+ *
+ * Conventions:
+ *   - every function returns PU_OK (0) or a PU_ERR_* code; pu_last_error()
+ *     gives a message (the reference aborts instead: Options.h:122-148,
+ *     dynamics_rk.h:799, ParallelComm.h:315-323);
+ *   - 3-D arrays are C-order (nz, ny, nx) doubles, the coupler's layout
+ *     (dynamics_rk.h:1269-1277, 1322-1330);
+ *   - one CUDA stream per handle (pu_config.stream, NULL = the legacy
+ *     default stream); calls are asynchronous on that stream unless stated;
+ *   - no internal host threads; a handle is not thread-safe (the reference's
+ *     Coupler is not either).
+ */
+#ifndef PU_DYCORE_H
+#define PU_DYCORE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PU_MAX_TRACERS 4   /* water_vapor + up to three more advected tracers */
+#define PU_ORD 9           /* WENO order; halo width PU_HS = (PU_ORD-1)/2 */
+#define PU_HS 4
+
+typedef enum {
+  PU_OK = 0,
+  PU_ERR_INVALID = 1,      /* bad argument or option (the reference aborts) */
+  PU_ERR_CUDA = 2,         /* a CUDA call failed */
+  PU_ERR_NONFINITE = 3,    /* the state became NaN/Inf during a step */
+  PU_ERR_STATE = 4,        /* call out of order (e.g. time_step before init) */
+  PU_ERR_NOMEM = 5,        /* device allocation failed */
+  PU_ERR_UNSUPPORTED = 6   /* configuration outside what this build supports */
+} pu_status;
+
+typedef enum { PU_BC_PERIODIC = 0, PU_BC_PRECURSOR = 1, PU_BC_WALL = 2 } pu_bc;
+typedef enum { PU_F32 = 0, PU_F64 = 1 } pu_precision;
+typedef enum { PU_WENO_PLAIN = 0, PU_WENO_LEARNED = 1 } pu_weno_mode;
+typedef enum { PU_MEM_HOST = 0, PU_MEM_DEVICE = 1 } pu_mem;
+
+/* Grid, tracer registry and the coupler options the dycore reads
+ * (dynamics_rk.h:508-531, 747, 930-933, 1262-1266, 1315-1319; defaults from
+ * sc_init.h:31-51 and abl_neutral.cpp:36-47). */
+typedef struct pu_config {
+  int nx, ny, nz;                          /* coupler.get_nx/ny/nz */
+  double dx, dy, dz;                       /* coupler.get_dx/dy/dz */
+  int ntracers;                            /* coupler.get_num_tracers */
+  int tracer_positive[PU_MAX_TRACERS];     /* add_tracer(...,positive,...) */
+  int tracer_adds_mass[PU_MAX_TRACERS];    /* add_tracer(...,adds_mass,...) */
+  int idWV;                                /* option "idWV": index of water_vapor */
+  double R_d, R_v, cp_d, gamma_d, C0, grav;/* options of the same names */
+  double cfl;                              /* option "cfl" (reference default 0.60) */
+  double immersed_power;                   /* option "immersed_power" (default 5) */
+  double latitude;                         /* option "latitude" in degrees (default 0) */
+  int bc_x, bc_y, bc_z;                    /* options "bc_x/bc_y/bc_z" as pu_bc */
+  int enable_gravity;                      /* option "enable_gravity" (default true) */
+  int weno_all;                            /* option "weno_all" (default true) */
+  int precision;                           /* pu_precision: stencil arithmetic type */
+  int weno_mode;                           /* pu_weno_mode */
+  int device;                              /* CUDA device ordinal */
+  void *stream;                            /* cudaStream_t, or NULL */
+  int z_chunk;                             /* levels per z-march work item; 0 = auto */
+} pu_config;
+
+/* The coupler-side state: density_dry, uvel, vvel, wvel, temp and the tracer
+ * arrays in the order of the tracer registry. */
+typedef struct pu_state_view {
+  double *rho_d, *uvel, *vvel, *wvel, *temp;
+  double *tracers[PU_MAX_TRACERS];
+  int mem; /* pu_mem: where the pointers live */
+} pu_state_view;
+
+/* Global FP64 integrals of the dycore state, accumulated with compensated
+ * (Neumaier) sums on the GPU.  Volumes in m^3, energies in J. */
+typedef struct pu_diag {
+  double mass;            /* sum rho dV */
+  double rho_theta;       /* sum rho*theta dV */
+  double kinetic;         /* sum 0.5 |rho u|^2 / rho dV */
+  double internal;        /* sum p/(gamma-1) dV */
+  double potential;       /* sum rho g z dV, z at cell centres */
+  double total_energy;    /* kinetic + internal + potential */
+  double tracer_mass[PU_MAX_TRACERS]; /* sum rho_q dV */
+} pu_diag;
+
+typedef struct pu_dycore pu_dycore;
+
+/* Version of this library (major*10000 + minor*100 + patch). */
+int pu_version(void);
+
+/* Message of the last failed call on this host thread. */
+const char *pu_last_error(void);
+
+/* Creates a handle and allocates its device buffers.  Replaces the
+ * construction of Dynamics_Euler_Stratified_WenoFV plus the option reads of
+ * its members (dynamics_rk.h:25-39, 508-531). */
+int pu_dycore_create(const pu_config *cfg, pu_dycore **out);
+
+/* Frees the handle and its device buffers. */
+int pu_dycore_destroy(pu_dycore *h);
+
+/* init(coupler), dynamics_rk.h:917-1246: converts the coupler state, takes
+ * the horizontal-mean hydrostatic profiles (FP64 on the GPU), extends them
+ * isentropically into the z halos, computes the edge profiles, and builds
+ * the immersed-boundary halos, flags (any_immersed within 10 cells) and
+ * relaxation time scales from immersed_proportion ((nz,ny,nx) doubles in
+ * `mem`; NULL = no immersed cells).  Synchronous. */
+int pu_dycore_init(pu_dycore *h, const pu_state_view *coupler, const double *immersed_proportion, int mem);
+
+/* compute_time_step(coupler), dynamics_rk.h:57-64: cfl*min(dx,dy,dz)/450. */
+int pu_dycore_compute_time_step(const pu_dycore *h, double *dt);
+
+/* time_step(coupler, dt_phys), dynamics_rk.h:103-137: converts the coupler
+ * state in, runs ncycles = ceil(dt_phys/dt_dyn) SSPRK3 steps of
+ * dt_phys/ncycles, converts back into the same arrays.  Synchronous; returns
+ * PU_ERR_NONFINITE if the state became non-finite.  ncycles may be NULL. */
+int pu_dycore_time_step(pu_dycore *h, pu_state_view *coupler, double dt_phys, int *ncycles);
+
+/* convert_coupler_to_dynamics (dynamics_rk.h:1304-1352) into the resident
+ * state, and convert_dynamics_to_coupler (dynamics_rk.h:1251-1299) out of it.
+ * store_state is synchronous and reports PU_ERR_NONFINITE like time_step. */
+int pu_dycore_load_state(pu_dycore *h, const pu_state_view *coupler);
+int pu_dycore_store_state(pu_dycore *h, pu_state_view *coupler);
+
+/* nsteps calls of time_step_rk_3_3 (dynamics_rk.h:279-367) with step dt_dyn
+ * on the resident state.  Asynchronous. */
+int pu_dycore_advance(pu_dycore *h, double dt_dyn, int nsteps);
+
+/* Conserved variables of the resident state (rho, rho*u, rho*v, rho*w,
+ * rho*theta as (5,nz,ny,nx) and tracers as (ntr,nz,ny,nx), absolute values,
+ * the reference's state/tracers arrays without halos).  Synchronous. */
+int pu_dycore_get_conserved(pu_dycore *h, double *state, double *tracers, int mem);
+int pu_dycore_set_conserved(pu_dycore *h, const double *state, const double *tracers, int mem);
+
+/* The hydrostatic profiles hy_{dens,theta,pressure}_cells ((nz+2*PU_HS)
+ * values each) and hy_{dens,theta,pressure}_edges (nz+1 each), as the values
+ * the stencil arithmetic uses.  Any pointer may be NULL. */
+int pu_dycore_get_hydrostasis(pu_dycore *h, double *dens_cells, double *theta_cells, double *pressure_cells,
+                              double *dens_edges, double *theta_edges, double *pressure_edges);
+
+/* Overwrites the cell profiles and recomputes the edge profiles: the
+ * dycore's restart hook (dynamics_rk.h:1235-1242).  The resident state is
+ * kept in absolute terms across the change. */
+int pu_dycore_set_hydrostasis(pu_dycore *h, const double *dens_cells, const double *theta_cells,
+                              const double *pressure_cells);
+
+/* FP64 compensated global integrals of the resident state.  Synchronous. */
+int pu_dycore_diagnostics(pu_dycore *h, pu_diag *out);
+
+/* Waits for all work of the handle; returns PU_ERR_NONFINITE if a step
+ * produced a non-finite value since the last check. */
+int pu_dycore_synchronize(pu_dycore *h);
+
+/* Number of kernels this handle has launched since creation (for launch
+ * accounting in benchmarks). */
+long long pu_dycore_kernel_launches(const pu_dycore *h);
+
+/* Per-kernel timing with CUDA events recorded on the handle's stream around
+ * every stencil-kernel launch while enabled (no counterpart in the reference,
+ * whose timers are YAKL's, dynamics_rk.h:104-106).  Kinds: 0 = x/y flux
+ * kernel, 1 = z flux + stage kernel, 2 = everything else.  Enabling resets
+ * the totals; pu_dycore_profile_read synchronizes. */
+#define PU_PROFILE_KINDS 3
+typedef struct pu_profile {
+  double ms[PU_PROFILE_KINDS];
+  long long launches[PU_PROFILE_KINDS];
+} pu_profile;
+int pu_dycore_profile(pu_dycore *h, int enable);
+int pu_dycore_profile_read(pu_dycore *h, pu_profile *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PU_DYCORE_H */

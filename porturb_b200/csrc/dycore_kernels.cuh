@@ -1,0 +1,809 @@
+// Kernels of the B200 dycore (order-9 WENO finite volume, SSPRK3).
+//
+// Storage: the resident state is structure-of-arrays, one (nz,ny,nx) array
+// per prognostic with no halos, in the stencil type R (float or double):
+//   q0 = rho - rho_h(k)             (density perturbation)
+//   q1..q3 = rho*u, rho*v, rho*w
+//   q4 = rho*theta - rho_h*theta_h(k)
+//   q5.. = tracer densities rho*q (the reference's tracers array)
+// rho_h, theta_h are the hydrostatic cell profiles (hy_dens_cells,
+// hy_theta_cells, dynamics_rk.h:961-1008).  Storing perturbations keeps FP32
+// state at the precision of the fluctuations rather than of the background.
+// Halos are never stored: periodic wraps, precursor clamps and wall values are
+// applied while tiles are loaded.
+//
+// Per SSPRK3 stage two kernels run:
+//   k_xy : one (x,y) tile of one level: primitive perturbation fields of the
+//          tile plus 5-cell halos into shared memory, WENO edges in x and y
+//          (dynamics_rk.h:572-607), upwind Riemann fluxes (:640-684) and their
+//          x/y divergence, written to the tendency buffer txy.
+//   k_z  : one column per thread marching up a chunk of levels with a 9-plane
+//          ring of primitive fields in shared memory: WENO edges in z
+//          (:608-625), wall/periodic face states (:891-908), Riemann fluxes
+//          (:685-706), the z divergence added to txy, gravity and Coriolis
+//          (:710-722), the SSPRK3 stage combination (:308-360), positivity
+//          clip and immersed relaxation (:429-469).
+#pragma once
+
+#include <cstdint>
+
+#include "weno9.cuh"
+
+namespace pu {
+
+constexpr int HS = 4;
+constexpr int BC_PERIODIC = 0, BC_PRECURSOR = 1, BC_WALL = 2;
+constexpr unsigned FLAG_IMM = 1u, FLAG_ANY10 = 2u;
+constexpr int iR = 0, iU = 1, iV = 2, iW = 3, iT = 4, iP = 5;
+
+template <class R>
+struct Grid {
+  int nx, ny, nz;
+  size_t N, NP;                 // nx*ny*nz and nx*ny
+  R rdx, rdy, rdz;
+  int bc_x, bc_y, bc_z;
+  int sim2d, weno_all, enable_gravity;
+  R grav, fcor, gamma;
+  unsigned tracer_positive;     // bit t: tracer t is positive definite
+  // Level tables.  Cell tables have nz+2*HS entries (index k+HS); edge tables nz+1.
+  const R *rho_h, *theta_h;     // hy_dens_cells, hy_theta_cells
+  const R *rt_inv;              // 1 / (rho_h*theta_h)
+  const R *p0_h;                // C0*(rho_h*theta_h)^gamma
+  const R *dp_h;                // p0_h - hy_pressure_cells
+  const R *rho_e, *theta_e;     // hy_dens_edges, hy_theta_edges
+  const R *rt_target;           // immersed relaxation target of q4 (index k)
+  const uint8_t *flags;         // FLAG_IMM | FLAG_ANY10 per cell, or null
+  const R *imm_mult;            // immersed_proportion^power / tau per cell, or null
+  int *err;                     // bit 0: a non-finite value was written
+};
+
+__device__ __forceinline__ int wrapi(int i, int n) {
+  i %= n;
+  return i < 0 ? i + n : i;
+}
+__device__ __forceinline__ int clampi(int i, int n) { return i < 0 ? 0 : (i >= n ? n - 1 : i); }
+
+__device__ __forceinline__ float pu_log1p(float x) { return log1pf(x); }
+__device__ __forceinline__ double pu_log1p(double x) { return log1p(x); }
+__device__ __forceinline__ float pu_expm1(float x) { return expm1f(x); }
+__device__ __forceinline__ double pu_expm1(double x) { return expm1(x); }
+
+// Primitive perturbation fields of one cell (dynamics_rk.h:550-558):
+// rho', u, v, w, theta', p', tracer mixing ratios.  theta' and p' are formed
+// from the perturbation storage without cancellation:
+//   theta' = (q4 - theta_h q0)/rho,   p' = P0_h*expm1(gamma*log1p(q4/(rho theta)_h)) + (P0_h - p_h).
+template <class R, int NTR>
+__device__ __forceinline__ void prims(const Grid<R> &G, const R *__restrict__ s, size_t idx, int k, R (&w)[6 + NTR]) {
+  const size_t N = G.N;
+  const int kh = k + HS;
+  R q0 = __ldg(s + idx), q1 = __ldg(s + N + idx), q2 = __ldg(s + 2 * N + idx), q3 = __ldg(s + 3 * N + idx),
+    q4 = __ldg(s + 4 * N + idx);
+  R rho = __ldg(G.rho_h + kh) + q0;
+  R rr = R(1) / rho;
+  w[0] = q0;
+  w[1] = q1 * rr;
+  w[2] = q2 * rr;
+  w[3] = q3 * rr;
+  w[4] = (q4 - __ldg(G.theta_h + kh) * q0) * rr;
+  w[5] = fma(__ldg(G.p0_h + kh), pu_expm1(G.gamma * pu_log1p(q4 * __ldg(G.rt_inv + kh))), __ldg(G.dp_h + kh));
+#pragma unroll
+  for (int t = 0; t < NTR; t++) w[6 + t] = __ldg(s + (5 + t) * N + idx) * rr;
+}
+
+// Upwind Riemann flux across one face (dynamics_rk.h:640-706): acoustic
+// upwinding of mass flux and pressure with a constant sound speed of 350 m/s,
+// advective upwinding of everything else.  L and Rt are the edge states of
+// the left and right cells (perturbation fields); hr, ht the hydrostatic
+// density and potential temperature at the face; idN the normal velocity.
+template <class R, int NTR>
+__device__ __forceinline__ void riemann(const R (&L)[6 + NTR], const R (&Rt)[6 + NTR], R hr, R ht, int idN,
+                                        R (&flux)[5 + NTR]) {
+  const R cs = R(350.), r_cs = R(1.) / R(350.);
+  R rL = L[iR] + hr, rR = Rt[iR] + hr;
+  R ruL = L[idN] * rL, ruR = Rt[idN] * rR;
+  R pL = L[iP], pR = Rt[iP];
+  R p_upw = R(0.5) * (pL + pR - cs * (ruR - ruL));
+  R ru_upw = R(0.5) * (ruL + ruR - (pR - pL) * r_cs);
+  const bool up = ru_upw > R(0);
+  flux[iR] = ru_upw;
+  flux[iU] = ru_upw * (up ? L[iU] : Rt[iU]);
+  flux[iV] = ru_upw * (up ? L[iV] : Rt[iV]);
+  flux[iW] = ru_upw * (up ? L[iW] : Rt[iW]);
+  flux[iT] = ru_upw * ((up ? L[iT] : Rt[iT]) + ht);
+  flux[idN] += p_upw;
+#pragma unroll
+  for (int t = 0; t < NTR; t++) flux[5 + t] = ru_upw * (up ? L[6 + t] : Rt[6 + t]);
+}
+
+template <class R, int NTR, int TX, int TY, bool IMM>
+struct XYShape {
+  static constexpr int F = 6 + NTR, S = 5 + NTR, NT = TX * TY;
+  static constexpr int HX = TX + 10, HY = TY + 10;       // tile plus 5-cell halos
+  static constexpr int EXN = TY * (TX + 2), EYN = (TY + 2) * TX;
+  static constexpr int EN = EXN > EYN ? EXN : EYN;
+  static constexpr int FXN = TY * (TX + 1), FYN = (TY + 1) * TX;
+  static constexpr int FN = FXN > FYN ? FXN : FYN;
+  static constexpr size_t bytes = sizeof(R) * (size_t(F) * HY * HX + 2 * size_t(F) * EN + size_t(S) * FN) +
+                                  (IMM ? size_t(HY) * HX : 0);
+};
+
+// x/y fluxes and their divergence for one (x,y) tile of one level.
+template <class R, int NTR, int TX, int TY, bool IMM>
+__global__ void __launch_bounds__(TX *TY) k_xy(const Grid<R> G, const R *__restrict__ sin, R *__restrict__ txy) {
+  using Sh = XYShape<R, NTR, TX, TY, IMM>;
+  constexpr int F = Sh::F, S = Sh::S, NT = Sh::NT, HX = Sh::HX, HY = Sh::HY, EN = Sh::EN, FN = Sh::FN;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *H = reinterpret_cast<R *>(smem_raw);
+  R *EL = H + F * HY * HX;
+  R *ER = EL + F * EN;
+  R *FL = ER + F * EN;
+  uint8_t *M = reinterpret_cast<uint8_t *>(FL + S * FN);
+
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k = blockIdx.z;
+  const int nx = G.nx, ny = G.ny;
+  const size_t plane = size_t(k) * G.NP;
+  const bool sim2d = G.sim2d != 0;
+
+  // 1. Primitive fields of the tile, its x halo rows and its y halo columns.
+  constexpr int NA = TY * HX, NB = 10 * TX;
+  for (int it = tid; it < NA + (sim2d ? 0 : NB); it += NT) {
+    int r, c;
+    if (it < NA) {
+      r = 5 + it / HX;
+      c = it % HX;
+    } else {
+      int b = it - NA, rr = b / TX;
+      c = 5 + b % TX;
+      r = rr < 5 ? rr : rr + TY;
+    }
+    const int gi = i0 - 5 + c, gj = j0 - 5 + r;
+    const int vi = G.bc_x == BC_PRECURSOR ? clampi(gi, nx) : wrapi(gi, nx);
+    const int vj = G.bc_y == BC_PRECURSOR ? clampi(gj, ny) : wrapi(gj, ny);
+    R w[F];
+    prims<R, NTR>(G, sin, plane + size_t(vj) * nx + vi, k, w);
+#pragma unroll
+    for (int f = 0; f < F; f++) H[(f * HY + r) * HX + c] = w[f];
+    if (IMM) M[r * HX + c] = __ldg(G.flags + plane + size_t(wrapi(gj, ny)) * nx + wrapi(gi, nx));
+  }
+  __syncthreads();
+
+  // 2. x edges of cells -1..TX of every tile row.
+  for (int it = tid; it < F * Sh::EXN; it += NT) {
+    const int f = it / Sh::EXN, rem = it % Sh::EXN, r = rem / (TX + 2), c = rem % (TX + 2);
+    const R *row = H + (f * HY + 5 + r) * HX + c;
+    R s[9];
+#pragma unroll
+    for (int m = 0; m < 9; m++) s[m] = row[m];
+    R qL, qR;
+    bool any10 = false;
+    unsigned imm = 0;
+    if (IMM) {
+      const uint8_t *mr = M + (5 + r) * HX + c;
+#pragma unroll
+      for (int m = 0; m < 9; m++) imm |= (unsigned(mr[m]) & FLAG_IMM) << m;
+      any10 = (mr[4] & FLAG_ANY10) != 0;
+      if (f == iV || f == iW || f == iP) der0_modify(s, imm);
+    }
+    if (!any10 && !G.weno_all) linear9_edges(s, qL, qR);
+    else weno9_edges(s, qL, qR, !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
+    EL[f * EN + rem] = qL;
+    ER[f * EN + rem] = qR;
+  }
+  __syncthreads();
+
+  // 3. Riemann fluxes on x faces 0..TX (face fi between cells fi-1 and fi).
+  const R hr = __ldg(G.rho_h + k + HS), ht = __ldg(G.theta_h + k + HS);
+  for (int it = tid; it < Sh::FXN; it += NT) {
+    const int r = it / (TX + 1), fi = it % (TX + 1);
+    const int cl = r * (TX + 2) + fi, cr = cl + 1;
+    R L[F], Rt[F];
+#pragma unroll
+    for (int f = 0; f < F; f++) {
+      L[f] = ER[f * EN + cl];
+      Rt[f] = EL[f * EN + cr];
+    }
+    if (G.bc_x == BC_PRECURSOR) {  // edge_exchange precursor mirror (dynamics_rk.h:864-875)
+      const int gf = i0 + fi;
+#pragma unroll
+      for (int f = 0; f < F; f++) {
+        if (gf == 0) L[f] = Rt[f];
+        if (gf == nx) Rt[f] = L[f];
+      }
+    }
+    R fl[S];
+    riemann<R, NTR>(L, Rt, hr, ht, iU, fl);
+#pragma unroll
+    for (int s = 0; s < S; s++) FL[s * FN + it] = fl[s];
+  }
+  __syncthreads();
+
+  // 4. x divergence of this thread's cell.
+  const int r = tid / TX, c = tid % TX;
+  R tend[S];
+#pragma unroll
+  for (int s = 0; s < S; s++) tend[s] = -(FL[s * FN + r * (TX + 1) + c + 1] - FL[s * FN + r * (TX + 1) + c]) * G.rdx;
+
+  if (!sim2d) {
+    // 5. y edges of cells -1..TY of every tile column.
+    for (int it = tid; it < F * Sh::EYN; it += NT) {
+      const int f = it / Sh::EYN, rem = it % Sh::EYN, rr = rem / TX, cc = rem % TX;
+      const R *col = H + (f * HY + rr) * HX + 5 + cc;
+      R s[9];
+#pragma unroll
+      for (int m = 0; m < 9; m++) s[m] = col[m * HX];
+      R qL, qR;
+      bool any10 = false;
+      unsigned imm = 0;
+      if (IMM) {
+        const uint8_t *mc = M + rr * HX + 5 + cc;
+#pragma unroll
+        for (int m = 0; m < 9; m++) imm |= (unsigned(mc[m * HX]) & FLAG_IMM) << m;
+        any10 = (mc[4 * HX] & FLAG_ANY10) != 0;
+        if (f == iU || f == iW || f == iP) der0_modify(s, imm);
+      }
+      if (!any10 && !G.weno_all) linear9_edges(s, qL, qR);
+      else weno9_edges(s, qL, qR, !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
+      EL[f * EN + rem] = qL;
+      ER[f * EN + rem] = qR;
+    }
+    __syncthreads();
+    // 6. Riemann fluxes on y faces 0..TY.
+    for (int it = tid; it < Sh::FYN; it += NT) {
+      const int fj = it / TX, cc = it % TX;
+      const int cl = fj * TX + cc, cr = cl + TX;
+      R L[F], Rt[F];
+#pragma unroll
+      for (int f = 0; f < F; f++) {
+        L[f] = ER[f * EN + cl];
+        Rt[f] = EL[f * EN + cr];
+      }
+      if (G.bc_y == BC_PRECURSOR) {
+        const int gf = j0 + fj;
+#pragma unroll
+        for (int f = 0; f < F; f++) {
+          if (gf == 0) L[f] = Rt[f];
+          if (gf == ny) Rt[f] = L[f];
+        }
+      }
+      R fl[S];
+      riemann<R, NTR>(L, Rt, hr, ht, iV, fl);
+#pragma unroll
+      for (int s = 0; s < S; s++) FL[s * FN + it] = fl[s];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < S; s++) tend[s] -= (FL[s * FN + (r + 1) * TX + c] - FL[s * FN + r * TX + c]) * G.rdy;
+  }
+
+  const int gi = i0 + c, gj = j0 + r;
+  if (gi < nx && gj < ny) {
+    const size_t idx = plane + size_t(gj) * nx + gi;
+#pragma unroll
+    for (int s = 0; s < S; s++) txy[s * G.N + idx] = tend[s];
+  }
+}
+
+// Immersed relaxation toward the hydrostatic state and positivity of
+// positive-definite tracers (enforce_immersed_boundaries, dynamics_rk.h:429-469)
+// on one cell's perturbation state.
+template <class R, int NTR, bool IMM>
+__device__ __forceinline__ void enforce_cell(const Grid<R> &G, R (&q)[5 + NTR], size_t idx, int k) {
+  if (IMM) {
+    const R mult = __ldg(G.imm_mult + idx);
+    q[0] = q[0] + (R(0) - q[0]) * mult;
+    q[1] = q[1] + (R(0) - q[1]) * mult;
+    q[2] = q[2] + (R(0) - q[2]) * mult;
+    q[3] = q[3] + (R(0) - q[3]) * mult;
+    q[4] = q[4] + (__ldg(G.rt_target + k) - q[4]) * mult;
+#pragma unroll
+    for (int t = 0; t < NTR; t++) q[5 + t] = q[5 + t] + (R(0) - q[5 + t]) * mult;
+  }
+#pragma unroll
+  for (int t = 0; t < NTR; t++)
+    if ((G.tracer_positive >> t) & 1u) q[5 + t] = fmax(R(0), q[5 + t]);
+}
+
+template <class R, int NTR, int TX, int TY>
+struct ZShape {
+  static constexpr int F = 6 + NTR, NT = TX * TY;
+  static constexpr size_t bytes = sizeof(R) * 9 * size_t(F) * NT;
+};
+
+// z fluxes, their divergence, sources and the SSPRK3 stage combination:
+//   out = a_n*sn + a_in*sin + a_dt*(txy - dFz/dz + sources)   (sn may be null)
+// followed by n_enforce applications of the immersed/positivity enforcement.
+template <class R, int NTR, int TX, int TY, bool IMM>
+__global__ void __launch_bounds__(TX *TY) k_z(const Grid<R> G, const R *__restrict__ sin, const R *__restrict__ sn,
+                                              R *__restrict__ sout, const R *__restrict__ txy, R a_n, R a_in, R a_dt,
+                                              int n_enforce, int kchunk) {
+  constexpr int F = 6 + NTR, S = 5 + NTR, NT = TX * TY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *ring = reinterpret_cast<R *>(smem_raw);   // [9][F][NT], thread-private columns
+  const int tid = threadIdx.x;
+  const int i = blockIdx.x * TX + tid % TX, j = blockIdx.y * TY + tid / TX;
+  if (i >= G.nx || j >= G.ny) return;          // no block-wide synchronisation below
+  const int nz = G.nz;
+  const int k0 = blockIdx.z * kchunk, k1 = min(nz, k0 + kchunk);
+  const bool wall = G.bc_z == BC_WALL;
+  const size_t col = size_t(j) * G.nx + i, NP = G.NP;
+
+  auto slot_ptr = [&](int p) { return ring + ((p % 9 + 9) % 9) * F * NT + tid; };
+  // Plane p of the column (p may lie in the halos): wall halos replicate the
+  // boundary cell with w' = theta' = 0; periodic halos wrap (:780-797).
+  auto load_plane = [&](int p) {
+    const bool out = p < 0 || p >= nz;
+    const int pc = !out ? p : (wall ? clampi(p, nz) : wrapi(p, nz));
+    R w[F];
+    prims<R, NTR>(G, sin, size_t(pc) * NP + col, pc, w);
+    if (out && wall) {
+      w[iW] = R(0);
+      w[iT] = R(0);
+    }
+    R *dst = slot_ptr(p);
+#pragma unroll
+    for (int f = 0; f < F; f++) dst[f * NT] = w[f];
+  };
+  // Immersed bits of the z stencil of canonical cell cc: levels beyond the
+  // domain count as immersed (the z halos of the proportion are 1, :1031-1034).
+  auto stencil_flags = [&](int cc) {
+    unsigned imm = 0;
+#pragma unroll
+    for (int m = 0; m < 9; m++) {
+      const int p = cc - 4 + m;
+      unsigned b = (p < 0 || p >= nz) ? 1u : (IMM ? (unsigned(__ldg(G.flags + size_t(p) * NP + col)) & FLAG_IMM) : 0u);
+      imm |= b << m;
+    }
+    return imm;
+  };
+
+  const int cstart = (wall && k0 == 0) ? 0 : k0 - 1;
+  for (int p = cstart - 4; p <= cstart + 3; p++) load_plane(p);
+
+  R ERp[F], Fp[S];
+#pragma unroll
+  for (int f = 0; f < F; f++) ERp[f] = R(0);
+#pragma unroll
+  for (int s = 0; s < S; s++) Fp[s] = R(0);
+
+  for (int c = cstart; c <= k1; c++) {
+    load_plane(c + 4);
+    R EL[F], ER[F];
+    const bool have_cell = !(wall && c >= nz);
+    if (have_cell) {
+      const int cc = wall ? c : wrapi(c, nz);
+      const unsigned imm = stencil_flags(cc);
+      const bool any10 = IMM && (__ldg(G.flags + size_t(cc) * NP + col) & FLAG_ANY10);
+#pragma unroll
+      for (int f = 0; f < F; f++) {
+        R s[9];
+#pragma unroll
+        for (int m = 0; m < 9; m++) s[m] = slot_ptr(c - 4 + m)[f * NT];
+        if (f == iU || f == iV || f == iP) der0_modify(s, imm);
+        if (!any10 && !G.weno_all) linear9_edges(s, EL[f], ER[f]);
+        else weno9_edges(s, EL[f], ER[f], !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
+      }
+    } else {
+#pragma unroll
+      for (int f = 0; f < F; f++) EL[f] = ER[f] = R(0);
+    }
+    if (c > cstart || (wall && c == 0)) {
+      // Face c between cells c-1 and c (edge_exchange z, :891-908).
+      R Lf[F], Rf[F];
+      if (wall && c == 0) {
+#pragma unroll
+        for (int f = 0; f < F; f++) Lf[f] = Rf[f] = EL[f];
+        Lf[iW] = Rf[iW] = Lf[iT] = Rf[iT] = R(0);
+      } else if (wall && c == nz) {
+#pragma unroll
+        for (int f = 0; f < F; f++) Lf[f] = Rf[f] = ERp[f];
+        Lf[iW] = Rf[iW] = Lf[iT] = Rf[iT] = R(0);
+      } else {
+#pragma unroll
+        for (int f = 0; f < F; f++) {
+          Lf[f] = ERp[f];
+          Rf[f] = EL[f];
+        }
+      }
+      R Fc[S];
+      riemann<R, NTR>(Lf, Rf, __ldg(G.rho_e + c), __ldg(G.theta_e + c), iW, Fc);
+      if (c - 1 >= k0) {
+        // Finalise cell c-1.
+        const int k = c - 1;
+        const size_t idx = size_t(k) * NP + col;
+        R qin[S], out[S];
+#pragma unroll
+        for (int s = 0; s < S; s++) qin[s] = sin[s * G.N + idx];
+        R tend[S];
+#pragma unroll
+        for (int s = 0; s < S; s++) tend[s] = txy[s * G.N + idx] - (Fc[s] - Fp[s]) * G.rdz;
+        if (G.sim2d) tend[iV] = R(0);
+        if (G.enable_gravity) tend[iW] += -G.grav * qin[iR];
+        if (G.fcor != R(0) && !G.sim2d) {
+          tend[iU] += G.fcor * qin[iV];
+          tend[iV] -= G.fcor * qin[iU];
+        }
+        if (sn) {
+#pragma unroll
+          for (int s = 0; s < S; s++) out[s] = a_n * sn[s * G.N + idx] + a_in * qin[s] + a_dt * tend[s];
+        } else {
+#pragma unroll
+          for (int s = 0; s < S; s++) out[s] = qin[s] + a_dt * tend[s];
+        }
+        for (int e = 0; e < n_enforce; e++) enforce_cell<R, NTR, IMM>(G, out, idx, k);
+        bool bad = false;
+#pragma unroll
+        for (int s = 0; s < S; s++) {
+          bad |= !isfinite(out[s]);
+          sout[s * G.N + idx] = out[s];
+        }
+        if (bad) atomicOr(G.err, 1);
+      }
+#pragma unroll
+      for (int s = 0; s < S; s++) Fp[s] = Fc[s];
+    }
+#pragma unroll
+    for (int f = 0; f < F; f++) ERp[f] = ER[f];
+  }
+}
+
+// Enforcement pass on a state in place (the call at the top of
+// time_step_rk_3_3, dynamics_rk.h:301).
+template <class R, int NTR, bool IMM>
+__global__ void k_enforce(const Grid<R> G, R *__restrict__ s) {
+  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= G.N) return;
+  const int k = int(idx / G.NP);
+  R q[5 + NTR];
+#pragma unroll
+  for (int v = 0; v < 5 + NTR; v++) q[v] = s[v * G.N + idx];
+  enforce_cell<R, NTR, IMM>(G, q, idx, k);
+#pragma unroll
+  for (int v = 0; v < 5 + NTR; v++) s[v * G.N + idx] = q[v];
+}
+
+// ---------------------------------------------------------------------------
+// Coupler <-> dycore conversions (FP64 arithmetic, dynamics_rk.h:1251-1352).
+// ---------------------------------------------------------------------------
+struct CouplerPtrs {
+  const double *rho_d, *u, *v, *w, *T;
+  const double *tr[8];
+};
+struct CouplerOut {
+  double *rho_d, *u, *v, *w, *T;
+  double *tr[8];
+};
+struct Thermo {
+  double R_d, R_v, C0, gamma;
+  int idWV;
+  unsigned adds_mass;
+};
+
+template <class R, int NTR>
+__global__ void k_load_coupler(CouplerPtrs cp, Thermo th, const double *__restrict__ rho_off,
+                               const double *__restrict__ rt_off, size_t N, size_t NP, R *__restrict__ s) {
+  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= N) return;
+  const int k = int(idx / NP);
+  const double rd = cp.rho_d[idx], u = cp.u[idx], v = cp.v[idx], w = cp.w[idx], temp = cp.T[idx];
+  const double rho_v = cp.tr[th.idWV][idx];
+  const double press = rd * th.R_d * temp + rho_v * th.R_v * temp;
+  double rho = rd;
+#pragma unroll
+  for (int t = 0; t < NTR; t++)
+    if ((th.adds_mass >> t) & 1u) rho += cp.tr[t][idx];
+  const double theta = pow(press / th.C0, 1. / th.gamma) / rho;
+  s[0 * N + idx] = R(rho - rho_off[k]);
+  s[1 * N + idx] = R(rho * u);
+  s[2 * N + idx] = R(rho * v);
+  s[3 * N + idx] = R(rho * w);
+  s[4 * N + idx] = R(rho * theta - rt_off[k]);
+#pragma unroll
+  for (int t = 0; t < NTR; t++) s[(5 + t) * N + idx] = R(cp.tr[t][idx]);
+}
+
+template <class R, int NTR>
+__global__ void k_store_coupler(CouplerOut co, Thermo th, const double *__restrict__ rho_off,
+                                const double *__restrict__ rt_off, size_t N, size_t NP, const R *__restrict__ s) {
+  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= N) return;
+  const int k = int(idx / NP);
+  const double rho = rho_off[k] + double(s[idx]);
+  const double u = double(s[1 * N + idx]) / rho, v = double(s[2 * N + idx]) / rho, w = double(s[3 * N + idx]) / rho;
+  const double theta = (rt_off[k] + double(s[4 * N + idx])) / rho;
+  const double press = th.C0 * pow(rho * theta, th.gamma);
+  const double rho_v = double(s[(5 + th.idWV) * N + idx]);
+  double rd = rho;
+#pragma unroll
+  for (int t = 0; t < NTR; t++)
+    if ((th.adds_mass >> t) & 1u) rd -= double(s[(5 + t) * N + idx]);
+  co.rho_d[idx] = rd;
+  co.u[idx] = u;
+  co.v[idx] = v;
+  co.w[idx] = w;
+  co.T[idx] = press / (rd * th.R_d + rho_v * th.R_v);
+#pragma unroll
+  for (int t = 0; t < NTR; t++) co.tr[t][idx] = double(s[(5 + t) * N + idx]);
+}
+
+// Absolute conserved variables <-> perturbation storage.
+template <class R, int NTR>
+__global__ void k_get_conserved(const R *__restrict__ s, const double *__restrict__ rho_off,
+                                const double *__restrict__ rt_off, size_t N, size_t NP, double *__restrict__ st,
+                                double *__restrict__ tr) {
+  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= N) return;
+  const int k = int(idx / NP);
+  st[idx] = rho_off[k] + double(s[idx]);
+  st[N + idx] = double(s[N + idx]);
+  st[2 * N + idx] = double(s[2 * N + idx]);
+  st[3 * N + idx] = double(s[3 * N + idx]);
+  st[4 * N + idx] = rt_off[k] + double(s[4 * N + idx]);
+#pragma unroll
+  for (int t = 0; t < NTR; t++) tr[t * N + idx] = double(s[(5 + t) * N + idx]);
+}
+
+template <class R, int NTR>
+__global__ void k_set_conserved(R *__restrict__ s, const double *__restrict__ rho_off, const double *__restrict__ rt_off,
+                                size_t N, size_t NP, const double *__restrict__ st, const double *__restrict__ tr) {
+  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= N) return;
+  const int k = int(idx / NP);
+  s[idx] = R(st[idx] - rho_off[k]);
+  s[N + idx] = R(st[N + idx]);
+  s[2 * N + idx] = R(st[2 * N + idx]);
+  s[3 * N + idx] = R(st[3 * N + idx]);
+  s[4 * N + idx] = R(st[4 * N + idx] - rt_off[k]);
+#pragma unroll
+  for (int t = 0; t < NTR; t++) s[(5 + t) * N + idx] = R(tr[t * N + idx]);
+}
+
+// Re-express the perturbation state on new level offsets (after the
+// hydrostatic profiles change).
+template <class R>
+__global__ void k_rebase(R *__restrict__ s, const double *__restrict__ old_r, const double *__restrict__ old_rt,
+                         const double *__restrict__ new_r, const double *__restrict__ new_rt, size_t N, size_t NP) {
+  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= N) return;
+  const int k = int(idx / NP);
+  s[idx] = R(double(s[idx]) + old_r[k] - new_r[k]);
+  s[4 * N + idx] = R(double(s[4 * N + idx]) + old_rt[k] - new_rt[k]);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 hydrostatic profiles (init, dynamics_rk.h:961-1008, 1145-1186).
+// ---------------------------------------------------------------------------
+// Neumaier-compensated running sum.
+struct CSum {
+  double s, c;
+  __device__ void add(double x) {
+    double t = s + x;
+    c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+  }
+  __device__ void merge(const CSum &o) {
+    add(o.s);
+    c += o.c;
+  }
+};
+
+// Per level: compensated sums of rho, rho*theta/rho and C0*(rho*theta)^gamma
+// over the level, from the coupler arrays (as the reference forms the state
+// in convert_coupler_to_dynamics and then averages it, :967-975).
+template <int NTR>
+__global__ void k_column_sums(CouplerPtrs cp, Thermo th, int nx, int ny, double *__restrict__ sums) {
+  const int k = blockIdx.x;
+  const size_t base = size_t(k) * nx * ny;
+  CSum a{0, 0}, b{0, 0}, c{0, 0};
+  for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
+    const size_t idx = base + e;
+    const double rd = cp.rho_d[idx], temp = cp.T[idx];
+    const double rho_v = cp.tr[th.idWV][idx];
+    const double press = rd * th.R_d * temp + rho_v * th.R_v * temp;
+    double rho = rd;
+#pragma unroll
+    for (int t = 0; t < NTR; t++)
+      if ((th.adds_mass >> t) & 1u) rho += cp.tr[t][idx];
+    const double rt = rho * (pow(press / th.C0, 1. / th.gamma) / rho);
+    a.add(rho);
+    b.add(rt / rho);
+    c.add(th.C0 * pow(rt, th.gamma));
+  }
+  __shared__ CSum sh[3][256];
+  sh[0][threadIdx.x] = a;
+  sh[1][threadIdx.x] = b;
+  sh[2][threadIdx.x] = c;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int q = 0; q < 3; q++) sh[q][threadIdx.x].merge(sh[q][threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 3; q++) sums[q * gridDim.x + k] = sh[q][0].s + sh[q][0].c;
+}
+
+struct HydroOut {
+  double *cells;   // [3][nz+2HS]  dens, theta, pressure
+  double *edges;   // [3][nz+1]
+  double *rho_off, *rt_off;  // [nz]
+};
+
+template <class R>
+struct LevelTables {
+  R *rho_h, *theta_h, *rt_inv, *p0_h, *dp_h;  // nz+2HS
+  R *rho_e, *theta_e;                          // nz+1
+  R *rt_target;                                // nz
+};
+
+// Means, isentropic halo extension and edge profiles in FP64.  With
+// round32, every stored profile is rounded to float as the reference's
+// float DataManager arrays are, and the derived tables use those values.
+// If sums is null the cell profiles already in out.cells are used (restart).
+template <class R>
+__global__ void k_hydro_finish(const double *__restrict__ sums, int nz, double r_nx_ny, double gamma, double C0,
+                               double grav, double dz, int round32, HydroOut out, LevelTables<R> tab) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int nzh = nz + 2 * HS;
+  double *r = out.cells, *t = out.cells + nzh, *p = out.cells + 2 * nzh;
+  auto rnd = [&](double x) { return round32 ? double(float(x)) : x; };
+  if (sums) {
+    for (int k = 0; k < nz; k++) {
+      r[HS + k] = rnd(sums[k] * r_nx_ny);
+      t[HS + k] = rnd(sums[nz + k] * r_nx_ny);
+      p[HS + k] = rnd(sums[2 * nz + k] * r_nx_ny);
+    }
+    for (int kk = 0; kk < HS; kk++) {
+      {
+        const int k0 = HS, k = k0 - 1 - kk;
+        const double rho0 = r[k0], theta0 = t[k0];
+        const double rho0_gm1 = pow(rho0, gamma - 1), theta0_g = pow(theta0, gamma);
+        r[k] = rnd(pow(rho0_gm1 + grav * (gamma - 1) * dz * (kk + 1) / (gamma * C0 * theta0_g), 1. / (gamma - 1)));
+        t[k] = rnd(theta0);
+        p[k] = rnd(C0 * pow(r[k] * theta0, gamma));
+      }
+      {
+        const int k0 = HS + nz - 1, k = k0 + 1 + kk;
+        const double rho0 = r[k0], theta0 = t[k0];
+        const double rho0_gm1 = pow(rho0, gamma - 1), theta0_g = pow(theta0, gamma);
+        r[k] = rnd(pow(rho0_gm1 - grav * (gamma - 1) * dz * (kk + 1) / (gamma * C0 * theta0_g), 1. / (gamma - 1)));
+        t[k] = rnd(theta0);
+        p[k] = rnd(C0 * pow(r[k] * theta0, gamma));
+      }
+    }
+  }
+  double *re = out.edges, *te = out.edges + (nz + 1), *pe = out.edges + 2 * (nz + 1);
+  for (int k = 0; k < nz + 1; k++) {
+    re[k] = rnd(exp(-1. / 12. * log(r[HS + k - 2]) + 7. / 12. * log(r[HS + k - 1]) + 7. / 12. * log(r[HS + k]) +
+                    -1. / 12. * log(r[HS + k + 1])));
+    te[k] = rnd(-1. / 12. * t[HS + k - 2] + 7. / 12. * t[HS + k - 1] + 7. / 12. * t[HS + k] + -1. / 12. * t[HS + k + 1]);
+    pe[k] = rnd(exp(-1. / 12. * log(p[HS + k - 2]) + 7. / 12. * log(p[HS + k - 1]) + 7. / 12. * log(p[HS + k]) +
+                    -1. / 12. * log(p[HS + k + 1])));
+    tab.rho_e[k] = R(re[k]);
+    tab.theta_e[k] = R(te[k]);
+  }
+  for (int k = 0; k < nzh; k++) {
+    const double rt = r[k] * t[k];
+    const double P0 = C0 * pow(rt, gamma);
+    tab.rho_h[k] = R(r[k]);
+    tab.theta_h[k] = R(t[k]);
+    tab.rt_inv[k] = R(1. / rt);
+    tab.p0_h[k] = R(P0);
+    tab.dp_h[k] = R(P0 - p[k]);
+  }
+  for (int k = 0; k < nz; k++) {
+    const double rt = r[HS + k] * t[HS + k];
+    out.rho_off[k] = r[HS + k];
+    out.rt_off[k] = rt;
+    // The reference's relaxation target for rho*theta is the float product
+    // hy_dens_cells*hy_theta_cells (dynamics_rk.h:459).
+    tab.rt_target[k] = R(round32 ? double(float(r[HS + k]) * float(t[HS + k])) - rt : 0.0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Immersed-boundary preprocessing (init, :389-425 and :1010-1143).
+// ---------------------------------------------------------------------------
+// Chebyshev distance (capped at cap+1) to the nearest cell whose indicator is
+// set, along one axis at a time; x and y wrap, z has nothing beyond the walls.
+static __global__ void k_dist_init(const double *__restrict__ prop, int mode, size_t N, uint8_t *__restrict__ d, int cap) {
+  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= N) return;
+  const bool set = mode == 0 ? prop[idx] > 0 : prop[idx] == 0;
+  d[idx] = set ? 0 : uint8_t(cap + 1);
+}
+
+static __global__ void k_dist_pass(const uint8_t *__restrict__ in, uint8_t *__restrict__ out, int nx, int ny, int nz, int axis,
+                            int cap) {
+  const size_t N = size_t(nx) * ny * nz;
+  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= N) return;
+  const int i = int(idx % nx), j = int((idx / nx) % ny), k = int(idx / (size_t(nx) * ny));
+  int best = in[idx];
+  for (int o = 1; o <= cap; o++) {
+    for (int sgn = -1; sgn <= 1; sgn += 2) {
+      int ii = i, jj = j, kk = k;
+      if (axis == 0) ii = wrapi(i + sgn * o, nx);
+      else if (axis == 1) jj = wrapi(j + sgn * o, ny);
+      else {
+        kk = k + sgn * o;
+        if (kk < 0 || kk >= nz) continue;
+      }
+      const int v = in[(size_t(kk) * ny + jj) * nx + ii];
+      const int cand = v > o ? v : o;
+      if (cand < best) best = cand;
+    }
+  }
+  out[idx] = uint8_t(best);
+}
+
+template <class R>
+__global__ void k_imm_finish(const double *__restrict__ prop, const uint8_t *__restrict__ d_imm,
+                             const uint8_t *__restrict__ d_zero, double power, size_t N, uint8_t *__restrict__ flags,
+                             R *__restrict__ mult) {
+  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= N) return;
+  const double pr = prop[idx];
+  const int dz = d_zero[idx];
+  const int tau = dz <= 1 ? 8 : dz == 2 ? 4 : dz == 3 ? 2 : 1;
+  flags[idx] = uint8_t((pr > 0 ? FLAG_IMM : 0u) | (d_imm[idx] <= 10 ? FLAG_ANY10 : 0u));
+  mult[idx] = R(pow(pr, power) / tau);
+}
+
+// ---------------------------------------------------------------------------
+// FP64 compensated global integrals.
+// ---------------------------------------------------------------------------
+constexpr int NDIAG = 6 + 8;
+
+template <class R, int NTR>
+__global__ void k_diag_partial(const R *__restrict__ s, const double *__restrict__ rho_off,
+                               const double *__restrict__ rt_off, size_t N, size_t NP, double dV, double dz,
+                               double grav, double C0, double gamma, double *__restrict__ partial) {
+  CSum acc[6 + NTR];
+#pragma unroll
+  for (int q = 0; q < 6 + NTR; q++) acc[q] = CSum{0, 0};
+  for (size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < N; idx += size_t(gridDim.x) * blockDim.x) {
+    const int k = int(idx / NP);
+    const double rho = rho_off[k] + double(s[idx]);
+    const double mu = double(s[N + idx]), mv = double(s[2 * N + idx]), mw = double(s[3 * N + idx]);
+    const double rt = rt_off[k] + double(s[4 * N + idx]);
+    const double ke = 0.5 * (mu * mu + mv * mv + mw * mw) / rho;
+    const double ie = C0 * pow(rt, gamma) / (gamma - 1);
+    const double pe = rho * grav * (k + 0.5) * dz;
+    acc[0].add(rho * dV);
+    acc[1].add(rt * dV);
+    acc[2].add(ke * dV);
+    acc[3].add(ie * dV);
+    acc[4].add(pe * dV);
+    acc[5].add((ke + ie + pe) * dV);
+#pragma unroll
+    for (int t = 0; t < NTR; t++) acc[6 + t].add(double(s[(5 + t) * N + idx]) * dV);
+  }
+  __shared__ CSum sh[256];
+  for (int q = 0; q < 6 + NTR; q++) {
+    sh[threadIdx.x] = acc[q];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) sh[threadIdx.x].merge(sh[threadIdx.x + w]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      partial[(size_t(blockIdx.x) * NDIAG + q) * 2 + 0] = sh[0].s;
+      partial[(size_t(blockIdx.x) * NDIAG + q) * 2 + 1] = sh[0].c;
+    }
+    __syncthreads();
+  }
+}
+
+static __global__ void k_diag_final(const double *__restrict__ partial, int nblocks, int nq, double *__restrict__ out) {
+  const int q = threadIdx.x;
+  if (q >= nq) return;
+  CSum a{0, 0};
+  for (int b = 0; b < nblocks; b++) {
+    a.add(partial[(size_t(b) * NDIAG + q) * 2 + 0]);
+    a.c += partial[(size_t(b) * NDIAG + q) * 2 + 1];
+  }
+  out[q] = a.s + a.c;
+}
+
+}  // namespace pu

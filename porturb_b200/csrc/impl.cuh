@@ -1,0 +1,518 @@
+// Host-side implementation of one dycore handle for a stencil type R and a
+// tracer count NTR.  pu_dycore.cu holds the C entry points; impl_inst.cu is
+// compiled once per (R, NTR) with PU_REAL / PU_NTR defined.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pu_dycore.h"
+#include "dycore_kernels.cuh"
+
+namespace pu {
+
+void set_error(const std::string &msg);
+
+#define PU_CK(x)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (x);                                                                 \
+    if (e_ != cudaSuccess) {                                                              \
+      set_error(std::string(#x) + ": " + cudaGetErrorString(e_));                         \
+      return PU_ERR_CUDA;                                                                 \
+    }                                                                                     \
+  } while (0)
+
+#define PU_LAUNCHED()                                                                     \
+  do {                                                                                    \
+    cudaError_t e_ = cudaGetLastError();                                                  \
+    if (e_ != cudaSuccess) {                                                              \
+      set_error(std::string("kernel launch: ") + cudaGetErrorString(e_));                 \
+      return PU_ERR_CUDA;                                                                 \
+    }                                                                                     \
+    launches++;                                                                           \
+  } while (0)
+
+struct ImplBase {
+  pu_config cfg{};
+  cudaStream_t st = nullptr;
+  int ntr = 0, S = 0, F = 0, nzh = 0;
+  size_t N = 0, NP = 0;
+  bool inited = false, has_imm = false;
+  long long launches = 0;
+  // Device buffers.
+  void *s[3] = {nullptr, nullptr, nullptr};   // state, two stage buffers
+  void *txy = nullptr;                        // x/y tendency of the current stage
+  double *staging = nullptr;                  // (5+ntr)*N doubles for host-side coupler views
+  double *cells = nullptr, *edges = nullptr;  // FP64 profiles [3][nzh], [3][nz+1]
+  double *rho_off = nullptr, *rt_off = nullptr;
+  void *tabs = nullptr;                       // level tables of type R
+  uint8_t *flags = nullptr;
+  void *imm_mult = nullptr;
+  int *err = nullptr;
+  double *sums = nullptr;
+  double *diag_part = nullptr, *diag_out = nullptr;
+  int diag_blocks = 0;
+  // Event-based per-kernel timing (pu_dycore_profile).
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pairs;
+  size_t ev_next = 0;
+
+  cudaEvent_t next_event() {
+    if (ev_next == ev_pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      ev_pool.push_back(e);
+    }
+    return ev_pool[ev_next++];
+  }
+  // Records a start event when profiling; returns it (or null).
+  cudaEvent_t prof_begin() {
+    if (!profiling) return nullptr;
+    cudaEvent_t e = next_event();
+    cudaEventRecord(e, st);
+    return e;
+  }
+  void prof_end(int kind, cudaEvent_t start) {
+    if (!start) return;
+    cudaEvent_t e = next_event();
+    cudaEventRecord(e, st);
+    ev_pairs.push_back({kind, {start, e}});
+  }
+  void prof_reset() {
+    ev_pairs.clear();
+    ev_next = 0;
+  }
+  int prof_read(pu_profile *out) {
+    PU_CK(cudaStreamSynchronize(st));
+    for (int q = 0; q < PU_PROFILE_KINDS; q++) {
+      out->ms[q] = 0;
+      out->launches[q] = 0;
+    }
+    for (auto &p : ev_pairs) {
+      float ms = 0;
+      PU_CK(cudaEventElapsedTime(&ms, p.second.first, p.second.second));
+      out->ms[p.first] += ms;
+      out->launches[p.first]++;
+    }
+    return PU_OK;
+  }
+
+  virtual ~ImplBase() {
+    for (auto e : ev_pool) cudaEventDestroy(e);
+  }
+  virtual int alloc() = 0;
+  virtual int init(const pu_state_view *v, const double *prop, int mem) = 0;
+  virtual int load_state(const pu_state_view *v) = 0;
+  virtual int store_state(pu_state_view *v) = 0;
+  virtual int advance(double dt, int nsteps) = 0;
+  virtual int get_conserved(double *st, double *tr, int mem) = 0;
+  virtual int set_conserved(const double *st, const double *tr, int mem) = 0;
+  virtual int set_hydrostasis(const double *r, const double *t, const double *p) = 0;
+  virtual int diagnostics(pu_diag *out) = 0;
+
+  int check_err() {
+    int h = 0;
+    PU_CK(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PU_CK(cudaStreamSynchronize(st));
+    if (h) {
+      PU_CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+      set_error("the dycore state became non-finite");
+      return PU_ERR_NONFINITE;
+    }
+    return PU_OK;
+  }
+};
+
+ImplBase *make_impl_f32(int ntr);
+ImplBase *make_impl_f64(int ntr);
+
+template <class R, int NTR>
+struct Impl : ImplBase {
+  static constexpr int XTX_BIG = 16, XTY_BIG = 16;   // x/y tile for ny >= 16
+  static constexpr int XTX_SM = 32, XTY_SM = 4;      // x/y tile for thin domains
+  static constexpr int ZTX = 32, ZTY = 4;            // z-march columns per block
+  LevelTables<R> lt{};
+  bool small_tile = false;
+
+  ~Impl() override {
+    for (auto p : {s[0], s[1], s[2], txy, (void *)staging, (void *)cells, (void *)edges, (void *)rho_off,
+                   (void *)rt_off, tabs, (void *)flags, imm_mult, (void *)err, (void *)sums, (void *)diag_part,
+                   (void *)diag_out})
+      if (p) cudaFree(p);
+  }
+
+  template <class T>
+  int dalloc(T *&p, size_t n) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T) > 0 ? n * sizeof(T) : 16);
+    if (e != cudaSuccess) {
+      set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      return e == cudaErrorMemoryAllocation ? PU_ERR_NOMEM : PU_ERR_CUDA;
+    }
+    p = static_cast<T *>(q);
+    return PU_OK;
+  }
+#define PU_TRY(x)                 \
+  do {                            \
+    int rc_ = (x);                \
+    if (rc_ != PU_OK) return rc_; \
+  } while (0)
+
+  int alloc() override {
+    F = 6 + NTR;
+    S = 5 + NTR;
+    for (int b = 0; b < 3; b++) {
+      R *p;
+      PU_TRY(dalloc(p, size_t(S) * N));
+      s[b] = p;
+    }
+    R *t;
+    PU_TRY(dalloc(t, size_t(S) * N));
+    txy = t;
+    PU_TRY(dalloc(staging, size_t(5 + NTR) * N));
+    PU_TRY(dalloc(cells, size_t(3) * nzh));
+    PU_TRY(dalloc(edges, size_t(3) * (cfg.nz + 1)));
+    PU_TRY(dalloc(rho_off, size_t(cfg.nz)));
+    PU_TRY(dalloc(rt_off, size_t(cfg.nz)));
+    R *tb;
+    const size_t ntab = 5 * size_t(nzh) + 2 * size_t(cfg.nz + 1) + size_t(cfg.nz);
+    PU_TRY(dalloc(tb, ntab));
+    tabs = tb;
+    lt.rho_h = tb;
+    lt.theta_h = tb + nzh;
+    lt.rt_inv = tb + 2 * nzh;
+    lt.p0_h = tb + 3 * nzh;
+    lt.dp_h = tb + 4 * nzh;
+    lt.rho_e = tb + 5 * nzh;
+    lt.theta_e = lt.rho_e + (cfg.nz + 1);
+    lt.rt_target = lt.theta_e + (cfg.nz + 1);
+    PU_TRY(dalloc(err, 1));
+    PU_CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+    PU_TRY(dalloc(sums, size_t(3) * cfg.nz));
+    diag_blocks = 296;
+    PU_TRY(dalloc(diag_part, size_t(diag_blocks) * NDIAG * 2));
+    PU_TRY(dalloc(diag_out, size_t(NDIAG)));
+    small_tile = cfg.ny < 16;
+    PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_BIG, XTY_BIG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(XYShape<R, NTR, XTX_BIG, XTY_BIG, false>::bytes)));
+    PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_BIG, XTY_BIG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(XYShape<R, NTR, XTX_BIG, XTY_BIG, true>::bytes)));
+    PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_SM, XTY_SM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(XYShape<R, NTR, XTX_SM, XTY_SM, false>::bytes)));
+    PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_SM, XTY_SM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(XYShape<R, NTR, XTX_SM, XTY_SM, true>::bytes)));
+    PU_CK(cudaFuncSetAttribute(k_z<R, NTR, ZTX, ZTY, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(ZShape<R, NTR, ZTX, ZTY>::bytes)));
+    PU_CK(cudaFuncSetAttribute(k_z<R, NTR, ZTX, ZTY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(ZShape<R, NTR, ZTX, ZTY>::bytes)));
+    return PU_OK;
+  }
+
+  Thermo thermo() const {
+    Thermo th;
+    th.R_d = cfg.R_d;
+    th.R_v = cfg.R_v;
+    th.C0 = cfg.C0;
+    th.gamma = cfg.gamma_d;
+    th.idWV = cfg.idWV;
+    th.adds_mass = 0;
+    for (int t = 0; t < NTR; t++)
+      if (cfg.tracer_adds_mass[t]) th.adds_mass |= 1u << t;
+    return th;
+  }
+
+  Grid<R> grid() const {
+    Grid<R> G;
+    G.nx = cfg.nx;
+    G.ny = cfg.ny;
+    G.nz = cfg.nz;
+    G.N = N;
+    G.NP = NP;
+    G.rdx = R(1. / cfg.dx);
+    G.rdy = R(1. / cfg.dy);
+    G.rdz = R(1. / cfg.dz);
+    G.bc_x = cfg.bc_x;
+    G.bc_y = cfg.bc_y;
+    G.bc_z = cfg.bc_z;
+    G.sim2d = cfg.ny == 1;
+    G.weno_all = cfg.weno_all;
+    G.enable_gravity = cfg.enable_gravity;
+    G.grav = R(cfg.grav);
+    G.fcor = R(2 * 7.2921e-5 * std::sin(cfg.latitude / 180 * M_PI));
+    G.gamma = R(cfg.gamma_d);
+    G.tracer_positive = 0;
+    for (int t = 0; t < NTR; t++)
+      if (cfg.tracer_positive[t]) G.tracer_positive |= 1u << t;
+    G.rho_h = lt.rho_h;
+    G.theta_h = lt.theta_h;
+    G.rt_inv = lt.rt_inv;
+    G.p0_h = lt.p0_h;
+    G.dp_h = lt.dp_h;
+    G.rho_e = lt.rho_e;
+    G.theta_e = lt.theta_e;
+    G.rt_target = lt.rt_target;
+    G.flags = has_imm ? flags : nullptr;
+    G.imm_mult = has_imm ? static_cast<const R *>(imm_mult) : nullptr;
+    G.err = err;
+    return G;
+  }
+
+  // Coupler view -> device pointers (copying host arrays into staging).
+  int device_view(const pu_state_view *v, CouplerPtrs &cp) {
+    const double *src[5] = {v->rho_d, v->uvel, v->vvel, v->wvel, v->temp};
+    for (int a = 0; a < 5; a++)
+      if (!src[a]) { set_error("coupler view has a null array"); return PU_ERR_INVALID; }
+    for (int t = 0; t < NTR; t++)
+      if (!v->tracers[t]) { set_error("coupler view has a null tracer array"); return PU_ERR_INVALID; }
+    const double *d[5 + NTR];
+    if (v->mem == PU_MEM_DEVICE) {
+      for (int a = 0; a < 5; a++) d[a] = src[a];
+      for (int t = 0; t < NTR; t++) d[5 + t] = v->tracers[t];
+    } else {
+      for (int a = 0; a < 5 + NTR; a++) {
+        const double *h = a < 5 ? src[a] : v->tracers[a - 5];
+        PU_CK(cudaMemcpyAsync(staging + size_t(a) * N, h, N * sizeof(double), cudaMemcpyHostToDevice, st));
+        d[a] = staging + size_t(a) * N;
+      }
+    }
+    cp.rho_d = d[0]; cp.u = d[1]; cp.v = d[2]; cp.w = d[3]; cp.T = d[4];
+    for (int t = 0; t < 8; t++) cp.tr[t] = t < NTR ? d[5 + t] : nullptr;
+    return PU_OK;
+  }
+
+  unsigned blocks(size_t n, int bs) const { return unsigned((n + bs - 1) / bs); }
+
+  int init(const pu_state_view *v, const double *prop, int mem) override {
+    CouplerPtrs cp;
+    PU_TRY(device_view(v, cp));
+    const Thermo th = thermo();
+    k_column_sums<NTR><<<cfg.nz, 256, 0, st>>>(cp, th, cfg.nx, cfg.ny, sums);
+    PU_LAUNCHED();
+    HydroOut ho{cells, edges, rho_off, rt_off};
+    const double r_nx_ny = 1. / (double(cfg.nx) * double(cfg.ny));
+    k_hydro_finish<R><<<1, 1, 0, st>>>(sums, cfg.nz, r_nx_ny, cfg.gamma_d, cfg.C0, cfg.grav, cfg.dz,
+                                       sizeof(R) == 4, ho, lt);
+    PU_LAUNCHED();
+    // Immersed preprocessing.
+    has_imm = false;
+    if (prop) {
+      double *dprop = nullptr;
+      PU_TRY(dalloc(dprop, N));
+      if (mem == PU_MEM_DEVICE) PU_CK(cudaMemcpyAsync(dprop, prop, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      else PU_CK(cudaMemcpyAsync(dprop, prop, N * sizeof(double), cudaMemcpyHostToDevice, st));
+      uint8_t *d0 = nullptr, *d1 = nullptr, *dz = nullptr;
+      int rc = dalloc(d0, N);
+      if (rc == PU_OK) rc = dalloc(d1, N);
+      if (rc == PU_OK) rc = dalloc(dz, N);
+      int *anyp = nullptr;
+      if (rc == PU_OK) rc = dalloc(anyp, 1);
+      if (rc == PU_OK) rc = imm_prepare(dprop, d0, d1, dz, anyp);
+      cudaStreamSynchronize(st);
+      for (void *p : {(void *)dprop, (void *)d0, (void *)d1, (void *)dz, (void *)anyp})
+        if (p) cudaFree(p);
+      if (rc != PU_OK) return rc;
+    }
+    PU_TRY(load_state(v));
+    PU_CK(cudaStreamSynchronize(st));
+    inited = true;
+    return PU_OK;
+  }
+
+  int imm_prepare(const double *dprop, uint8_t *a, uint8_t *b, uint8_t *dzero, int *anyp) {
+    // Any immersed cell at all?
+    PU_CK(cudaMemsetAsync(anyp, 0, sizeof(int), st));
+    k_dist_init<<<blocks(N, 256), 256, 0, st>>>(dprop, 0, N, a, 10);
+    PU_LAUNCHED();
+    // a: distance to immersed (cap 10) -> any_immersed10
+    for (int axis = 0; axis < 3; axis++) {
+      k_dist_pass<<<blocks(N, 256), 256, 0, st>>>(a, b, cfg.nx, cfg.ny, cfg.nz, axis, 10);
+      PU_LAUNCHED();
+      std::swap(a, b);
+    }
+    // dzero: distance to a non-immersed cell (cap 3) -> immersed_tau
+    k_dist_init<<<blocks(N, 256), 256, 0, st>>>(dprop, 1, N, dzero, 3);
+    PU_LAUNCHED();
+    for (int axis = 0; axis < 3; axis++) {
+      k_dist_pass<<<blocks(N, 256), 256, 0, st>>>(dzero, b, cfg.nx, cfg.ny, cfg.nz, axis, 3);
+      PU_LAUNCHED();
+      PU_CK(cudaMemcpyAsync(dzero, b, N, cudaMemcpyDeviceToDevice, st));
+    }
+    if (!flags) PU_TRY(dalloc(flags, N));
+    if (!imm_mult) {
+      R *m;
+      PU_TRY(dalloc(m, N));
+      imm_mult = m;
+    }
+    k_imm_finish<R><<<blocks(N, 256), 256, 0, st>>>(dprop, a, dzero, cfg.immersed_power, N, flags,
+                                                    static_cast<R *>(imm_mult));
+    PU_LAUNCHED();
+    // has_imm: any flag set (a cell with prop > 0 has distance 0 in `a`).
+    std::vector<uint8_t> hf(N);
+    PU_CK(cudaMemcpyAsync(hf.data(), flags, N, cudaMemcpyDeviceToHost, st));
+    PU_CK(cudaStreamSynchronize(st));
+    has_imm = false;
+    for (size_t q = 0; q < N && !has_imm; q++) has_imm = (hf[q] & FLAG_IMM) != 0;
+    return PU_OK;
+  }
+
+  int load_state(const pu_state_view *v) override {
+    CouplerPtrs cp;
+    PU_TRY(device_view(v, cp));
+    k_load_coupler<R, NTR><<<blocks(N, 256), 256, 0, st>>>(cp, thermo(), rho_off, rt_off, N, NP,
+                                                           static_cast<R *>(s[0]));
+    PU_LAUNCHED();
+    return PU_OK;
+  }
+
+  int store_state(pu_state_view *v) override {
+    CouplerOut co;
+    double *d[5 + NTR];
+    double *dst[5] = {v->rho_d, v->uvel, v->vvel, v->wvel, v->temp};
+    for (int a = 0; a < 5; a++)
+      if (!dst[a]) { set_error("coupler view has a null array"); return PU_ERR_INVALID; }
+    for (int t = 0; t < NTR; t++)
+      if (!v->tracers[t]) { set_error("coupler view has a null tracer array"); return PU_ERR_INVALID; }
+    for (int a = 0; a < 5 + NTR; a++) {
+      double *h = a < 5 ? dst[a] : v->tracers[a - 5];
+      d[a] = v->mem == PU_MEM_DEVICE ? h : staging + size_t(a) * N;
+    }
+    co.rho_d = d[0]; co.u = d[1]; co.v = d[2]; co.w = d[3]; co.T = d[4];
+    for (int t = 0; t < 8; t++) co.tr[t] = t < NTR ? d[5 + t] : nullptr;
+    k_store_coupler<R, NTR><<<blocks(N, 256), 256, 0, st>>>(co, thermo(), rho_off, rt_off, N, NP,
+                                                            static_cast<const R *>(s[0]));
+    PU_LAUNCHED();
+    if (v->mem != PU_MEM_DEVICE)
+      for (int a = 0; a < 5 + NTR; a++) {
+        double *h = a < 5 ? dst[a] : v->tracers[a - 5];
+        PU_CK(cudaMemcpyAsync(h, staging + size_t(a) * N, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+      }
+    return check_err();
+  }
+
+  template <bool IMM>
+  int stage(const Grid<R> &G, const R *sin, const R *sn, R *sout, R a_n, R a_in, R a_dt, int n_enforce) {
+    R *t = static_cast<R *>(txy);
+    cudaEvent_t e0 = prof_begin();
+    if (small_tile) {
+      using Sh = XYShape<R, NTR, XTX_SM, XTY_SM, IMM>;
+      dim3 g(blocks(cfg.nx, XTX_SM), blocks(cfg.ny, XTY_SM), cfg.nz);
+      k_xy<R, NTR, XTX_SM, XTY_SM, IMM><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
+    } else {
+      using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM>;
+      dim3 g(blocks(cfg.nx, XTX_BIG), blocks(cfg.ny, XTY_BIG), cfg.nz);
+      k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
+    }
+    PU_LAUNCHED();
+    prof_end(0, e0);
+    const int kc = cfg.z_chunk > 0 ? cfg.z_chunk : (cfg.nz < 32 ? cfg.nz : 32);
+    dim3 gz(blocks(cfg.nx, ZTX), blocks(cfg.ny, ZTY), blocks(cfg.nz, kc));
+    cudaEvent_t e1 = prof_begin();
+    k_z<R, NTR, ZTX, ZTY, IMM><<<gz, ZTX * ZTY, ZShape<R, NTR, ZTX, ZTY>::bytes, st>>>(G, sin, sn, sout, t, a_n, a_in,
+                                                                                     a_dt, n_enforce, kc);
+    PU_LAUNCHED();
+    prof_end(1, e1);
+    return PU_OK;
+  }
+
+  template <bool IMM>
+  int advance_t(double dt, int nsteps) {
+    const Grid<R> G = grid();
+    R *s0 = static_cast<R *>(s[0]), *s1 = static_cast<R *>(s[1]), *s2 = static_cast<R *>(s[2]);
+    cudaEvent_t e0 = prof_begin();
+    k_enforce<R, NTR, IMM><<<blocks(N, 256), 256, 0, st>>>(G, s0);
+    PU_LAUNCHED();
+    prof_end(2, e0);
+    for (int n = 0; n < nsteps; n++) {
+      PU_TRY(stage<IMM>(G, s0, nullptr, s1, R(0), R(1), R(dt), 1));
+      PU_TRY(stage<IMM>(G, s1, s0, s2, R(3. / 4.), R(1. / 4.), R(1. / 4. * dt), 1));
+      PU_TRY(stage<IMM>(G, s2, s0, s0, R(1. / 3.), R(2. / 3.), R(2. / 3. * dt), n == nsteps - 1 ? 1 : 2));
+    }
+    return PU_OK;
+  }
+
+  int advance(double dt, int nsteps) override {
+    if (nsteps <= 0) return PU_OK;
+    return has_imm ? advance_t<true>(dt, nsteps) : advance_t<false>(dt, nsteps);
+  }
+
+  int get_conserved(double *stp, double *trp, int mem) override {
+    double *dst = staging;
+    k_get_conserved<R, NTR><<<blocks(N, 256), 256, 0, st>>>(static_cast<const R *>(s[0]), rho_off, rt_off, N, NP,
+                                                            dst, dst + 5 * N);
+    PU_LAUNCHED();
+    auto kind = mem == PU_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    PU_CK(cudaMemcpyAsync(stp, dst, 5 * N * sizeof(double), kind, st));
+    if (trp) PU_CK(cudaMemcpyAsync(trp, dst + 5 * N, size_t(NTR) * N * sizeof(double), kind, st));
+    PU_CK(cudaStreamSynchronize(st));
+    return PU_OK;
+  }
+
+  int set_conserved(const double *stp, const double *trp, int mem) override {
+    auto kind = mem == PU_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    PU_CK(cudaMemcpyAsync(staging, stp, 5 * N * sizeof(double), kind, st));
+    PU_CK(cudaMemcpyAsync(staging + 5 * N, trp, size_t(NTR) * N * sizeof(double), kind, st));
+    k_set_conserved<R, NTR><<<blocks(N, 256), 256, 0, st>>>(static_cast<R *>(s[0]), rho_off, rt_off, N, NP, staging,
+                                                            staging + 5 * N);
+    PU_LAUNCHED();
+    PU_CK(cudaStreamSynchronize(st));
+    return PU_OK;
+  }
+
+  int set_hydrostasis(const double *r, const double *t, const double *p) override {
+    double *old_r = nullptr, *old_rt = nullptr;
+    PU_TRY(dalloc(old_r, cfg.nz));
+    int rc = dalloc(old_rt, cfg.nz);
+    if (rc == PU_OK) {
+      cudaMemcpyAsync(old_r, rho_off, cfg.nz * sizeof(double), cudaMemcpyDeviceToDevice, st);
+      cudaMemcpyAsync(old_rt, rt_off, cfg.nz * sizeof(double), cudaMemcpyDeviceToDevice, st);
+      std::vector<double> h(3 * size_t(nzh));
+      for (int k = 0; k < nzh; k++) {
+        double a = r[k], b = t[k], c = p[k];
+        if (sizeof(R) == 4) { a = double(float(a)); b = double(float(b)); c = double(float(c)); }
+        h[k] = a;
+        h[nzh + k] = b;
+        h[2 * nzh + k] = c;
+      }
+      cudaMemcpyAsync(cells, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+      HydroOut ho{cells, edges, rho_off, rt_off};
+      k_hydro_finish<R><<<1, 1, 0, st>>>(nullptr, cfg.nz, 0., cfg.gamma_d, cfg.C0, cfg.grav, cfg.dz, sizeof(R) == 4, ho,
+                                         lt);
+      launches++;
+      k_rebase<R><<<blocks(N, 256), 256, 0, st>>>(static_cast<R *>(s[0]), old_r, old_rt, rho_off, rt_off, N, NP);
+      launches++;
+      cudaError_t e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); rc = PU_ERR_CUDA; }
+    }
+    cudaFree(old_r);
+    if (old_rt) cudaFree(old_rt);
+    return rc;
+  }
+
+  int diagnostics(pu_diag *out) override {
+    const double dV = cfg.dx * cfg.dy * cfg.dz;
+    k_diag_partial<R, NTR><<<diag_blocks, 256, 0, st>>>(static_cast<const R *>(s[0]), rho_off, rt_off, N, NP, dV, cfg.dz,
+                                                        cfg.grav, cfg.C0, cfg.gamma_d, diag_part);
+    PU_LAUNCHED();
+    k_diag_final<<<1, 32, 0, st>>>(diag_part, diag_blocks, 6 + NTR, diag_out);
+    PU_LAUNCHED();
+    double h[NDIAG] = {0};
+    PU_CK(cudaMemcpyAsync(h, diag_out, (6 + NTR) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PU_CK(cudaStreamSynchronize(st));
+    out->mass = h[0];
+    out->rho_theta = h[1];
+    out->kinetic = h[2];
+    out->internal = h[3];
+    out->potential = h[4];
+    out->total_energy = h[5];
+    for (int t = 0; t < PU_MAX_TRACERS; t++) out->tracer_mass[t] = t < NTR ? h[6 + t] : 0.0;
+    return PU_OK;
+  }
+#undef PU_TRY
+};
+
+}  // namespace pu

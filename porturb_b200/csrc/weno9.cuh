@@ -1,0 +1,145 @@
+// Order-9 WENO reconstruction of the two cell-edge values of one stencil.
+//
+// Follows limiter::WenoLimiter<real,9>::compute_limited_edges
+// (model/modules/helpers/WenoLimiter.h:349-437):
+//   1. smoothness indicators TV_1..TV_5 of the five 5-cell sub-stencils
+//      (TransformMatrices.h:429-433, 19841-19880), normalised to sum 1
+//      (convexify, WenoLimiter.h:30-34);
+//   2. imm_L: TV_5 = max(TV), imm_R: TV_1 = max(TV)  (WenoLimiter.h:430-437);
+//   3. per edge: w_k = ideal_k / (TV_k^2 + 1e-20), normalise, optionally
+//      apply map_rs (k=6, m=3, s=2000; WenoLimiter.h:75-82) and normalise
+//      again, then the weighted sub-stencil edge values (WenoLimiter.h:382-426).
+// The arithmetic is rearranged (see gen_weno9.py): stencil differences, an
+// LDL^T form of TV, edge values as s_4 plus linear forms, and one reciprocal
+// shared by both edges for each 1/(TV_k^2+1e-20).  In FP32 the reciprocals
+// use rcp.approx.ftz; every operand is a normal number there: TV_k^2+1e-20 >=
+// 1e-20, the normalisation sums exceed 1e-20 on the branch that divides, and
+// the map_rs denominator is at least ideal_k^6 > 2e-13.
+#pragma once
+
+#include "weno9_tables.cuh"
+
+namespace pu {
+
+template <class R>
+__device__ __forceinline__ R fast_rcp(R x) { return R(1) / x; }
+
+template <>
+__device__ __forceinline__ float fast_rcp<float>(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+template <class R>
+__device__ __forceinline__ void convexify5(R (&w)[5]) {
+  R tot = w[0] + w[1] + w[2] + w[3] + w[4];
+  if (tot > R(1.e-20)) {
+    R r = fast_rcp(tot);
+#pragma unroll
+    for (int k = 0; k < 5; k++) w[k] *= r;
+  }
+}
+
+// One edge: weights from the shared reciprocals rk = 1/(TV_k^2 + 1e-20).
+template <class R, bool LEFT>
+__device__ __forceinline__ R weno9_edge(const R (&d)[8], R s4, const R (&rk)[5], bool do_map) {
+  using namespace pu_weno9;
+  R w[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) w[k] = R(LEFT ? IDEAL_L[k] : IDEAL_R[k]) * rk[k];
+  convexify5(w);
+  if (do_map) {
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      const R dk = R(LEFT ? IDEAL_L[k] : IDEAL_R[k]);
+      R t = w[k] - dk;
+      R t2 = t * t;
+      R t6 = t2 * t2 * t2;
+      R u = fma(-w[k], w[k], w[k]);   // w (1 - w)
+      R u3 = u * u * u;
+      R den = fma(R(2000.), u3, t6);
+      w[k] = fma(t6 * t, fast_rcp(den), dk);
+    }
+    convexify5(w);
+  }
+  R acc = R(0);
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    R lin = R(LEFT ? LIN_L[k][0] : LIN_R[k][0]) * d[k];
+#pragma unroll
+    for (int m = 1; m < 4; m++) lin = fma(R(LEFT ? LIN_L[k][m] : LIN_R[k][m]), d[k + m], lin);
+    acc = fma(w[k], lin, acc);
+  }
+  return s4 + acc;
+}
+
+template <class R>
+__device__ __forceinline__ void weno9_edges(const R (&s)[9], R &qL, R &qR, bool do_map, bool imm_L, bool imm_R) {
+  using namespace pu_weno9;
+  R d[8];
+#pragma unroll
+  for (int m = 0; m < 8; m++) d[m] = s[m + 1] - s[m];
+  R tv[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    R y3 = d[k + 3];
+    R y2 = fma(R(TV_L[k][3][2]), d[k + 3], d[k + 2]);
+    R y1 = fma(R(TV_L[k][3][1]), d[k + 3], fma(R(TV_L[k][2][1]), d[k + 2], d[k + 1]));
+    R y0 = fma(R(TV_L[k][3][0]), d[k + 3], fma(R(TV_L[k][2][0]), d[k + 2], fma(R(TV_L[k][1][0]), d[k + 1], d[k])));
+    R t = R(TV_D[k][3]) * y3 * y3;
+    t = fma(R(TV_D[k][2]) * y2, y2, t);
+    t = fma(R(TV_D[k][1]) * y1, y1, t);
+    tv[k] = fma(R(TV_D[k][0]) * y0, y0, t);
+  }
+  convexify5(tv);
+  if (imm_L || imm_R) {
+    R mx = fmax(fmax(fmax(fmax(tv[0], tv[1]), tv[2]), tv[3]), tv[4]);
+    if (imm_L) tv[4] = mx;
+    if (imm_R) tv[0] = mx;
+  }
+  R rk[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) rk[k] = fast_rcp(fma(tv[k], tv[k], R(1.e-20)));
+  qL = weno9_edge<R, true>(d, s[4], rk, do_map);
+  qR = weno9_edge<R, false>(d, s[4], rk, do_map);
+}
+
+// Nine-cell linear edges (weno_all == false away from immersed cells,
+// dynamics_rk.h:539-545, 584-588).
+template <class R>
+__device__ __forceinline__ void linear9_edges(const R (&s)[9], R &qL, R &qR) {
+  using namespace pu_weno9;
+  R l = R(0), r = R(0);
+#pragma unroll
+  for (int m = 0; m < 8; m++) {
+    R dm = s[m + 1] - s[m];
+    l = fma(R(S2E_L[m]), dm, l);
+    r = fma(R(S2E_R[m]), dm, r);
+  }
+  qL = s[4] + l;
+  qR = s[4] + r;
+}
+
+// Zero-derivative extension past the first immersed cell, outward from the
+// centre, for a stencil whose centre is not immersed (dynamics_rk.h:478-493).
+// imm: bit m set when stencil entry m is immersed.
+template <class R>
+__device__ __forceinline__ void der0_modify(R (&s)[9], unsigned imm) {
+  if (imm & 0x10u) return;
+  bool hit = false;
+  R v = s[4];
+#pragma unroll
+  for (int i = 5; i < 9; i++) {
+    if (!hit && ((imm >> i) & 1u)) { hit = true; v = s[i - 1]; }
+    if (hit) s[i] = v;
+  }
+  hit = false;
+#pragma unroll
+  for (int i = 3; i >= 0; i--) {
+    if (!hit && ((imm >> i) & 1u)) { hit = true; v = s[i + 1]; }
+    if (hit) s[i] = v;
+  }
+}
+
+}  // namespace pu

@@ -158,6 +158,31 @@ def setup_dist():
     return world, rank, local
 
 
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def reduce_max(x, world, device="cuda"):
+    """Max of a per-rank scalar over all ranks (the timing rule: the job is as
+    slow as its slowest rank)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_value(cells_per_rank, steps, seconds_max, world):
+    """Whole-job throughput: every rank advanced its own replica of the
+    workload, so the job processed world*cells*steps cell-steps in the time of
+    the slowest rank."""
+    return world * cells_per_rank * steps / seconds_max
+
+
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
@@ -205,24 +230,13 @@ def main():
     N = case.ncells
     S = 5 + len(case.tracers)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # Warm-up, then the timed region.
     for _ in range(args.warmup):
         g.advance(dt, 1)
     g.synchronize()
     clocks = ClockSampler(local)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
+    barrier(world)
     torch.cuda.synchronize()
     clocks.start()
     time.sleep(0.3)
@@ -237,10 +251,10 @@ def main():
     prof = g.profile_read()
     g.profile(False)
     clk = clocks.stop()
-    barrier()
+    barrier(world)
     g.synchronize()
-    ms = max_over_ranks(ev0.elapsed_time(ev1))
-    value = world * N * args.steps / (ms / 1e3)
+    ms = reduce_max(ev0.elapsed_time(ev1), world)
+    value = aggregate_value(N, args.steps, ms / 1e3, world)
 
     # e2e through the C-ABI with pinned host coupler arrays.
     shp = (case.nz, case.ny, case.nx)
@@ -249,15 +263,15 @@ def main():
     g.store_state(*pinned, ptrc)
     dt_phys = DYN_CYCLE * dt
     g.time_step(*pinned, ptrc, dt_phys)   # warm-up call
-    barrier()
+    barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     ncyc = 0
     for _ in range(args.e2e_calls):
         ncyc += g.time_step(*pinned, ptrc, dt_phys)
     torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = world * N * ncyc / e2e_s
+    e2e_s = reduce_max(time.perf_counter() - t0, world)
+    e2e_value = aggregate_value(N, ncyc, e2e_s, world)
     bytes_io = (5 + len(case.tracers)) * N * 8
 
     if rank == 0:

@@ -98,13 +98,31 @@ struct Limiter9 {
     qR = weights_and_value(TV_1, TV_2, TV_3, TV_4, TV_5, do_map, s, false);
   }
   // Linear nine-cell edges for weno_all == false away from immersed cells
-  // (dynamics_rk.h:539-545, 584-588).  Coefficients are the exact rationals
-  // rounded to T; the reference forms them by a float matrix product.
+  // (dynamics_rk.h:539-545, 584-588): s2e = matmul_cr(c2e, s2c) formed in T
+  // from sten_to_coefs and the edge powers of coefs_to_gll_lower, then
+  // vals = matmul_cr(s2e, stencil), both as column-row products summed in
+  // ascending index order.
   static inline void linear(const T *s, T &qL, T &qR) {
     using namespace orc_tables;
-    T l = 0, r = 0;
-    for (int i = 0; i < 9; i++) { l += T(S2E_LEFT[i]) * s[i]; r += T(S2E_RIGHT[i]) * s[i]; }
-    qL = l; qR = r;
+    T s2e[9][2];
+    for (int st = 0; st < 9; st++)
+      for (int pt = 0; pt < 2; pt++) {
+        T tmp = 0;
+        T x = pt == 0 ? T(-0.5) : T(0.5), xp = 1;
+        for (int c = 0; c < 9; c++) {
+          tmp += xp * T(STEN_TO_COEFS9[st][c]);
+          xp *= x;
+        }
+        s2e[st][pt] = tmp;
+      }
+    T v[2];
+    for (int pt = 0; pt < 2; pt++) {
+      T tmp = 0;
+      for (int st = 0; st < 9; st++) tmp += s2e[st][pt] * s[st];
+      v[pt] = tmp;
+    }
+    qL = v[0];
+    qR = v[1];
   }
 };
 

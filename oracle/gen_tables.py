@@ -187,6 +187,12 @@ def main():
     w("// Nine-cell linear edge operator (weno_all == false path).\n")
     w("static const double S2E_LEFT[9] = {%s};\n" % ", ".join(lit(v) for v in P9L))
     w("static const double S2E_RIGHT[9] = {%s};\n" % ", ".join(lit(v) for v in P9R))
+    w("// sten_to_coefs for the nine-cell stencil, indexed (stencil entry, coefficient)\n")
+    w("// like TransformMatrices::sten_to_coefs(SArray<FP,2,9,9>).\n")
+    w("static const double STEN_TO_COEFS9[9][9] = {\n")
+    for j in range(9):
+        w("  {%s},\n" % ", ".join(lit(C9[dd][j]) for dd in range(9)))
+    w("};\n")
     w("\n}  // namespace orc_tables\n")
 
 

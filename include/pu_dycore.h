@@ -51,7 +51,9 @@ typedef enum {
 typedef enum { PU_BC_PERIODIC = 0, PU_BC_PRECURSOR = 1, PU_BC_WALL = 2 } pu_bc;
 typedef enum { PU_F32 = 0, PU_F64 = 1 } pu_precision;
 typedef enum { PU_WENO_PLAIN = 0, PU_WENO_LEARNED = 1 } pu_weno_mode;
-typedef enum { PU_MEM_HOST = 0, PU_MEM_DEVICE = 1 } pu_mem;
+/* Where coupler arrays live; PU_MEM_AUTO asks the library to inspect the
+ * pointers (cudaPointerGetAttributes). */
+typedef enum { PU_MEM_HOST = 0, PU_MEM_DEVICE = 1, PU_MEM_AUTO = 2 } pu_mem;
 
 /* Grid, tracer registry and the coupler options the dycore reads
  * (dynamics_rk.h:508-531, 747, 930-933, 1262-1266, 1315-1319; defaults from

@@ -128,8 +128,16 @@ struct ImplBase {
   }
 };
 
-ImplBase *make_impl_f32(int ntr);
-ImplBase *make_impl_f64(int ntr);
+// PU_MEM_AUTO: device (or managed) memory if CUDA knows the pointer as such.
+inline int resolve_mem(int mem, const void *p) {
+  if (mem != PU_MEM_AUTO) return mem;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return PU_MEM_HOST;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) ? PU_MEM_DEVICE : PU_MEM_HOST;
+}
 
 template <class R, int NTR>
 struct Impl : ImplBase {
@@ -270,7 +278,7 @@ struct Impl : ImplBase {
     for (int t = 0; t < NTR; t++)
       if (!v->tracers[t]) { set_error("coupler view has a null tracer array"); return PU_ERR_INVALID; }
     const double *d[5 + NTR];
-    if (v->mem == PU_MEM_DEVICE) {
+    if (resolve_mem(v->mem, v->rho_d) == PU_MEM_DEVICE) {
       for (int a = 0; a < 5; a++) d[a] = src[a];
       for (int t = 0; t < NTR; t++) d[5 + t] = v->tracers[t];
     } else {
@@ -303,7 +311,8 @@ struct Impl : ImplBase {
     if (prop) {
       double *dprop = nullptr;
       PU_TRY(dalloc(dprop, N));
-      if (mem == PU_MEM_DEVICE) PU_CK(cudaMemcpyAsync(dprop, prop, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      if (resolve_mem(mem, prop) == PU_MEM_DEVICE)
+        PU_CK(cudaMemcpyAsync(dprop, prop, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
       else PU_CK(cudaMemcpyAsync(dprop, prop, N * sizeof(double), cudaMemcpyHostToDevice, st));
       uint8_t *d0 = nullptr, *d1 = nullptr, *dz = nullptr;
       int rc = dalloc(d0, N);
@@ -377,16 +386,17 @@ struct Impl : ImplBase {
       if (!dst[a]) { set_error("coupler view has a null array"); return PU_ERR_INVALID; }
     for (int t = 0; t < NTR; t++)
       if (!v->tracers[t]) { set_error("coupler view has a null tracer array"); return PU_ERR_INVALID; }
+    const bool on_device = resolve_mem(v->mem, v->rho_d) == PU_MEM_DEVICE;
     for (int a = 0; a < 5 + NTR; a++) {
       double *h = a < 5 ? dst[a] : v->tracers[a - 5];
-      d[a] = v->mem == PU_MEM_DEVICE ? h : staging + size_t(a) * N;
+      d[a] = on_device ? h : staging + size_t(a) * N;
     }
     co.rho_d = d[0]; co.u = d[1]; co.v = d[2]; co.w = d[3]; co.T = d[4];
     for (int t = 0; t < 8; t++) co.tr[t] = t < NTR ? d[5 + t] : nullptr;
     k_store_coupler<R, NTR><<<blocks(N, 256), 256, 0, st>>>(co, thermo(), rho_off, rt_off, N, NP,
                                                             static_cast<const R *>(s[0]));
     PU_LAUNCHED();
-    if (v->mem != PU_MEM_DEVICE)
+    if (!on_device)
       for (int a = 0; a < 5 + NTR; a++) {
         double *h = a < 5 ? dst[a] : v->tracers[a - 5];
         PU_CK(cudaMemcpyAsync(h, staging + size_t(a) * N, N * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -445,7 +455,7 @@ struct Impl : ImplBase {
     k_get_conserved<R, NTR><<<blocks(N, 256), 256, 0, st>>>(static_cast<const R *>(s[0]), rho_off, rt_off, N, NP,
                                                             dst, dst + 5 * N);
     PU_LAUNCHED();
-    auto kind = mem == PU_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    auto kind = resolve_mem(mem, stp) == PU_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     PU_CK(cudaMemcpyAsync(stp, dst, 5 * N * sizeof(double), kind, st));
     if (trp) PU_CK(cudaMemcpyAsync(trp, dst + 5 * N, size_t(NTR) * N * sizeof(double), kind, st));
     PU_CK(cudaStreamSynchronize(st));
@@ -453,7 +463,7 @@ struct Impl : ImplBase {
   }
 
   int set_conserved(const double *stp, const double *trp, int mem) override {
-    auto kind = mem == PU_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    auto kind = resolve_mem(mem, stp) == PU_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     PU_CK(cudaMemcpyAsync(staging, stp, 5 * N * sizeof(double), kind, st));
     PU_CK(cudaMemcpyAsync(staging + 5 * N, trp, size_t(NTR) * N * sizeof(double), kind, st));
     k_set_conserved<R, NTR><<<blocks(N, 256), 256, 0, st>>>(static_cast<R *>(s[0]), rho_off, rt_off, N, NP, staging,

@@ -1,0 +1,23 @@
+"""Builds tests/cpp/_build/dropin_driver: the C++ drop-in module driven like
+the reference's example drivers, on the stand-in coupler of oracle/ref_shim
+(which includes the reference's MultipleFields.h, so the build needs the
+reference tree; the GPU box uses the binary built here)."""
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+EXE = os.path.join(HERE, "_build", "dropin_driver")
+REF_CORE = "/root/reference/model/core"
+
+
+def build(libdir):
+    if not os.path.isdir(REF_CORE):
+        return EXE if os.path.exists(EXE) else None
+    os.makedirs(os.path.dirname(EXE), exist_ok=True)
+    cmd = ["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "porturb_b200", "cpp"),
+           "-I", os.path.join(ROOT, "oracle", "ref_shim"), "-I", os.path.join(ROOT, "include"), "-I", REF_CORE,
+           os.path.join(HERE, "dropin_driver.cpp"), "-o", EXE,
+           "-L", libdir, "-lpu_dycore", "-Wl,-rpath," + libdir]
+    subprocess.run(cmd, check=True)
+    return EXE

@@ -1,0 +1,64 @@
+"""The C++ drop-in module (porturb_b200/cpp/dynamics_rk.h) used the way the
+reference's drivers use Dynamics_Euler_Stratified_WenoFV.  The build runs on
+CPU; the run needs a GPU and must reproduce the Python front end's results."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "tests", "cpp", "_build", "dropin_driver")
+
+
+def build_driver():
+    from porturb_b200 import build
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("build_driver", os.path.join(ROOT, "tests", "cpp", "build_driver.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    exe = mod.build(os.path.dirname(build.build()))
+    if exe is None:
+        pytest.skip("no reference tree to build the stand-in coupler and no prebuilt driver")
+    return exe
+
+
+def test_dropin_builds_and_links():
+    assert os.path.exists(build_driver())
+
+
+def _write_input(path, case, ncalls, dt_phys):
+    o = case.options
+    rd, u, v, w, T, trc = case.coupler_arrays(perturbed=False)
+    prd, pu_, pv, pw, pT, ptr = case.coupler_arrays(perturbed=True)
+    ntr = len(case.tracers)
+    with open(path, "wb") as f:
+        np.array([case.nx, case.ny, case.nz, ntr, ncalls], np.int32).tofile(f)
+        np.array([case.xlen, case.ylen, case.zlen, dt_phys, o["R_d"], o["R_v"], o["cp_d"], o["gamma_d"], o["C0"],
+                  o["grav"], o["cfl"]], np.float64).tofile(f)
+        np.array([[t.name for t in case.tracers].index("water_vapor")], np.int32).tofile(f)
+        np.array([t.positive for t in case.tracers], np.int32).tofile(f)
+        np.array([t.adds_mass for t in case.tracers], np.int32).tofile(f)
+        np.concatenate([np.stack([rd, u, v, w, T]).ravel(), trc.ravel()]).tofile(f)
+        np.concatenate([np.stack([prd, pu_, pv, pw, pT]).ravel(), ptr.ravel()]).tofile(f)
+
+
+@pytest.mark.gpu
+def test_dropin_matches_python_front_end(tmp_path):
+    from porturb_b200 import Dycore, cases
+    exe = build_driver()
+    case = cases.small_mixed(immersed=False)
+    g = Dycore.from_case(case, precision="f32")
+    dt_phys = 2.5 * g.compute_time_step()
+    _write_input(tmp_path / "in.bin", case, 2, dt_phys)
+    r = subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = np.fromfile(tmp_path / "out.bin", np.float64).reshape(5 + len(case.tracers), case.nz, case.ny, case.nx)
+    rd, u, v, w, T, trc = [np.ascontiguousarray(a) for a in case.coupler_arrays(perturbed=False)]
+    g.init(rd, u, v, w, T, list(trc), None)
+    arrs = [np.ascontiguousarray(a.copy()) for a in case.coupler_arrays(perturbed=True)]
+    trs = [np.ascontiguousarray(a) for a in arrs[5]]
+    for _ in range(2):
+        g.time_step(*arrs[:5], trs, dt_phys)
+    ref = np.concatenate([np.stack(arrs[:5]), np.stack(trs)])
+    assert np.array_equal(out, ref)

@@ -184,6 +184,37 @@ typedef struct pu_profile {
 int pu_dycore_profile(pu_dycore *h, int enable);
 int pu_dycore_profile_read(pu_dycore *h, pu_profile *out);
 
+/* A time step that allocates no device memory.
+ *
+ * No counterpart in the reference.  It is for callers that cannot call
+ * cudaMalloc: a host model whose own allocator has already reserved the GPU's
+ * memory, or a plug-in that runs inside a time loop where device allocation is
+ * not allowed.  pu_dycore_create allocates its buffers, so such callers use this
+ * entry point instead: it performs what pu_dycore_time_step does (convert the
+ * coupler state in, ncycles = ceil(dt_phys/dt_dyn) SSPRK3 steps, convert back
+ * into the same arrays) for an FP32 dycore without immersed cells, given the
+ * configuration and the hydrostatic cell profiles (hy_dens_cells,
+ * hy_theta_cells, hy_pressure_cells: nz+2*PU_HS host doubles each, e.g. from
+ * pu_dycore_get_hydrostasis of an earlier init, or a restart file).
+ *   - coupler arrays must be device memory (PU_MEM_DEVICE, or PU_MEM_AUTO
+ *     resolving to device); there is no staging;
+ *   - all working memory comes from one static device array of
+ *     PU_NOALLOC_SCRATCH_BYTES bytes, which every GPU that loads the library
+ *     holds until the process exits; grids that need more return
+ *     PU_ERR_UNSUPPORTED (about 110 bytes per cell with two tracers, i.e. up
+ *     to roughly 600k cells);
+ *   - the first call on a device looks up that array's device address
+ *     (cudaGetSymbolAddress, with the device current); make that first call
+ *     before any stream capture;
+ *   - every call shares the one array and it keeps the previous call's
+ *     contents (only the error word is cleared per call), so calls whose GPU
+ *     work overlaps -- on different streams or host threads -- race;
+ *   - synchronous; returns PU_ERR_NONFINITE like pu_dycore_time_step. */
+#define PU_NOALLOC_SCRATCH_BYTES (64u << 20)
+int pu_dycore_time_step_noalloc(const pu_config *cfg, const double *hy_dens_cells, const double *hy_theta_cells,
+                                const double *hy_pressure_cells, pu_state_view *coupler, double dt_phys,
+                                int *ncycles);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,9 +65,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False
         cmd = [nvcc()] + NVFLAGS + extra + ["-DPU_REAL=%s" % real, "-DPU_NTR=%d" % ntr, "-DPU_TAG=%s" % tag,
                                             "-c", os.path.join(CSRC, "impl_inst.cu"), "-o", obj]
         jobs.append((obj, cmd))
-    jobs.append((os.path.join(OBJDIR, "pu_dycore.o"),
-                 [nvcc()] + NVFLAGS + extra + ["-c", os.path.join(CSRC, "pu_dycore.cu"), "-o",
-                                               os.path.join(OBJDIR, "pu_dycore.o")]))
+    for src in ("pu_dycore", "pu_noalloc"):
+        jobs.append((os.path.join(OBJDIR, src + ".o"),
+                     [nvcc()] + NVFLAGS + extra + ["-c", os.path.join(CSRC, src + ".cu"), "-o",
+                                                   os.path.join(OBJDIR, src + ".o")]))
     with cf.ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
         outs = list(ex.map(lambda j: _run(j[1]), jobs))
     if verbose:

@@ -89,7 +89,10 @@ SIGNATURES = {
     "pu_dycore_kernel_launches": (C.c_longlong, [_P]),
     "pu_dycore_profile": (_I, [_P, _I]),
     "pu_dycore_profile_read": (_I, [_P, C.POINTER(pu_profile)]),
+    "pu_dycore_time_step_noalloc": (_I, [C.POINTER(pu_config), _P, _P, _P, C.POINTER(pu_state_view), _D,
+                                         C.POINTER(_I)]),
 }
+PU_NOALLOC_SCRATCH_BYTES = 64 << 20
 
 _lib = None
 

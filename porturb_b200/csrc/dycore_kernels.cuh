@@ -647,6 +647,8 @@ __global__ void k_hydro_finish(const double *__restrict__ sums, int nz, double r
   const int nzh = nz + 2 * HS;
   double *r = out.cells, *t = out.cells + nzh, *p = out.cells + 2 * nzh;
   auto rnd = [&](double x) { return round32 ? double(float(x)) : x; };
+  if (!sums && round32)
+    for (int k = 0; k < 3 * nzh; k++) out.cells[k] = rnd(out.cells[k]);
   if (sums) {
     for (int k = 0; k < nz; k++) {
       r[HS + k] = rnd(sums[k] * r_nx_ny);

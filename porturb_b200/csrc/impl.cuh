@@ -42,6 +42,7 @@ struct ImplBase {
   int ntr = 0, S = 0, F = 0, nzh = 0;
   size_t N = 0, NP = 0;
   bool inited = false, has_imm = false;
+  bool owns = true;                           // false: buffers point into caller-provided scratch
   long long launches = 0;
   // Device buffers.
   void *s[3] = {nullptr, nullptr, nullptr};   // state, two stage buffers
@@ -148,6 +149,7 @@ struct Impl : ImplBase {
   bool small_tile = false;
 
   ~Impl() override {
+    if (!owns) return;
     for (auto p : {s[0], s[1], s[2], txy, (void *)staging, (void *)cells, (void *)edges, (void *)rho_off,
                    (void *)rt_off, tabs, (void *)flags, imm_mult, (void *)err, (void *)sums, (void *)diag_part,
                    (void *)diag_out})
@@ -205,6 +207,11 @@ struct Impl : ImplBase {
     diag_blocks = 296;
     PU_TRY(dalloc(diag_part, size_t(diag_blocks) * NDIAG * 2));
     PU_TRY(dalloc(diag_out, size_t(NDIAG)));
+    return configure();
+  }
+
+  // Kernel attributes (no allocation).
+  int configure() {
     small_tile = cfg.ny < 16;
     PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_BIG, XTY_BIG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(XYShape<R, NTR, XTX_BIG, XTY_BIG, false>::bytes)));
@@ -521,6 +528,80 @@ struct Impl : ImplBase {
     out->total_energy = h[5];
     for (int t = 0; t < PU_MAX_TRACERS; t++) out->tracer_mass[t] = t < NTR ? h[6 + t] : 0.0;
     return PU_OK;
+  }
+
+  // Bytes of working memory a time step needs when every buffer is carved
+  // out of one caller-provided region (each piece 256-byte aligned).
+  static size_t scratch_bytes(const pu_config &c) {
+    const size_t N = size_t(c.nx) * c.ny * c.nz, nzh = size_t(c.nz) + 2 * HS;
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    return al(sizeof(int)) + al(3 * nzh * sizeof(double)) + al(3 * size_t(c.nz + 1) * sizeof(double)) +
+           2 * al(size_t(c.nz) * sizeof(double)) +
+           al((5 * nzh + 2 * size_t(c.nz + 1) + size_t(c.nz)) * sizeof(R)) + 4 * al(size_t(5 + NTR) * N * sizeof(R));
+  }
+
+  // time_step (dynamics_rk.h:103-137) on a device-resident coupler view with
+  // the caller's hydrostatic cell profiles, every buffer taken from `scratch`
+  // (no allocation).  The handle object lives on the stack and does not own
+  // the buffers.
+  static int noalloc_time_step(const pu_config &c, unsigned char *scratch, const double *dens_cells,
+                               const double *theta_cells, const double *pressure_cells, pu_state_view *v,
+                               double dt_phys, int *ncycles) {
+    Impl im;
+    im.owns = false;
+    im.cfg = c;
+    im.st = static_cast<cudaStream_t>(c.stream);
+    im.ntr = NTR;
+    im.F = 6 + NTR;
+    im.S = 5 + NTR;
+    im.N = size_t(c.nx) * c.ny * c.nz;
+    im.NP = size_t(c.nx) * c.ny;
+    im.nzh = c.nz + 2 * HS;
+    unsigned char *p = scratch;
+    auto take = [&](size_t b) {
+      unsigned char *q = p;
+      p += (b + 255) / 256 * 256;
+      return q;
+    };
+    im.err = reinterpret_cast<int *>(take(sizeof(int)));
+    im.cells = reinterpret_cast<double *>(take(3 * size_t(im.nzh) * sizeof(double)));
+    im.edges = reinterpret_cast<double *>(take(3 * size_t(c.nz + 1) * sizeof(double)));
+    im.rho_off = reinterpret_cast<double *>(take(size_t(c.nz) * sizeof(double)));
+    im.rt_off = reinterpret_cast<double *>(take(size_t(c.nz) * sizeof(double)));
+    R *tb = reinterpret_cast<R *>(take((5 * size_t(im.nzh) + 2 * size_t(c.nz + 1) + size_t(c.nz)) * sizeof(R)));
+    im.lt.rho_h = tb;
+    im.lt.theta_h = tb + im.nzh;
+    im.lt.rt_inv = tb + 2 * im.nzh;
+    im.lt.p0_h = tb + 3 * im.nzh;
+    im.lt.dp_h = tb + 4 * im.nzh;
+    im.lt.rho_e = tb + 5 * im.nzh;
+    im.lt.theta_e = im.lt.rho_e + (c.nz + 1);
+    im.lt.rt_target = im.lt.theta_e + (c.nz + 1);
+    for (int b = 0; b < 3; b++) im.s[b] = take(size_t(im.S) * im.N * sizeof(R));
+    im.txy = take(size_t(im.S) * im.N * sizeof(R));
+    int rc = im.configure();
+    if (rc) return rc;
+    // The array keeps the previous call's contents: the error word must start at zero.
+    PU_CK(cudaMemsetAsync(im.err, 0, sizeof(int), im.st));
+    const size_t nzh = im.nzh;
+    PU_CK(cudaMemcpyAsync(im.cells, dens_cells, nzh * sizeof(double), cudaMemcpyHostToDevice, im.st));
+    PU_CK(cudaMemcpyAsync(im.cells + nzh, theta_cells, nzh * sizeof(double), cudaMemcpyHostToDevice, im.st));
+    PU_CK(cudaMemcpyAsync(im.cells + 2 * nzh, pressure_cells, nzh * sizeof(double), cudaMemcpyHostToDevice, im.st));
+    HydroOut ho{im.cells, im.edges, im.rho_off, im.rt_off};
+    k_hydro_finish<R><<<1, 1, 0, im.st>>>(nullptr, c.nz, 0., c.gamma_d, c.C0, c.grav, c.dz, sizeof(R) == 4, ho, im.lt);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      set_error(std::string("kernel launch: ") + cudaGetErrorString(e));
+      return PU_ERR_CUDA;
+    }
+    im.inited = true;
+    const double dt0 = c.cfl * std::fmin(std::fmin(c.dx, c.dy), c.dz) / (350. + 100.);
+    const int n = (int)std::ceil(dt_phys / dt0);
+    rc = im.load_state(v);
+    if (!rc) rc = im.advance(dt_phys / n, n);
+    if (!rc) rc = im.store_state(v);
+    if (ncycles) *ncycles = n;
+    return rc;
   }
 #undef PU_TRY
 };

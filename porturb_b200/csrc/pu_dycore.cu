@@ -68,6 +68,9 @@ struct DeviceGuard {
   }
 };
 
+}  // namespace
+
+namespace pu {
 int check_config(const pu_config *c) {
   if (!c) return fail(PU_ERR_INVALID, "null config");
   if (c->nx < 1 || c->ny < 1 || c->nz < 1) return fail(PU_ERR_INVALID, "grid dimensions must be positive");
@@ -88,7 +91,10 @@ int check_config(const pu_config *c) {
   if (c->z_chunk < 0) return fail(PU_ERR_INVALID, "z_chunk must be >= 0");
   return PU_OK;
 }
+}  // namespace pu
 
+namespace {
+using pu::check_config;
 }  // namespace
 
 extern "C" {

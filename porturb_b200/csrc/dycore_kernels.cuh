@@ -307,40 +307,70 @@ __device__ __forceinline__ void enforce_cell(const Grid<R> &G, R (&q)[5 + NTR], 
 template <class R, int NTR, int TX, int TY>
 struct ZShape {
   static constexpr int F = 6 + NTR, NT = TX * TY;
-  static constexpr size_t bytes = sizeof(R) * 9 * size_t(F) * NT;
+  // 9-plane ring of primitive fields, left edges of the current cell, right
+  // edges of the current and the previous cell; all thread-private columns.
+  static constexpr size_t bytes = sizeof(R) * (9 + 3) * size_t(F) * NT;
 };
+
+// Raw state of one cell (S values) for a later conversion to primitive fields.
+template <class R, int NTR>
+__device__ __forceinline__ void load_cell(const Grid<R> &G, const R *__restrict__ s, size_t idx, R (&q)[5 + NTR]) {
+#pragma unroll
+  for (int v = 0; v < 5 + NTR; v++) q[v] = __ldg(s + v * G.N + idx);
+}
+
+template <class R, int NTR>
+__device__ __forceinline__ void prims_of(const Grid<R> &G, const R (&q)[5 + NTR], int k, R (&w)[6 + NTR]) {
+  const int kh = k + HS;
+  R rho = __ldg(G.rho_h + kh) + q[0];
+  R rr = R(1) / rho;
+  w[0] = q[0];
+  w[1] = q[1] * rr;
+  w[2] = q[2] * rr;
+  w[3] = q[3] * rr;
+  w[4] = (q[4] - __ldg(G.theta_h + kh) * q[0]) * rr;
+  w[5] = fma(__ldg(G.p0_h + kh), pu_expm1(G.gamma * pu_log1p(q[4] * __ldg(G.rt_inv + kh))), __ldg(G.dp_h + kh));
+#pragma unroll
+  for (int t = 0; t < NTR; t++) w[6 + t] = q[5 + t] * rr;
+}
 
 // z fluxes, their divergence, sources and the SSPRK3 stage combination:
 //   out = a_n*sn + a_in*sin + a_dt*(txy - dFz/dz + sources)   (sn may be null)
 // followed by n_enforce applications of the immersed/positivity enforcement.
+// One thread per column marches up levels k0..k1-1 of its chunk.  The raw
+// state of the plane entering the ring is loaded one step ahead, and the
+// inputs of the cell being finalised are loaded before the reconstruction, so
+// global-load latency overlaps the limiter work.  The field loop is not
+// unrolled: one inlined limiter keeps the kernel small.
 template <class R, int NTR, int TX, int TY, bool IMM>
-__global__ void __launch_bounds__(TX *TY) k_z(const Grid<R> G, const R *__restrict__ sin, const R *__restrict__ sn,
-                                              R *__restrict__ sout, const R *__restrict__ txy, R a_n, R a_in, R a_dt,
-                                              int n_enforce, int kchunk) {
+__global__ void __launch_bounds__(TX *TY) k_z(const Grid<R> G, const R *__restrict__ sin, const R *sn, R *sout,
+                                              const R *__restrict__ txy, R a_n, R a_in, R a_dt, int n_enforce,
+                                              int kchunk) {
   constexpr int F = 6 + NTR, S = 5 + NTR, NT = TX * TY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *ring = reinterpret_cast<R *>(smem_raw);   // [9][F][NT], thread-private columns
+  R *ring = reinterpret_cast<R *>(smem_raw);   // [9][F][NT]
+  R *eL = ring + 9 * F * NT;                     // [F][NT]
+  R *eR = eL + F * NT;                           // [2][F][NT]
   const int tid = threadIdx.x;
   const int i = blockIdx.x * TX + tid % TX, j = blockIdx.y * TY + tid / TX;
-  if (i >= G.nx || j >= G.ny) return;          // no block-wide synchronisation below
+  if (i >= G.nx || j >= G.ny) return;            // no block-wide synchronisation below
   const int nz = G.nz;
   const int k0 = blockIdx.z * kchunk, k1 = min(nz, k0 + kchunk);
   const bool wall = G.bc_z == BC_WALL;
   const size_t col = size_t(j) * G.nx + i, NP = G.NP;
 
-  auto slot_ptr = [&](int p) { return ring + ((p % 9 + 9) % 9) * F * NT + tid; };
-  // Plane p of the column (p may lie in the halos): wall halos replicate the
-  // boundary cell with w' = theta' = 0; periodic halos wrap (:780-797).
-  auto load_plane = [&](int p) {
-    const bool out = p < 0 || p >= nz;
-    const int pc = !out ? p : (wall ? clampi(p, nz) : wrapi(p, nz));
+  auto slot_of = [](int p) { return (p % 9 + 9) % 9; };
+  // Level whose state feeds plane p (wall halos replicate the boundary cell,
+  // periodic halos wrap; :780-797).
+  auto src_level = [&](int p) { return (p >= 0 && p < nz) ? p : (wall ? clampi(p, nz) : wrapi(p, nz)); };
+  auto store_plane = [&](int p, const R (&q)[S]) {
     R w[F];
-    prims<R, NTR>(G, sin, size_t(pc) * NP + col, pc, w);
-    if (out && wall) {
+    prims_of<R, NTR>(G, q, src_level(p), w);
+    if (wall && (p < 0 || p >= nz)) {
       w[iW] = R(0);
       w[iT] = R(0);
     }
-    R *dst = slot_ptr(p);
+    R *dst = ring + slot_of(p) * F * NT + tid;
 #pragma unroll
     for (int f = 0; f < F; f++) dst[f * NT] = w[f];
   };
@@ -358,65 +388,84 @@ __global__ void __launch_bounds__(TX *TY) k_z(const Grid<R> G, const R *__restri
   };
 
   const int cstart = (wall && k0 == 0) ? 0 : k0 - 1;
-  for (int p = cstart - 4; p <= cstart + 3; p++) load_plane(p);
+  {
+    R q[S];
+    for (int p = cstart - 4; p <= cstart + 3; p++) {
+      load_cell<R, NTR>(G, sin, size_t(src_level(p)) * NP + col, q);
+      store_plane(p, q);
+    }
+  }
+  R qnext[S];   // raw state of plane c+4, loaded one step ahead
+  load_cell<R, NTR>(G, sin, size_t(src_level(cstart + 4)) * NP + col, qnext);
 
-  R ERp[F], Fp[S];
-#pragma unroll
-  for (int f = 0; f < F; f++) ERp[f] = R(0);
+  R Fp[S];
 #pragma unroll
   for (int s = 0; s < S; s++) Fp[s] = R(0);
+  int par = 0;   // eR double-buffer index of the current cell
 
   for (int c = cstart; c <= k1; c++) {
-    load_plane(c + 4);
-    R EL[F], ER[F];
+    store_plane(c + 4, qnext);
+    if (c < k1) load_cell<R, NTR>(G, sin, size_t(src_level(c + 5)) * NP + col, qnext);
+    // Inputs of cell c-1 (finalised below), loaded before the reconstruction.
+    const bool fin = c > cstart && c - 1 >= k0;
+    R qin[S], qn[S], tx[S];
+    if (fin) {
+      const size_t idx = size_t(c - 1) * NP + col;
+#pragma unroll
+      for (int s = 0; s < S; s++) {
+        qin[s] = sin[s * G.N + idx];
+        tx[s] = txy[s * G.N + idx];
+        qn[s] = sn ? sn[s * G.N + idx] : R(0);
+      }
+    }
     const bool have_cell = !(wall && c >= nz);
+    R *eRc = eR + par * F * NT + tid, *eRp = eR + (par ^ 1) * F * NT + tid;
     if (have_cell) {
       const int cc = wall ? c : wrapi(c, nz);
       const unsigned imm = stencil_flags(cc);
       const bool any10 = IMM && (__ldg(G.flags + size_t(cc) * NP + col) & FLAG_ANY10);
+      int sl[9];
 #pragma unroll
+      for (int m = 0; m < 9; m++) sl[m] = slot_of(c - 4 + m) * F * NT + tid;
+#pragma unroll 1
       for (int f = 0; f < F; f++) {
         R s[9];
 #pragma unroll
-        for (int m = 0; m < 9; m++) s[m] = slot_ptr(c - 4 + m)[f * NT];
+        for (int m = 0; m < 9; m++) s[m] = ring[sl[m] + f * NT];
         if (f == iU || f == iV || f == iP) der0_modify(s, imm);
-        if (!any10 && !G.weno_all) linear9_edges(s, EL[f], ER[f]);
-        else weno9_edges(s, EL[f], ER[f], !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
+        R qL, qR;
+        if (!any10 && !G.weno_all) linear9_edges(s, qL, qR);
+        else weno9_edges(s, qL, qR, !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
+        eL[f * NT + tid] = qL;
+        eRc[f * NT] = qR;
       }
-    } else {
-#pragma unroll
-      for (int f = 0; f < F; f++) EL[f] = ER[f] = R(0);
     }
     if (c > cstart || (wall && c == 0)) {
       // Face c between cells c-1 and c (edge_exchange z, :891-908).
       R Lf[F], Rf[F];
       if (wall && c == 0) {
 #pragma unroll
-        for (int f = 0; f < F; f++) Lf[f] = Rf[f] = EL[f];
+        for (int f = 0; f < F; f++) Lf[f] = Rf[f] = eL[f * NT + tid];
         Lf[iW] = Rf[iW] = Lf[iT] = Rf[iT] = R(0);
       } else if (wall && c == nz) {
 #pragma unroll
-        for (int f = 0; f < F; f++) Lf[f] = Rf[f] = ERp[f];
+        for (int f = 0; f < F; f++) Lf[f] = Rf[f] = eRp[f * NT];
         Lf[iW] = Rf[iW] = Lf[iT] = Rf[iT] = R(0);
       } else {
 #pragma unroll
         for (int f = 0; f < F; f++) {
-          Lf[f] = ERp[f];
-          Rf[f] = EL[f];
+          Lf[f] = eRp[f * NT];
+          Rf[f] = eL[f * NT + tid];
         }
       }
       R Fc[S];
       riemann<R, NTR>(Lf, Rf, __ldg(G.rho_e + c), __ldg(G.theta_e + c), iW, Fc);
-      if (c - 1 >= k0) {
-        // Finalise cell c-1.
+      if (fin) {
         const int k = c - 1;
         const size_t idx = size_t(k) * NP + col;
-        R qin[S], out[S];
+        R tend[S], out[S];
 #pragma unroll
-        for (int s = 0; s < S; s++) qin[s] = sin[s * G.N + idx];
-        R tend[S];
-#pragma unroll
-        for (int s = 0; s < S; s++) tend[s] = txy[s * G.N + idx] - (Fc[s] - Fp[s]) * G.rdz;
+        for (int s = 0; s < S; s++) tend[s] = tx[s] - (Fc[s] - Fp[s]) * G.rdz;
         if (G.sim2d) tend[iV] = R(0);
         if (G.enable_gravity) tend[iW] += -G.grav * qin[iR];
         if (G.fcor != R(0) && !G.sim2d) {
@@ -425,7 +474,7 @@ __global__ void __launch_bounds__(TX *TY) k_z(const Grid<R> G, const R *__restri
         }
         if (sn) {
 #pragma unroll
-          for (int s = 0; s < S; s++) out[s] = a_n * sn[s * G.N + idx] + a_in * qin[s] + a_dt * tend[s];
+          for (int s = 0; s < S; s++) out[s] = a_n * qn[s] + a_in * qin[s] + a_dt * tend[s];
         } else {
 #pragma unroll
           for (int s = 0; s < S; s++) out[s] = qin[s] + a_dt * tend[s];
@@ -442,8 +491,7 @@ __global__ void __launch_bounds__(TX *TY) k_z(const Grid<R> G, const R *__restri
 #pragma unroll
       for (int s = 0; s < S; s++) Fp[s] = Fc[s];
     }
-#pragma unroll
-    for (int f = 0; f < F; f++) ERp[f] = ER[f];
+    par ^= 1;
   }
 }
 

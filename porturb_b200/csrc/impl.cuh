@@ -426,7 +426,7 @@ struct Impl : ImplBase {
     }
     PU_LAUNCHED();
     prof_end(0, e0);
-    const int kc = cfg.z_chunk > 0 ? cfg.z_chunk : (cfg.nz < 32 ? cfg.nz : 32);
+    const int kc = cfg.z_chunk > 0 ? cfg.z_chunk : (cfg.nz < 16 ? cfg.nz : 16);
     dim3 gz(blocks(cfg.nx, ZTX), blocks(cfg.ny, ZTY), blocks(cfg.nz, kc));
     cudaEvent_t e1 = prof_begin();
     k_z<R, NTR, ZTX, ZTY, IMM><<<gz, ZTX * ZTY, ZShape<R, NTR, ZTX, ZTY>::bytes, st>>>(G, sin, sn, sout, t, a_n, a_in,

@@ -18,6 +18,9 @@ tracers water_vapor + TKE), one JSON line on rank 0.
 * cpu_baseline: the reference's own dycore code (oracle/_ref, built from the
   reference's headers with a single-rank shim) on all host cores, on a
   bounded sample of the same workload.
+* learned: the learned-weight form on the same state and timed region,
+  after harvesting 2^21 stencils from it and training the network on the GPU
+  (3000 Adam steps, batch 16384); kernel times and the fallback fraction.
 * Multi-GPU: the dycore is not domain-decomposed here; N ranks run N
   independent replicas (ensemble members) with no collective in the data
   path (weak scaling).
@@ -41,6 +44,7 @@ sys.path.insert(0, ROOT)
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
 WORKLOAD = dict(nx=256, ny=256, nz=128, dx=10.0)
 DYN_CYCLE = 10
+LEARNED_THRESHOLD = 0.5
 
 
 def measured_peaks():
@@ -205,6 +209,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-calls", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()
     world, rank, local = setup_dist()
     if args.impl == "reference":
@@ -274,6 +279,40 @@ def main():
     e2e_value = aggregate_value(N, ncyc, e2e_s, world)
     bytes_io = (5 + len(case.tracers)) * N * 8
 
+    # Learned-weight form: network trained on stencils harvested from this
+    # run's own state (GPU training kernels), then the same timed region.
+    learned = None
+    if not args.no_learned:
+        g.learned_harvest(1 << 21, seed=1 + rank)
+        tstats = g.learned_train(3000, batch=16384, lr=2e-3, seed=3)
+        g.set_weno_mode("learned")
+        g.learned_set_threshold(LEARNED_THRESHOLD)
+        g.advance(dt, 1)
+        g.learned_counts()
+        barrier(world)
+        torch.cuda.synchronize()
+        g.profile(True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            g.advance(dt, 1)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        lprof = g.profile_read()
+        g.profile(False)
+        barrier(world)
+        g.synchronize()
+        nl, nf = g.learned_counts()
+        g.set_weno_mode("plain")
+        ms_l = reduce_max(ev0.elapsed_time(ev1), world)
+        learned = {"value": aggregate_value(N, args.steps, ms_l / 1e3, world), "unit": "cell-steps/s",
+                   "ms_per_step": ms_l / args.steps, "dtype": "f32 stencils, bf16 network (fp32 accumulate)",
+                   "threshold": LEARNED_THRESHOLD, "fallback_frac": nf / max(1, nl + nf),
+                   "kernel_ms": {"k_xy": lprof["xy"][0] / max(lprof["xy"][1], 1),
+                                 "k_z": lprof["z"][0] / max(lprof["z"][1], 1)},
+                   "training": {"samples": tstats["samples"], "steps": tstats["steps"], "batch": 16384,
+                                "loss_first": tstats["loss_first"], "loss_last": tstats["loss_last"],
+                                "ms": tstats["ms"]}}
+
     if rank == 0:
         peaks = measured_peaks()
         hbm_peak = peaks.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
@@ -316,6 +355,7 @@ def main():
                     "d2h_bytes_per_step": bytes_io, "calls": args.e2e_calls, "dycore_steps_per_call": ncyc // max(1, args.e2e_calls)},
             "gpu_launches": launches,
             "clocks": clk,
+            "learned": learned,
         }
         print(json.dumps(line), flush=True)
     g.close()

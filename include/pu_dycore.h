@@ -171,6 +171,55 @@ int pu_dycore_synchronize(pu_dycore *h);
  * accounting in benchmarks). */
 long long pu_dycore_kernel_launches(const pu_dycore *h);
 
+/* ---- Learned WENO weights -------------------------------------------------
+ * No counterpart in the reference: a network (9 -> 32 -> 32 -> 5, ReLU,
+ * softmax; bfloat16 weights and activations, FP32 biases and accumulation)
+ * that maps a stencil normalised to its local range (the convention of
+ * dynamics_rk.h:42-53) to the nonlinear weights of the left edge
+ * (WenoLimiter.h:382-403); the right edge uses the mirrored stencil.  It is
+ * trained on stencils harvested from the handle's resident state with the
+ * plain limiter's weights as targets.  Parameter vector (PU_MLP_PARAMS floats):
+ * W1 (32x9, row major), b1 (32), W2 (32x32), b2 (32), W3 (5x32), b3 (5). */
+#define PU_MLP_PARAMS 1541
+typedef struct pu_learn_stats {
+  double loss_first, loss_last; /* mean cross-entropy of the first and last batch */
+  long long steps, samples;     /* optimiser steps, harvested stencils */
+  double ms;                    /* GPU time of the training loop */
+} pu_learn_stats;
+
+/* Appends n stencils of the resident state (random field, direction and cell,
+ * away from immersed cells and z walls) with their plain left-edge weights to
+ * the training set.  Synchronous. */
+int pu_dycore_learned_harvest(pu_dycore *h, long long n, unsigned long long seed);
+/* Adam steps on random batches of the training set (hand-written forward,
+ * backward and Adam kernels), then installs the weights for inference. */
+int pu_dycore_learned_train(pu_dycore *h, int steps, int batch, double lr, unsigned long long seed,
+                            pu_learn_stats *out);
+int pu_dycore_learned_get_weights(pu_dycore *h, float *theta);
+int pu_dycore_learned_set_weights(pu_dycore *h, const float *theta);
+/* Network weights of n normalised stencils (host arrays n*9 -> n*5).  With
+ * use_mma the tensor-core path also returns the right-edge weights (wr). */
+int pu_dycore_learned_eval(pu_dycore *h, const float *x, long long n, float *wl, float *wr, int use_mma);
+/* Mean cross-entropy and its gradient over the n given samples (host arrays):
+ * the training kernels' forward and backward pass, for checking. */
+int pu_dycore_learned_gradient(pu_dycore *h, const float *x, const float *t, long long n, float *grad,
+                               double *loss);
+/* Selects PU_WENO_PLAIN or PU_WENO_LEARNED for the following steps.  Learned
+ * needs trained or loaded weights, the FP32 build and weno_all (it replaces
+ * the nonlinear limiter, which otherwise runs only near immersed cells):
+ * PU_ERR_STATE / PU_ERR_UNSUPPORTED otherwise.  In learned mode the stencil
+ * kernels evaluate the network with tensor-core MMAs inside the
+ * reconstruction; stencils with an immersed cell or a z wall within reach,
+ * or with a normalised neighbour jump above the threshold, use the plain
+ * limiter. */
+int pu_dycore_set_weno_mode(pu_dycore *h, int mode);
+/* Largest normalised neighbour jump |x[m+1]-x[m]| (of the stencil scaled to
+ * [0,1]) given learned weights; default 0.5; values >= 1 disable the check. */
+int pu_dycore_learned_set_threshold(pu_dycore *h, double max_jump);
+/* Stencils reconstructed with learned weights and stencils that fell back to
+ * the plain limiter since the last call (counters are reset). */
+int pu_dycore_learned_counts(pu_dycore *h, long long *learned, long long *fallback);
+
 /* Per-kernel timing with CUDA events recorded on the handle's stream around
  * every stencil-kernel launch while enabled (no counterpart in the reference,
  * whose timers are YAKL's, dynamics_rk.h:104-106).  Kinds: 0 = x/y flux

@@ -58,6 +58,14 @@ class pu_diag(C.Structure):
                 ("tracer_mass", C.c_double * PU_MAX_TRACERS)]
 
 
+PU_MLP_PARAMS = 1541
+
+
+class pu_learn_stats(C.Structure):
+    _fields_ = [("loss_first", C.c_double), ("loss_last", C.c_double), ("steps", C.c_longlong),
+                ("samples", C.c_longlong), ("ms", C.c_double)]
+
+
 PU_PROFILE_KINDS = 3
 
 
@@ -87,6 +95,15 @@ SIGNATURES = {
     "pu_dycore_diagnostics": (_I, [_P, C.POINTER(pu_diag)]),
     "pu_dycore_synchronize": (_I, [_P]),
     "pu_dycore_kernel_launches": (C.c_longlong, [_P]),
+    "pu_dycore_learned_harvest": (_I, [_P, C.c_longlong, C.c_ulonglong]),
+    "pu_dycore_learned_train": (_I, [_P, _I, _I, _D, C.c_ulonglong, C.POINTER(pu_learn_stats)]),
+    "pu_dycore_learned_get_weights": (_I, [_P, _P]),
+    "pu_dycore_learned_set_weights": (_I, [_P, _P]),
+    "pu_dycore_learned_eval": (_I, [_P, _P, C.c_longlong, _P, _P, _I]),
+    "pu_dycore_learned_gradient": (_I, [_P, _P, _P, C.c_longlong, _P, C.POINTER(_D)]),
+    "pu_dycore_set_weno_mode": (_I, [_P, _I]),
+    "pu_dycore_learned_set_threshold": (_I, [_P, _D]),
+    "pu_dycore_learned_counts": (_I, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "pu_dycore_profile": (_I, [_P, _I]),
     "pu_dycore_profile_read": (_I, [_P, C.POINTER(pu_profile)]),
     "pu_dycore_time_step_noalloc": (_I, [C.POINTER(pu_config), _P, _P, _P, C.POINTER(pu_state_view), _D,

@@ -27,9 +27,19 @@
 
 #include <cstdint>
 
+#include "mlp_infer.cuh"
 #include "weno9.cuh"
 
 namespace pu {
+
+// Minimum resident blocks per SM requested for the learned stencil kernels
+// (caps their registers: the network's operand fragments stay in registers).
+#ifndef PU_LEARNED_XY_MIN_BLOCKS
+#define PU_LEARNED_XY_MIN_BLOCKS 2
+#endif
+#ifndef PU_LEARNED_Z_MIN_BLOCKS
+#define PU_LEARNED_Z_MIN_BLOCKS 3
+#endif
 
 constexpr int HS = 4;
 constexpr int BC_PERIODIC = 0, BC_PRECURSOR = 1, BC_WALL = 2;
@@ -55,6 +65,10 @@ struct Grid {
   const uint8_t *flags;         // FLAG_IMM | FLAG_ANY10 per cell, or null
   const R *imm_mult;            // immersed_proportion^power / tau per cell, or null
   int *err;                     // bit 0: a non-finite value was written
+  // Learned WENO weights (kernels instantiated with LEARNED only).
+  const uint32_t *ml_frags;     // per-lane operand fragments of the network
+  unsigned long long *ml_counts;  // [0] stencils given learned weights, [1] limiter fallbacks
+  float ml_jump;                // largest normalised neighbour jump given learned weights
 };
 
 __device__ __forceinline__ int wrapi(int i, int n) {
@@ -115,7 +129,7 @@ __device__ __forceinline__ void riemann(const R (&L)[6 + NTR], const R (&Rt)[6 +
   for (int t = 0; t < NTR; t++) flux[5 + t] = ru_upw * (up ? L[6 + t] : Rt[6 + t]);
 }
 
-template <class R, int NTR, int TX, int TY, bool IMM>
+template <class R, int NTR, int TX, int TY, bool IMM, bool LEARNED = false>
 struct XYShape {
   static constexpr int F = 6 + NTR, S = 5 + NTR, NT = TX * TY;
   static constexpr int HX = TX + 10, HY = TY + 10;       // tile plus 5-cell halos
@@ -123,14 +137,75 @@ struct XYShape {
   static constexpr int EN = EXN > EYN ? EXN : EYN;
   static constexpr int FXN = TY * (TX + 1), FYN = (TY + 1) * TX;
   static constexpr int FN = FXN > FYN ? FXN : FYN;
+  // Learned mode: per-warp network scratch and two fallback counters; the
+  // fallback queue (16-bit stencil indices) lives in the flux buffer, which
+  // is idle while edges are reconstructed.
+  static constexpr size_t learned_bytes = LEARNED ? size_t(NT / 32) * mlp::WARP_SMEM_BYTES + 16 : 0;
   static constexpr size_t bytes = sizeof(R) * (size_t(F) * HY * HX + 2 * size_t(F) * EN + size_t(S) * FN) +
-                                  (IMM ? size_t(HY) * HX : 0);
+                                  (IMM ? (size_t(HY) * HX + 15) / 16 * 16 : 0) + learned_bytes;
+  static_assert(!LEARNED || size_t(F) * EN * 2 <= sizeof(R) * S * FN, "fallback queue exceeds the flux buffer");
+  static_assert(NT % 32 == 0, "whole warps");
 };
 
+// Edge reconstruction of `total` stencils with learned weights by the NT
+// threads of a block.  Every warp walks the stencil list in lock step (one
+// stencil per lane), so the network is always evaluated by full warps.
+// Stencils with an immersed cell within reach, or a normalised neighbour jump
+// above G.ml_jump, go to a queue and are then reconstructed by the plain
+// limiter, again by all threads.  load(it, s, imm, any10) fetches stencil it
+// (with the immersed modifications applied), store(it, qL, qR) writes its
+// edges.  Returns the number of fallbacks.
+template <int NT, class Load, class Store>
+__device__ __forceinline__ int recon_learned(const Grid<float> &G, uint32_t *sW, uint16_t *queue, int *qn, int total,
+                                             Load load, Store store) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  MlpLane L;
+  load_lane(G.ml_frags, L);
+  for (int base = tid & ~31; base < total; base += NT) {
+    const int it = base + lane;
+    const bool valid = it < total;
+    float s[9];
+    unsigned imm;
+    bool any10;
+    load(valid ? it : base, s, imm, any10);
+    float x[9], wl[5], wr[5];
+    const float jmp = normalize9(s, x);
+    mlp_warp_weights(L, sW, x, wl, wr);
+    const bool fb = valid && (any10 || imm != 0u || jmp > G.ml_jump);
+    if (valid && !fb) {
+      float qL, qR;
+      edges_from_weights(s, wl, wr, qL, qR);
+      store(it, qL, qR);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, fb);
+    if (m) {
+      int pos = 0;
+      if (lane == 0) pos = atomicAdd(qn, __popc(m));
+      pos = __shfl_sync(0xffffffffu, pos, 0);
+      if (fb) queue[pos + __popc(m & ((1u << lane) - 1u))] = uint16_t(it);
+    }
+  }
+  __syncthreads();
+  const int nq = *qn;
+  for (int q = tid; q < nq; q += NT) {
+    const int it = queue[q];
+    float s[9];
+    unsigned imm;
+    bool any10;
+    load(it, s, imm, any10);
+    float qL, qR;
+    weno9_edges(s, qL, qR, !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
+    store(it, qL, qR);
+  }
+  return nq;
+}
+
 // x/y fluxes and their divergence for one (x,y) tile of one level.
-template <class R, int NTR, int TX, int TY, bool IMM>
-__global__ void __launch_bounds__(TX *TY) k_xy(const Grid<R> G, const R *__restrict__ sin, R *__restrict__ txy) {
-  using Sh = XYShape<R, NTR, TX, TY, IMM>;
+// LEARNED (FP32, weno_all only): edges from the network's weights, with the
+// plain limiter as the fallback.
+template <class R, int NTR, int TX, int TY, bool IMM, bool LEARNED = false>
+__global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : 1) k_xy(const Grid<R> G, const R *__restrict__ sin, R *__restrict__ txy) {
+  using Sh = XYShape<R, NTR, TX, TY, IMM, LEARNED>;
   constexpr int F = Sh::F, S = Sh::S, NT = Sh::NT, HX = Sh::HX, HY = Sh::HY, EN = Sh::EN, FN = Sh::FN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R *H = reinterpret_cast<R *>(smem_raw);
@@ -138,12 +213,17 @@ __global__ void __launch_bounds__(TX *TY) k_xy(const Grid<R> G, const R *__restr
   R *ER = EL + F * EN;
   R *FL = ER + F * EN;
   uint8_t *M = reinterpret_cast<uint8_t *>(FL + S * FN);
+  unsigned char *lrn = reinterpret_cast<unsigned char *>(FL + S * FN) + (IMM ? (size_t(HY) * HX + 15) / 16 * 16 : 0);
+  int *qn = reinterpret_cast<int *>(lrn);                    // [2] fallback counts (x, y)
+  uint32_t *sW = reinterpret_cast<uint32_t *>(lrn + 16) + (threadIdx.x >> 5) * (mlp::WARP_SMEM_BYTES / 4);
+  uint16_t *queue = reinterpret_cast<uint16_t *>(FL);
 
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k = blockIdx.z;
   const int nx = G.nx, ny = G.ny;
   const size_t plane = size_t(k) * G.NP;
   const bool sim2d = G.sim2d != 0;
+  if (LEARNED && tid < 2) qn[tid] = 0;
 
   // 1. Primitive fields of the tile, its x halo rows and its y halo columns.
   constexpr int NA = TY * HX, NB = 10 * TX;
@@ -169,15 +249,13 @@ __global__ void __launch_bounds__(TX *TY) k_xy(const Grid<R> G, const R *__restr
   __syncthreads();
 
   // 2. x edges of cells -1..TX of every tile row.
-  for (int it = tid; it < F * Sh::EXN; it += NT) {
+  auto load_x = [&](int it, R (&s)[9], unsigned &imm, bool &any10) {
     const int f = it / Sh::EXN, rem = it % Sh::EXN, r = rem / (TX + 2), c = rem % (TX + 2);
     const R *row = H + (f * HY + 5 + r) * HX + c;
-    R s[9];
 #pragma unroll
     for (int m = 0; m < 9; m++) s[m] = row[m];
-    R qL, qR;
-    bool any10 = false;
-    unsigned imm = 0;
+    imm = 0;
+    any10 = false;
     if (IMM) {
       const uint8_t *mr = M + (5 + r) * HX + c;
 #pragma unroll
@@ -185,10 +263,26 @@ __global__ void __launch_bounds__(TX *TY) k_xy(const Grid<R> G, const R *__restr
       any10 = (mr[4] & FLAG_ANY10) != 0;
       if (f == iV || f == iW || f == iP) der0_modify(s, imm);
     }
-    if (!any10 && !G.weno_all) linear9_edges(s, qL, qR);
-    else weno9_edges(s, qL, qR, !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
+  };
+  auto store_x = [&](int it, R qL, R qR) {
+    const int f = it / Sh::EXN, rem = it % Sh::EXN;
     EL[f * EN + rem] = qL;
     ER[f * EN + rem] = qR;
+  };
+  int n_fb = 0;
+  if constexpr (LEARNED) {
+    n_fb += recon_learned<NT>(G, sW, queue, qn, F * Sh::EXN, load_x, store_x);
+  } else {
+    for (int it = tid; it < F * Sh::EXN; it += NT) {
+      R s[9];
+      unsigned imm;
+      bool any10;
+      load_x(it, s, imm, any10);
+      R qL, qR;
+      if (!any10 && !G.weno_all) linear9_edges(s, qL, qR);
+      else weno9_edges(s, qL, qR, !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
+      store_x(it, qL, qR);
+    }
   }
   __syncthreads();
 
@@ -226,15 +320,13 @@ __global__ void __launch_bounds__(TX *TY) k_xy(const Grid<R> G, const R *__restr
 
   if (!sim2d) {
     // 5. y edges of cells -1..TY of every tile column.
-    for (int it = tid; it < F * Sh::EYN; it += NT) {
+    auto load_y = [&](int it, R (&s)[9], unsigned &imm, bool &any10) {
       const int f = it / Sh::EYN, rem = it % Sh::EYN, rr = rem / TX, cc = rem % TX;
       const R *col = H + (f * HY + rr) * HX + 5 + cc;
-      R s[9];
 #pragma unroll
       for (int m = 0; m < 9; m++) s[m] = col[m * HX];
-      R qL, qR;
-      bool any10 = false;
-      unsigned imm = 0;
+      imm = 0;
+      any10 = false;
       if (IMM) {
         const uint8_t *mc = M + rr * HX + 5 + cc;
 #pragma unroll
@@ -242,10 +334,26 @@ __global__ void __launch_bounds__(TX *TY) k_xy(const Grid<R> G, const R *__restr
         any10 = (mc[4 * HX] & FLAG_ANY10) != 0;
         if (f == iU || f == iW || f == iP) der0_modify(s, imm);
       }
-      if (!any10 && !G.weno_all) linear9_edges(s, qL, qR);
-      else weno9_edges(s, qL, qR, !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
+    };
+    auto store_y = [&](int it, R qL, R qR) {
+      const int f = it / Sh::EYN, rem = it % Sh::EYN;
       EL[f * EN + rem] = qL;
       ER[f * EN + rem] = qR;
+    };
+    if constexpr (LEARNED) {
+      __syncthreads();   // step 4 has read the flux buffer that holds the queue
+      n_fb += recon_learned<NT>(G, sW, queue, qn + 1, F * Sh::EYN, load_y, store_y);
+    } else {
+      for (int it = tid; it < F * Sh::EYN; it += NT) {
+        R s[9];
+        unsigned imm;
+        bool any10;
+        load_y(it, s, imm, any10);
+        R qL, qR;
+        if (!any10 && !G.weno_all) linear9_edges(s, qL, qR);
+        else weno9_edges(s, qL, qR, !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
+        store_y(it, qL, qR);
+      }
     }
     __syncthreads();
     // 6. Riemann fluxes on y faces 0..TY.
@@ -274,6 +382,11 @@ __global__ void __launch_bounds__(TX *TY) k_xy(const Grid<R> G, const R *__restr
     __syncthreads();
 #pragma unroll
     for (int s = 0; s < S; s++) tend[s] -= (FL[s * FN + (r + 1) * TX + c] - FL[s * FN + r * TX + c]) * G.rdy;
+  }
+  if (LEARNED && tid == 0) {
+    const int total = F * (Sh::EXN + (sim2d ? 0 : Sh::EYN));
+    atomicAdd(G.ml_counts, (unsigned long long)(total - n_fb));
+    atomicAdd(G.ml_counts + 1, (unsigned long long)n_fb);
   }
 
   const int gi = i0 + c, gj = j0 + r;
@@ -304,12 +417,15 @@ __device__ __forceinline__ void enforce_cell(const Grid<R> &G, R (&q)[5 + NTR], 
     if ((G.tracer_positive >> t) & 1u) q[5 + t] = fmax(R(0), q[5 + t]);
 }
 
-template <class R, int NTR, int TX, int TY>
+template <class R, int NTR, int TX, int TY, bool LEARNED = false>
 struct ZShape {
   static constexpr int F = 6 + NTR, NT = TX * TY;
   // 9-plane ring of primitive fields, left edges of the current cell, right
   // edges of the current and the previous cell; all thread-private columns.
-  static constexpr size_t bytes = sizeof(R) * (9 + 3) * size_t(F) * NT;
+  // Learned mode adds per-warp network scratch and a per-warp fallback queue
+  // of up to F*32 entries.
+  static constexpr size_t learned_bytes = LEARNED ? size_t(NT / 32) * (mlp::WARP_SMEM_BYTES + F * 32 * 4) : 0;
+  static constexpr size_t bytes = sizeof(R) * (9 + 3) * size_t(F) * NT + learned_bytes;
 };
 
 // Raw state of one cell (S values) for a later conversion to primitive fields.
@@ -342,8 +458,13 @@ __device__ __forceinline__ void prims_of(const Grid<R> &G, const R (&q)[5 + NTR]
 // inputs of the cell being finalised are loaded before the reconstruction, so
 // global-load latency overlaps the limiter work.  The field loop is not
 // unrolled: one inlined limiter keeps the kernel small.
-template <class R, int NTR, int TX, int TY, bool IMM>
-__global__ void __launch_bounds__(TX *TY) k_z(const Grid<R> G, const R *__restrict__ sin, const R *sn, R *sout,
+// LEARNED (FP32, weno_all only, every block full: nx % TX == ny % TY == 0):
+// each warp evaluates the network for its 32 columns field by field; stencils
+// near walls or immersed cells, or with a normalised neighbour jump above
+// G.ml_jump, are queued per warp and reconstructed by the plain limiter after
+// the level's field loop, by all lanes of the warp.
+template <class R, int NTR, int TX, int TY, bool IMM, bool LEARNED = false>
+__global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : 1) k_z(const Grid<R> G, const R *__restrict__ sin, const R *sn, R *sout,
                                               const R *__restrict__ txy, R a_n, R a_in, R a_dt, int n_enforce,
                                               int kchunk) {
   constexpr int F = 6 + NTR, S = 5 + NTR, NT = TX * TY;
@@ -351,6 +472,10 @@ __global__ void __launch_bounds__(TX *TY) k_z(const Grid<R> G, const R *__restri
   R *ring = reinterpret_cast<R *>(smem_raw);   // [9][F][NT]
   R *eL = ring + 9 * F * NT;                     // [F][NT]
   R *eR = eL + F * NT;                           // [2][F][NT]
+  uint32_t *sW = reinterpret_cast<uint32_t *>(eR + 2 * F * NT) +
+                 (threadIdx.x >> 5) * ((mlp::WARP_SMEM_BYTES + F * 32 * 4) / 4);
+  uint32_t *wq = sW + mlp::WARP_SMEM_BYTES / 4;  // per-warp fallback queue
+  unsigned long long n_learned = 0, n_fallback = 0;
   const int tid = threadIdx.x;
   const int i = blockIdx.x * TX + tid % TX, j = blockIdx.y * TY + tid / TX;
   if (i >= G.nx || j >= G.ny) return;            // no block-wide synchronisation below
@@ -427,17 +552,61 @@ __global__ void __launch_bounds__(TX *TY) k_z(const Grid<R> G, const R *__restri
       int sl[9];
 #pragma unroll
       for (int m = 0; m < 9; m++) sl[m] = slot_of(c - 4 + m) * F * NT + tid;
+      if constexpr (LEARNED) {
+        const int lane = tid & 31;
+        MlpLane L;
+        load_lane(G.ml_frags, L);
+        int cnt = 0;   // queued stencils of this warp (the same in every lane)
 #pragma unroll 1
-      for (int f = 0; f < F; f++) {
-        R s[9];
+        for (int f = 0; f < F; f++) {
+          float s[9], x[9], wl[5], wr[5];
 #pragma unroll
-        for (int m = 0; m < 9; m++) s[m] = ring[sl[m] + f * NT];
-        if (f == iU || f == iV || f == iP) der0_modify(s, imm);
-        R qL, qR;
-        if (!any10 && !G.weno_all) linear9_edges(s, qL, qR);
-        else weno9_edges(s, qL, qR, !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
-        eL[f * NT + tid] = qL;
-        eRc[f * NT] = qR;
+          for (int m = 0; m < 9; m++) s[m] = ring[sl[m] + f * NT];
+          const float jmp = normalize9(s, x);
+          mlp_warp_weights(L, sW, x, wl, wr);
+          const bool fb = any10 || imm != 0u || jmp > G.ml_jump;
+          if (!fb) {
+            float qL, qR;
+            edges_from_weights(s, wl, wr, qL, qR);
+            eL[f * NT + tid] = qL;
+            eRc[f * NT] = qR;
+          }
+          const unsigned mk = __ballot_sync(0xffffffffu, fb);
+          if (fb)
+            wq[cnt + __popc(mk & ((1u << lane) - 1u))] =
+                unsigned(f) | (unsigned(lane) << 4) | (imm << 9) | (unsigned(any10) << 18);
+          cnt += __popc(mk);
+        }
+        __syncwarp();
+        for (int q = lane; q < cnt; q += 32) {
+          const unsigned e = wq[q];
+          const int f = int(e & 15u), t2 = (tid & ~31) + int((e >> 4) & 31u);
+          const unsigned im = (e >> 9) & 511u;
+          float s[9];
+#pragma unroll
+          for (int m = 0; m < 9; m++) s[m] = ring[sl[m] - tid + t2 + f * NT];
+          if (f == iU || f == iV || f == iP) der0_modify(s, im);
+          float qL, qR;
+          weno9_edges(s, qL, qR, ((e >> 18) & 1u) == 0u, (im >> 3) & 1u, (im >> 5) & 1u);
+          eL[f * NT + t2] = qL;
+          eR[par * F * NT + f * NT + t2] = qR;
+        }
+        __syncwarp();
+        n_learned += unsigned(F * 32 - cnt);
+        n_fallback += unsigned(cnt);
+      } else {
+#pragma unroll 1
+        for (int f = 0; f < F; f++) {
+          R s[9];
+#pragma unroll
+          for (int m = 0; m < 9; m++) s[m] = ring[sl[m] + f * NT];
+          if (f == iU || f == iV || f == iP) der0_modify(s, imm);
+          R qL, qR;
+          if (!any10 && !G.weno_all) linear9_edges(s, qL, qR);
+          else weno9_edges(s, qL, qR, !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
+          eL[f * NT + tid] = qL;
+          eRc[f * NT] = qR;
+        }
       }
     }
     if (c > cstart || (wall && c == 0)) {
@@ -492,6 +661,10 @@ __global__ void __launch_bounds__(TX *TY) k_z(const Grid<R> G, const R *__restri
       for (int s = 0; s < S; s++) Fp[s] = Fc[s];
     }
     par ^= 1;
+  }
+  if (LEARNED && (tid & 31) == 0) {
+    atomicAdd(G.ml_counts, n_learned);
+    atomicAdd(G.ml_counts + 1, n_fallback);
   }
 }
 

@@ -5,13 +5,16 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/pu_dycore.h"
 #include "dycore_kernels.cuh"
+#include "learned.cuh"
 
 namespace pu {
 
@@ -103,8 +106,226 @@ struct ImplBase {
     return PU_OK;
   }
 
+  // Learned weights (pu_dycore_learned_*): FP32 master parameters with Adam
+  // moments, their bfloat16-rounded copy, tensor-core fragments, the harvested
+  // training set and fallback counters.
+  int weno_mode = PU_WENO_PLAIN;
+  float ml_jump = 0.5f;   // largest normalised neighbour jump given learned weights
+  float *ml_theta = nullptr, *ml_m = nullptr, *ml_v = nullptr, *ml_wq = nullptr, *ml_grad = nullptr;
+  float *ml_partial = nullptr;
+  int ml_partial_blocks = 0;
+  uint32_t *ml_frags = nullptr;
+  float *ml_xs = nullptr, *ml_ts = nullptr;
+  long ml_n = 0, ml_cap = 0, ml_step = 0;
+  bool ml_ready = false;
+  unsigned long long *ml_counts = nullptr;   // [0] stencils on the learned path, [1] fallbacks
+
+  int ml_alloc() {
+    if (ml_theta) return PU_OK;
+    const size_t P = mlp::NPARAM;
+    void *p;
+    for (float **dst : {&ml_theta, &ml_m, &ml_v, &ml_wq}) {
+      PU_CK(cudaMalloc(&p, P * sizeof(float)));
+      *dst = static_cast<float *>(p);
+    }
+    PU_CK(cudaMalloc(&p, (P + 1) * sizeof(float)));
+    ml_grad = static_cast<float *>(p);
+    PU_CK(cudaMalloc(&p, 32 * mlp::FRAG_WORDS * sizeof(uint32_t)));
+    ml_frags = static_cast<uint32_t *>(p);
+    PU_CK(cudaMalloc(&p, 2 * sizeof(unsigned long long)));
+    ml_counts = static_cast<unsigned long long *>(p);
+    PU_CK(cudaMemsetAsync(ml_counts, 0, 2 * sizeof(unsigned long long), st));
+    // He-uniform weights and zero biases from splitmix64(seed 0 << 32 | index).
+    std::vector<float> h(P, 0.f);
+    for (size_t q = 0; q < P; q++) {
+      if (mlp::is_bias(int(q))) continue;
+      unsigned long long z = q + 0x9E3779B97F4A7C15ull;
+      z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+      z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+      z = z ^ (z >> 31);
+      const double u = double(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+      const int fan_in = int(q) < mlp::OFF_B1 ? mlp::NIN : mlp::NH;
+      h[q] = float(u * std::sqrt(6.0 / fan_in));
+    }
+    return ml_set(h.data());
+  }
+
+  int ml_set(const float *theta_host) {
+    PU_CK(cudaMemcpyAsync(ml_theta, theta_host, mlp::NPARAM * sizeof(float), cudaMemcpyHostToDevice, st));
+    PU_CK(cudaMemsetAsync(ml_m, 0, mlp::NPARAM * sizeof(float), st));
+    PU_CK(cudaMemsetAsync(ml_v, 0, mlp::NPARAM * sizeof(float), st));
+    ml_step = 0;
+    return ml_refresh();
+  }
+
+  // bfloat16 copy and tensor-core fragments of the current master parameters.
+  int ml_refresh() {
+    k_mlp_prepare<<<(mlp::NPARAM + 255) / 256, 256, 0, st>>>(ml_theta, ml_wq);
+    PU_LAUNCHED();
+    k_mlp_frags<<<1, 32, 0, st>>>(ml_theta, ml_frags);
+    PU_LAUNCHED();
+    ml_ready = true;
+    return PU_OK;
+  }
+
+  int ml_get(float *theta_host) {
+    PU_CK(cudaMemcpyAsync(theta_host, ml_theta, mlp::NPARAM * sizeof(float), cudaMemcpyDeviceToHost, st));
+    PU_CK(cudaStreamSynchronize(st));
+    return PU_OK;
+  }
+
+  int ml_reserve(long n) {
+    if (n <= ml_cap) return PU_OK;
+    n = std::max(n, 2 * ml_cap);
+    void *xs, *ts;
+    PU_CK(cudaMalloc(&xs, size_t(n) * 9 * sizeof(float)));
+    cudaError_t e = cudaMalloc(&ts, size_t(n) * 5 * sizeof(float));
+    if (e != cudaSuccess) {
+      cudaFree(xs);
+      set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      return PU_ERR_NOMEM;
+    }
+    if (ml_n) {
+      PU_CK(cudaMemcpyAsync(xs, ml_xs, size_t(ml_n) * 9 * sizeof(float), cudaMemcpyDeviceToDevice, st));
+      PU_CK(cudaMemcpyAsync(ts, ml_ts, size_t(ml_n) * 5 * sizeof(float), cudaMemcpyDeviceToDevice, st));
+      PU_CK(cudaStreamSynchronize(st));
+    }
+    cudaFree(ml_xs);
+    cudaFree(ml_ts);
+    ml_xs = static_cast<float *>(xs);
+    ml_ts = static_cast<float *>(ts);
+    ml_cap = n;
+    return PU_OK;
+  }
+
+  int ml_partials(int nblocks) {
+    if (nblocks <= ml_partial_blocks) return PU_OK;
+    cudaFree(ml_partial);
+    void *p;
+    PU_CK(cudaMalloc(&p, size_t(nblocks) * (mlp::NPARAM + 1) * sizeof(float)));
+    ml_partial = static_cast<float *>(p);
+    ml_partial_blocks = nblocks;
+    return PU_OK;
+  }
+
+  // One forward/backward over `batch` samples of (xs, ts): gradient in ml_grad.
+  int ml_fwd_bwd(const float *xs, const float *ts, long ndata, int batch, unsigned long long seed, int sequential) {
+    const int nb = (batch + mlp::TB - 1) / mlp::TB;
+    int rc = ml_partials(nb);
+    if (rc) return rc;
+    PU_CK(cudaFuncSetAttribute(k_mlp_fwd_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(mlp_train_smem_bytes())));
+    k_mlp_fwd_bwd<<<nb, mlp::TB, mlp_train_smem_bytes(), st>>>(ml_wq, xs, ts, ndata, ml_step, seed, batch, sequential,
+                                                               ml_partial);
+    PU_LAUNCHED();
+    k_mlp_reduce<<<(mlp::NPARAM + 1 + 255) / 256, 256, 0, st>>>(ml_partial, nb, ml_grad);
+    PU_LAUNCHED();
+    return PU_OK;
+  }
+
+  int ml_train(int steps, int batch, double lr, unsigned long long seed, pu_learn_stats *out) {
+    if (ml_n <= 0) {
+      set_error("no harvested stencils: call pu_dycore_learned_harvest first");
+      return PU_ERR_STATE;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    float loss0 = 0, loss1 = 0;
+    for (int it = 0; it < steps; it++) {
+      int rc = ml_fwd_bwd(ml_xs, ml_ts, ml_n, batch, seed, 0);
+      if (rc) return rc;
+      if (it == 0 || it == steps - 1) {
+        float L;
+        PU_CK(cudaMemcpyAsync(&L, ml_grad + mlp::NPARAM, sizeof(float), cudaMemcpyDeviceToHost, st));
+        PU_CK(cudaStreamSynchronize(st));
+        (it == 0 ? loss0 : loss1) = L / batch;
+      }
+      ml_step++;
+      const float b1 = 0.9f, b2 = 0.999f;
+      const float bc1 = float(1.0 - std::pow(0.9, double(ml_step))), bc2 = float(1.0 - std::pow(0.999, double(ml_step)));
+      k_adam<<<(mlp::NPARAM + 255) / 256, 256, 0, st>>>(ml_theta, ml_m, ml_v, ml_grad, float(lr), b1, b2, 1e-8f, bc1, bc2);
+      PU_LAUNCHED();
+      k_mlp_prepare<<<(mlp::NPARAM + 255) / 256, 256, 0, st>>>(ml_theta, ml_wq);
+      PU_LAUNCHED();
+    }
+    cudaEventRecord(e1, st);
+    PU_CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int rc = ml_refresh();
+    if (rc) return rc;
+    if (out) {
+      out->loss_first = loss0;
+      out->loss_last = loss1;
+      out->steps = steps;
+      out->samples = ml_n;
+      out->ms = ms;
+    }
+    return PU_OK;
+  }
+
+  // Check entries: network weights or gradients of host-provided stencils.
+  int ml_eval(const float *x, long n, float *wl, float *wr, int use_mma) {
+    float *dx, *dl, *dr;
+    void *p;
+    PU_CK(cudaMalloc(&p, size_t(n) * 19 * sizeof(float)));
+    dx = static_cast<float *>(p);
+    dl = dx + n * 9;
+    dr = dl + n * 5;
+    int rc = PU_OK;
+    cudaMemcpyAsync(dx, x, size_t(n) * 9 * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (use_mma) {
+      const int warps = 4;
+      k_mlp_eval_mma<<<unsigned((n + 32 * warps - 1) / (32 * warps)), 32 * warps, warps * mlp::WARP_SMEM_BYTES, st>>>(
+          ml_frags, dx, n, dl, dr);
+    } else {
+      k_mlp_eval<<<unsigned((n + 255) / 256), 256, 0, st>>>(ml_wq, dx, n, dl);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      set_error(std::string("kernel launch: ") + cudaGetErrorString(e));
+      rc = PU_ERR_CUDA;
+    } else {
+      launches++;
+      cudaMemcpyAsync(wl, dl, size_t(n) * 5 * sizeof(float), cudaMemcpyDeviceToHost, st);
+      if (use_mma && wr) cudaMemcpyAsync(wr, dr, size_t(n) * 5 * sizeof(float), cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) rc = PU_ERR_CUDA;
+    }
+    cudaFree(dx);
+    return rc;
+  }
+
+  int ml_gradient(const float *x, const float *t, long n, float *grad, double *loss) {
+    void *p;
+    PU_CK(cudaMalloc(&p, size_t(n) * 14 * sizeof(float)));
+    float *dx = static_cast<float *>(p), *dt = dx + n * 9;
+    cudaMemcpyAsync(dx, x, size_t(n) * 9 * sizeof(float), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dt, t, size_t(n) * 5 * sizeof(float), cudaMemcpyHostToDevice, st);
+    int rc = ml_fwd_bwd(dx, dt, n, int(n), 0, 1);
+    float h[mlp::NPARAM + 1];
+    if (!rc && cudaMemcpyAsync(h, ml_grad, sizeof(h), cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+        cudaStreamSynchronize(st) == cudaSuccess) {
+      for (int q = 0; q < mlp::NPARAM; q++) grad[q] = h[q];
+      if (loss) *loss = double(h[mlp::NPARAM]) / double(n);
+    } else if (!rc) {
+      rc = PU_ERR_CUDA;
+    }
+    cudaFree(p);
+    return rc;
+  }
+
+  virtual int ml_harvest(long n, unsigned long long seed) = 0;
+
   virtual ~ImplBase() {
     for (auto e : ev_pool) cudaEventDestroy(e);
+    if (owns)
+      for (void *q : {(void *)ml_theta, (void *)ml_m, (void *)ml_v, (void *)ml_wq, (void *)ml_grad, (void *)ml_partial,
+                      (void *)ml_frags, (void *)ml_xs, (void *)ml_ts, (void *)ml_counts})
+        if (q) cudaFree(q);
   }
   virtual int alloc() = 0;
   virtual int init(const pu_state_view *v, const double *prop, int mem) = 0;
@@ -225,6 +446,22 @@ struct Impl : ImplBase {
                                int(ZShape<R, NTR, ZTX, ZTY>::bytes)));
     PU_CK(cudaFuncSetAttribute(k_z<R, NTR, ZTX, ZTY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(ZShape<R, NTR, ZTX, ZTY>::bytes)));
+    if constexpr (std::is_same<R, float>::value) {
+      PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_BIG, XTY_BIG, false, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(XYShape<R, NTR, XTX_BIG, XTY_BIG, false, true>::bytes)));
+      PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_BIG, XTY_BIG, true, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(XYShape<R, NTR, XTX_BIG, XTY_BIG, true, true>::bytes)));
+      PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_SM, XTY_SM, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(XYShape<R, NTR, XTX_SM, XTY_SM, false, true>::bytes)));
+      PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_SM, XTY_SM, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(XYShape<R, NTR, XTX_SM, XTY_SM, true, true>::bytes)));
+      PU_CK(cudaFuncSetAttribute(k_z<R, NTR, ZTX, ZTY, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(ZShape<R, NTR, ZTX, ZTY, true>::bytes)));
+      PU_CK(cudaFuncSetAttribute(k_z<R, NTR, ZTX, ZTY, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(ZShape<R, NTR, ZTX, ZTY, true>::bytes)));
+    }
     return PU_OK;
   }
 
@@ -274,6 +511,9 @@ struct Impl : ImplBase {
     G.flags = has_imm ? flags : nullptr;
     G.imm_mult = has_imm ? static_cast<const R *>(imm_mult) : nullptr;
     G.err = err;
+    G.ml_frags = ml_frags;
+    G.ml_counts = ml_counts;
+    G.ml_jump = ml_jump;
     return G;
   }
 
@@ -411,32 +651,44 @@ struct Impl : ImplBase {
     return check_err();
   }
 
-  template <bool IMM>
+  // Learned weights replace the nonlinear limiter where it runs on every
+  // stencil (weno_all) in FP32.
+  bool learned_active() const {
+    return std::is_same<R, float>::value && weno_mode == PU_WENO_LEARNED && ml_ready && cfg.weno_all;
+  }
+
+  template <bool IMM, bool LRN>
   int stage(const Grid<R> &G, const R *sin, const R *sn, R *sout, R a_n, R a_in, R a_dt, int n_enforce) {
+    constexpr bool L = LRN && std::is_same<R, float>::value;
     R *t = static_cast<R *>(txy);
     cudaEvent_t e0 = prof_begin();
     if (small_tile) {
-      using Sh = XYShape<R, NTR, XTX_SM, XTY_SM, IMM>;
+      using Sh = XYShape<R, NTR, XTX_SM, XTY_SM, IMM, L>;
       dim3 g(blocks(cfg.nx, XTX_SM), blocks(cfg.ny, XTY_SM), cfg.nz);
-      k_xy<R, NTR, XTX_SM, XTY_SM, IMM><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
+      k_xy<R, NTR, XTX_SM, XTY_SM, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
     } else {
-      using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM>;
+      using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM, L>;
       dim3 g(blocks(cfg.nx, XTX_BIG), blocks(cfg.ny, XTY_BIG), cfg.nz);
-      k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
+      k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
     }
     PU_LAUNCHED();
     prof_end(0, e0);
     const int kc = cfg.z_chunk > 0 ? cfg.z_chunk : (cfg.nz < 16 ? cfg.nz : 16);
     dim3 gz(blocks(cfg.nx, ZTX), blocks(cfg.ny, ZTY), blocks(cfg.nz, kc));
     cudaEvent_t e1 = prof_begin();
-    k_z<R, NTR, ZTX, ZTY, IMM><<<gz, ZTX * ZTY, ZShape<R, NTR, ZTX, ZTY>::bytes, st>>>(G, sin, sn, sout, t, a_n, a_in,
-                                                                                     a_dt, n_enforce, kc);
+    // The learned z march needs full warps: every block's columns inside the domain.
+    if (L && cfg.nx % ZTX == 0 && cfg.ny % ZTY == 0)
+      k_z<R, NTR, ZTX, ZTY, IMM, L><<<gz, ZTX * ZTY, ZShape<R, NTR, ZTX, ZTY, L>::bytes, st>>>(
+          G, sin, sn, sout, t, a_n, a_in, a_dt, n_enforce, kc);
+    else
+      k_z<R, NTR, ZTX, ZTY, IMM><<<gz, ZTX * ZTY, ZShape<R, NTR, ZTX, ZTY>::bytes, st>>>(G, sin, sn, sout, t, a_n,
+                                                                                       a_in, a_dt, n_enforce, kc);
     PU_LAUNCHED();
     prof_end(1, e1);
     return PU_OK;
   }
 
-  template <bool IMM>
+  template <bool IMM, bool LRN>
   int advance_t(double dt, int nsteps) {
     const Grid<R> G = grid();
     R *s0 = static_cast<R *>(s[0]), *s1 = static_cast<R *>(s[1]), *s2 = static_cast<R *>(s[2]);
@@ -445,16 +697,17 @@ struct Impl : ImplBase {
     PU_LAUNCHED();
     prof_end(2, e0);
     for (int n = 0; n < nsteps; n++) {
-      PU_TRY(stage<IMM>(G, s0, nullptr, s1, R(0), R(1), R(dt), 1));
-      PU_TRY(stage<IMM>(G, s1, s0, s2, R(3. / 4.), R(1. / 4.), R(1. / 4. * dt), 1));
-      PU_TRY(stage<IMM>(G, s2, s0, s0, R(1. / 3.), R(2. / 3.), R(2. / 3. * dt), n == nsteps - 1 ? 1 : 2));
+      PU_TRY((stage<IMM, LRN>(G, s0, nullptr, s1, R(0), R(1), R(dt), 1)));
+      PU_TRY((stage<IMM, LRN>(G, s1, s0, s2, R(3. / 4.), R(1. / 4.), R(1. / 4. * dt), 1)));
+      PU_TRY((stage<IMM, LRN>(G, s2, s0, s0, R(1. / 3.), R(2. / 3.), R(2. / 3. * dt), n == nsteps - 1 ? 1 : 2)));
     }
     return PU_OK;
   }
 
   int advance(double dt, int nsteps) override {
     if (nsteps <= 0) return PU_OK;
-    return has_imm ? advance_t<true>(dt, nsteps) : advance_t<false>(dt, nsteps);
+    if (learned_active()) return has_imm ? advance_t<true, true>(dt, nsteps) : advance_t<false, true>(dt, nsteps);
+    return has_imm ? advance_t<true, false>(dt, nsteps) : advance_t<false, false>(dt, nsteps);
   }
 
   int get_conserved(double *stp, double *trp, int mem) override {
@@ -508,6 +761,20 @@ struct Impl : ImplBase {
     cudaFree(old_r);
     if (old_rt) cudaFree(old_rt);
     return rc;
+  }
+
+  int ml_harvest(long n, unsigned long long seed) override {
+    int rc = ml_alloc();
+    if (rc) return rc;
+    rc = ml_reserve(ml_n + n);
+    if (rc) return rc;
+    const Grid<R> G = grid();
+    k_harvest<R, NTR><<<blocks(size_t(n), 128), 128, 0, st>>>(G, static_cast<const R *>(s[0]), n, seed, ml_n,
+                                                              ml_xs + size_t(ml_n) * 9, ml_ts + size_t(ml_n) * 5);
+    PU_LAUNCHED();
+    PU_CK(cudaStreamSynchronize(st));
+    ml_n += n;
+    return PU_OK;
   }
 
   int diagnostics(pu_diag *out) override {

@@ -86,7 +86,7 @@ int check_config(const pu_config *c) {
   if (c->bc_z != PU_BC_WALL && c->bc_z != PU_BC_PERIODIC)
     return fail(PU_ERR_INVALID, "ERROR: Specified invalid bc_z in coupler options");
   if (c->precision != PU_F32 && c->precision != PU_F64) return fail(PU_ERR_INVALID, "precision must be PU_F32 or PU_F64");
-  if (c->weno_mode != PU_WENO_PLAIN) return fail(PU_ERR_UNSUPPORTED, "this build only has the plain WENO path");
+  if (c->weno_mode != PU_WENO_PLAIN && c->weno_mode != PU_WENO_LEARNED) return fail(PU_ERR_INVALID, "bad WENO mode");
   if (!(c->gamma_d > 1 && c->C0 > 0 && c->R_d > 0 && c->cfl > 0)) return fail(PU_ERR_INVALID, "bad thermodynamic options");
   if (c->z_chunk < 0) return fail(PU_ERR_INVALID, "z_chunk must be >= 0");
   return PU_OK;
@@ -123,6 +123,7 @@ int pu_dycore_create(const pu_config *cfg, pu_dycore **out) {
   I.N = size_t(cfg->nx) * cfg->ny * cfg->nz;
   I.NP = size_t(cfg->nx) * cfg->ny;
   I.nzh = cfg->nz + 2 * PU_HS;
+  I.weno_mode = cfg->weno_mode;
   rc = I.alloc();
   if (rc) return rc;
   *out = h.release();
@@ -244,6 +245,90 @@ int pu_dycore_synchronize(pu_dycore *h) {
 }
 
 long long pu_dycore_kernel_launches(const pu_dycore *h) { return h ? h->impl->launches : 0; }
+
+int pu_dycore_learned_harvest(pu_dycore *h, long long n, unsigned long long seed) {
+  if (!h || n <= 0) return fail(PU_ERR_INVALID, "bad argument");
+  if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
+  DeviceGuard g(h->device);
+  return h->impl->ml_harvest(long(n), seed);
+}
+
+int pu_dycore_learned_train(pu_dycore *h, int steps, int batch, double lr, unsigned long long seed,
+                            pu_learn_stats *out) {
+  if (!h || steps < 0 || batch <= 0 || !(lr > 0)) return fail(PU_ERR_INVALID, "bad argument");
+  DeviceGuard g(h->device);
+  int rc = h->impl->ml_alloc();
+  if (rc) return rc;
+  return h->impl->ml_train(steps, batch, lr, seed, out);
+}
+
+int pu_dycore_learned_get_weights(pu_dycore *h, float *theta) {
+  if (!h || !theta) return fail(PU_ERR_INVALID, "null argument");
+  DeviceGuard g(h->device);
+  int rc = h->impl->ml_alloc();
+  if (rc) return rc;
+  return h->impl->ml_get(theta);
+}
+
+int pu_dycore_learned_set_weights(pu_dycore *h, const float *theta) {
+  if (!h || !theta) return fail(PU_ERR_INVALID, "null argument");
+  DeviceGuard g(h->device);
+  int rc = h->impl->ml_alloc();
+  if (rc) return rc;
+  return h->impl->ml_set(theta);
+}
+
+int pu_dycore_learned_eval(pu_dycore *h, const float *x, long long n, float *wl, float *wr, int use_mma) {
+  if (!h || !x || !wl || n <= 0) return fail(PU_ERR_INVALID, "bad argument");
+  DeviceGuard g(h->device);
+  int rc = h->impl->ml_alloc();
+  if (rc) return rc;
+  return h->impl->ml_eval(x, long(n), wl, wr, use_mma);
+}
+
+int pu_dycore_learned_gradient(pu_dycore *h, const float *x, const float *t, long long n, float *grad,
+                               double *loss) {
+  if (!h || !x || !t || !grad || n <= 0 || n > (1 << 20)) return fail(PU_ERR_INVALID, "bad argument");
+  DeviceGuard g(h->device);
+  int rc = h->impl->ml_alloc();
+  if (rc) return rc;
+  return h->impl->ml_gradient(x, t, long(n), grad, loss);
+}
+
+int pu_dycore_set_weno_mode(pu_dycore *h, int mode) {
+  if (!h) return fail(PU_ERR_INVALID, "null handle");
+  if (mode != PU_WENO_PLAIN && mode != PU_WENO_LEARNED) return fail(PU_ERR_INVALID, "bad WENO mode");
+  if (mode == PU_WENO_LEARNED) {
+    if (h->impl->cfg.precision != PU_F32) return fail(PU_ERR_UNSUPPORTED, "learned weights run in the FP32 build only");
+    if (!h->impl->cfg.weno_all)
+      return fail(PU_ERR_UNSUPPORTED, "learned weights replace the limiter of weno_all; this dycore uses linear edges");
+    if (!h->impl->ml_ready) return fail(PU_ERR_STATE, "learned weights are neither trained nor loaded");
+  }
+  h->impl->weno_mode = mode;
+  return PU_OK;
+}
+
+int pu_dycore_learned_set_threshold(pu_dycore *h, double max_jump) {
+  if (!h) return fail(PU_ERR_INVALID, "null handle");
+  if (!(max_jump >= 0)) return fail(PU_ERR_INVALID, "the jump threshold must be >= 0");
+  h->impl->ml_jump = float(max_jump);
+  return PU_OK;
+}
+
+int pu_dycore_learned_counts(pu_dycore *h, long long *learned, long long *fallback) {
+  if (!h) return fail(PU_ERR_INVALID, "null handle");
+  DeviceGuard g(h->device);
+  unsigned long long c[2] = {0, 0};
+  auto &I = *h->impl;
+  if (I.ml_counts) {
+    if (cudaMemcpyAsync(c, I.ml_counts, sizeof(c), cudaMemcpyDeviceToHost, I.st) != cudaSuccess ||
+        cudaMemsetAsync(I.ml_counts, 0, sizeof(c), I.st) != cudaSuccess || cudaStreamSynchronize(I.st) != cudaSuccess)
+      return fail(PU_ERR_CUDA, "reading the learned-path counters failed");
+  }
+  if (learned) *learned = (long long)c[0];
+  if (fallback) *fallback = (long long)c[1];
+  return PU_OK;
+}
 
 int pu_dycore_profile(pu_dycore *h, int enable) {
   if (!h) return fail(PU_ERR_INVALID, "null handle");

@@ -105,6 +105,61 @@ __device__ __forceinline__ void weno9_edges(const R (&s)[9], R &qL, R &qR, bool 
   qR = weno9_edge<R, false>(d, s[4], rk, do_map);
 }
 
+// Normalised nonlinear weights of the left edge (after map_rs when do_map),
+// the quantity the learned network is trained to reproduce.
+template <class R>
+__device__ __forceinline__ void weno9_left_weights(const R (&s)[9], R (&w)[5]) {
+  using namespace pu_weno9;
+  R d[8];
+#pragma unroll
+  for (int m = 0; m < 8; m++) d[m] = s[m + 1] - s[m];
+  R tv[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    R y3 = d[k + 3];
+    R y2 = fma(R(TV_L[k][3][2]), d[k + 3], d[k + 2]);
+    R y1 = fma(R(TV_L[k][3][1]), d[k + 3], fma(R(TV_L[k][2][1]), d[k + 2], d[k + 1]));
+    R y0 = fma(R(TV_L[k][3][0]), d[k + 3], fma(R(TV_L[k][2][0]), d[k + 2], fma(R(TV_L[k][1][0]), d[k + 1], d[k])));
+    R t = R(TV_D[k][3]) * y3 * y3;
+    t = fma(R(TV_D[k][2]) * y2, y2, t);
+    t = fma(R(TV_D[k][1]) * y1, y1, t);
+    tv[k] = fma(R(TV_D[k][0]) * y0, y0, t);
+  }
+  convexify5(tv);
+#pragma unroll
+  for (int k = 0; k < 5; k++) w[k] = R(IDEAL_L[k]) * fast_rcp(fma(tv[k], tv[k], R(1.e-20)));
+  convexify5(w);
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    const R dk = R(IDEAL_L[k]);
+    R t = w[k] - dk;
+    R t2 = t * t;
+    R t6 = t2 * t2 * t2;
+    R u = fma(-w[k], w[k], w[k]);
+    R u3 = u * u * u;
+    w[k] = fma(t6 * t, fast_rcp(fma(R(2000.), u3, t6)), dk);
+  }
+  convexify5(w);
+}
+
+// Edge values from given left-edge and right-edge weights (the last step of
+// gll_1 / gll_2, WenoLimiter.h:402-403, 425-426).
+template <class R>
+__device__ __forceinline__ void edges_from_weights(const R (&s)[9], const R (&wl)[5], const R (&wr)[5], R &qL, R &qR) {
+  using namespace pu_weno9;
+  R aL = R(0), aR = R(0);
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    R dk0 = s[k + 1] - s[k], dk1 = s[k + 2] - s[k + 1], dk2 = s[k + 3] - s[k + 2], dk3 = s[k + 4] - s[k + 3];
+    R ll = fma(R(LIN_L[k][3]), dk3, fma(R(LIN_L[k][2]), dk2, fma(R(LIN_L[k][1]), dk1, R(LIN_L[k][0]) * dk0)));
+    R lr = fma(R(LIN_R[k][3]), dk3, fma(R(LIN_R[k][2]), dk2, fma(R(LIN_R[k][1]), dk1, R(LIN_R[k][0]) * dk0)));
+    aL = fma(wl[k], ll, aL);
+    aR = fma(wr[k], lr, aR);
+  }
+  qL = s[4] + aL;
+  qR = s[4] + aR;
+}
+
 // Nine-cell linear edges (weno_all == false away from immersed cells,
 // dynamics_rk.h:539-545, 584-588).
 template <class R>

@@ -186,6 +186,55 @@ class Dycore:
     def kernel_launches(self) -> int:
         return int(self.lib.pu_dycore_kernel_launches(self.h))
 
+    # -- learned WENO weights -----------------------------------------------
+    def learned_harvest(self, n, seed=0):
+        check(self.lib.pu_dycore_learned_harvest(self.h, int(n), int(seed)))
+
+    def learned_train(self, steps, batch=65536, lr=1e-3, seed=0):
+        s = capi.pu_learn_stats()
+        check(self.lib.pu_dycore_learned_train(self.h, int(steps), int(batch), float(lr), int(seed), C.byref(s)))
+        return dict(loss_first=s.loss_first, loss_last=s.loss_last, steps=s.steps, samples=s.samples, ms=s.ms)
+
+    def learned_get_weights(self):
+        th = np.zeros(capi.PU_MLP_PARAMS, np.float32)
+        check(self.lib.pu_dycore_learned_get_weights(self.h, th.ctypes.data))
+        return th
+
+    def learned_set_weights(self, theta):
+        th = np.ascontiguousarray(theta, dtype=np.float32)
+        assert th.size == capi.PU_MLP_PARAMS
+        check(self.lib.pu_dycore_learned_set_weights(self.h, th.ctypes.data))
+
+    def learned_eval(self, x, use_mma=True):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        n = x.shape[0]
+        wl = np.zeros((n, 5), np.float32)
+        wr = np.zeros((n, 5), np.float32)
+        check(self.lib.pu_dycore_learned_eval(self.h, x.ctypes.data, n, wl.ctypes.data, wr.ctypes.data, int(use_mma)))
+        return wl, wr
+
+    def learned_gradient(self, x, t):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.zeros(capi.PU_MLP_PARAMS, np.float32)
+        loss = C.c_double()
+        check(self.lib.pu_dycore_learned_gradient(self.h, x.ctypes.data, t.ctypes.data, x.shape[0], g.ctypes.data,
+                                                  C.byref(loss)))
+        return g, loss.value
+
+    def set_weno_mode(self, mode):
+        check(self.lib.pu_dycore_set_weno_mode(self.h, {"plain": capi.PU_WENO_PLAIN,
+                                                        "learned": capi.PU_WENO_LEARNED}[mode]))
+
+    def learned_set_threshold(self, max_jump):
+        check(self.lib.pu_dycore_learned_set_threshold(self.h, float(max_jump)))
+
+    def learned_counts(self):
+        """(stencils given learned weights, limiter fallbacks) since the last call."""
+        a, b = C.c_longlong(), C.c_longlong()
+        check(self.lib.pu_dycore_learned_counts(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def profile(self, enable=True):
         check(self.lib.pu_dycore_profile(self.h, int(enable)))
 

@@ -1,0 +1,76 @@
+"""Run one of the synthetic cases on the GPU dycore and report its speed.
+
+    python -m porturb_b200.run_case abl_neutral --nx 256 --ny 256 --nz 64 --steps 3
+    python -m porturb_b200.run_case abl_neutral --nz 64 --learned --train-steps 300
+
+Plain mode advances the FP32 (or --precision f64) dycore; --learned first
+harvests stencils from the initial state, trains the network on the GPU and
+then advances with learned weights.  Prints one JSON line with the per-kernel
+CUDA-event times and, in learned mode, the fallback fraction.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import cases
+from .dycore import Dycore
+
+CASES = {
+    "abl_neutral": lambda a: cases.abl_neutral(nx=a.nx, ny=a.ny, nz=a.nz),
+    "warm_bubble": lambda a: cases.warm_bubble(nx=a.nx, ny=a.ny, nz=a.nz),
+    "urban_canopy": lambda a: cases.urban_canopy(nx=a.nx, ny=a.ny, nz=a.nz),
+}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=sorted(CASES))
+    ap.add_argument("--nx", type=int, default=256)
+    ap.add_argument("--ny", type=int, default=256)
+    ap.add_argument("--nz", type=int, default=128)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--learned", action="store_true")
+    ap.add_argument("--harvest", type=int, default=1 << 18)
+    ap.add_argument("--train-steps", type=int, default=300)
+    ap.add_argument("--threshold", type=float, default=0.5)
+    a = ap.parse_args(argv)
+
+    case = CASES[a.case](a)
+    g = Dycore.from_case(case, precision=a.precision)
+    rd, u, v, w, T, trc = [np.ascontiguousarray(x) for x in case.coupler_arrays(perturbed=True)]
+    prop = np.ascontiguousarray(case.immersed_proportion)
+    g.init(rd, u, v, w, T, list(trc), prop if prop.any() else None)
+    dt = g.compute_time_step()
+    out = {"case": a.case, "grid": [a.nx, a.ny, a.nz], "precision": a.precision, "steps": a.steps,
+           "weno": "learned" if a.learned else "plain"}
+    if a.learned:
+        g.learned_harvest(a.harvest, seed=1)
+        out["training"] = g.learned_train(a.train_steps, batch=16384, lr=2e-3, seed=3)
+        g.set_weno_mode("learned")
+        g.learned_set_threshold(a.threshold)
+        g.learned_counts()
+    g.synchronize()
+    g.profile(True)
+    t0 = time.perf_counter()
+    g.advance(dt, a.steps)
+    g.synchronize()
+    wall = time.perf_counter() - t0
+    prof = g.profile_read()
+    g.profile(False)
+    out["ms_per_step"] = wall * 1e3 / max(a.steps, 1)
+    out["kernel_ms"] = {k: v[0] / max(v[1], 1) for k, v in prof.items()}
+    out["cell_steps_per_s"] = case.ncells * a.steps / wall
+    if a.learned:
+        nl, nf = g.learned_counts()
+        out["fallback_frac"] = nf / max(1, nl + nf)
+    g.close()
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

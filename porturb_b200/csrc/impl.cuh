@@ -658,7 +658,7 @@ struct Impl : ImplBase {
   }
 
   template <bool IMM, bool LRN>
-  int stage(const Grid<R> &G, const R *sin, const R *sn, R *sout, R a_n, R a_in, R a_dt, int n_enforce) {
+  int stage(const Grid<R> &G, const R *sin, const R *sn, R *sout, R a_n, R a_dt, int n_enforce) {
     constexpr bool L = LRN && std::is_same<R, float>::value;
     R *t = static_cast<R *>(txy);
     cudaEvent_t e0 = prof_begin();
@@ -679,10 +679,10 @@ struct Impl : ImplBase {
     // The learned z march needs full warps: every block's columns inside the domain.
     if (L && cfg.nx % ZTX == 0 && cfg.ny % ZTY == 0)
       k_z<R, NTR, ZTX, ZTY, IMM, L><<<gz, ZTX * ZTY, ZShape<R, NTR, ZTX, ZTY, L>::bytes, st>>>(
-          G, sin, sn, sout, t, a_n, a_in, a_dt, n_enforce, kc);
+          G, sin, sn, sout, t, a_n, a_dt, n_enforce, kc);
     else
       k_z<R, NTR, ZTX, ZTY, IMM><<<gz, ZTX * ZTY, ZShape<R, NTR, ZTX, ZTY>::bytes, st>>>(G, sin, sn, sout, t, a_n,
-                                                                                       a_in, a_dt, n_enforce, kc);
+                                                                                       a_dt, n_enforce, kc);
     PU_LAUNCHED();
     prof_end(1, e1);
     return PU_OK;
@@ -697,9 +697,11 @@ struct Impl : ImplBase {
     PU_LAUNCHED();
     prof_end(2, e0);
     for (int n = 0; n < nsteps; n++) {
-      PU_TRY((stage<IMM, LRN>(G, s0, nullptr, s1, R(0), R(1), R(dt), 1)));
-      PU_TRY((stage<IMM, LRN>(G, s1, s0, s2, R(3. / 4.), R(1. / 4.), R(1. / 4. * dt), 1)));
-      PU_TRY((stage<IMM, LRN>(G, s2, s0, s0, R(1. / 3.), R(2. / 3.), R(2. / 3. * dt), n == nsteps - 1 ? 1 : 2)));
+      // Shu-Osher SSPRK(3,3) (dynamics_rk.h:308-360): s1 = s0 + dt L(s0);
+      // s2 = 3/4 s0 + 1/4 (s1 + dt L(s1)); s0 <- 1/3 s0 + 2/3 (s2 + dt L(s2)).
+      PU_TRY((stage<IMM, LRN>(G, s0, nullptr, s1, R(0), R(dt), 1)));
+      PU_TRY((stage<IMM, LRN>(G, s1, s0, s2, R(3. / 4.), R(1. / 4. * dt), 1)));
+      PU_TRY((stage<IMM, LRN>(G, s2, s0, s0, R(1. / 3.), R(2. / 3. * dt), n == nsteps - 1 ? 1 : 2)));
     }
     return PU_OK;
   }

@@ -105,6 +105,102 @@ __device__ __forceinline__ void weno9_edges(const R (&s)[9], R &qL, R &qR, bool 
   qR = weno9_edge<R, false>(d, s[4], rk, do_map);
 }
 
+// ---------------------------------------------------------------------------
+// Two stencils at once with packed FP32 arithmetic (FFMA2/FADD2/FMUL2 on
+// sm_100): the same operations in the same order as weno9_edges<float>, per
+// component, so each component's result is bit-identical to the scalar
+// limiter's.  Halves the issue slots of the FP32 work; reciprocals stay
+// scalar (rcp.approx.ftz per component).  Branches of the scalar form
+// become per-component selects (a multiply by exactly 1 where the scalar
+// form skips the normalisation).
+// ---------------------------------------------------------------------------
+struct bool2 {
+  bool x, y;
+};
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(fast_rcp(a.x), fast_rcp(a.y)); }
+
+__device__ __forceinline__ void convexify5x2(float2 (&w)[5]) {
+  const float2 tot = add2(add2(add2(add2(w[0], w[1]), w[2]), w[3]), w[4]);
+  const float2 r = make_float2(tot.x > 1.e-20f ? fast_rcp(tot.x) : 1.f, tot.y > 1.e-20f ? fast_rcp(tot.y) : 1.f);
+#pragma unroll
+  for (int k = 0; k < 5; k++) w[k] = mul2(w[k], r);
+}
+
+template <bool LEFT>
+__device__ __forceinline__ float2 weno9_edge2(const float2 (&d)[8], float2 s4, const float2 (&rk)[5], bool2 do_map) {
+  using namespace pu_weno9;
+  float2 w[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) w[k] = mul2(f2(float(LEFT ? IDEAL_L[k] : IDEAL_R[k])), rk[k]);
+  convexify5x2(w);
+  if (do_map.x || do_map.y) {
+    float2 m[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      const float2 dk = f2(float(LEFT ? IDEAL_L[k] : IDEAL_R[k]));
+      const float2 t = sub2(w[k], dk);
+      const float2 t2 = mul2(t, t);
+      const float2 t6 = mul2(mul2(t2, t2), t2);
+      const float2 u = fma2(make_float2(-w[k].x, -w[k].y), w[k], w[k]);
+      const float2 u3 = mul2(mul2(u, u), u);
+      const float2 den = fma2(f2(2000.f), u3, t6);
+      m[k] = fma2(mul2(t6, t), rcp2(den), dk);
+    }
+    convexify5x2(m);
+#pragma unroll
+    for (int k = 0; k < 5; k++) w[k] = make_float2(do_map.x ? m[k].x : w[k].x, do_map.y ? m[k].y : w[k].y);
+  }
+  float2 acc = f2(0.f);
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    float2 lin = mul2(f2(float(LEFT ? LIN_L[k][0] : LIN_R[k][0])), d[k]);
+#pragma unroll
+    for (int m = 1; m < 4; m++) lin = fma2(f2(float(LEFT ? LIN_L[k][m] : LIN_R[k][m])), d[k + m], lin);
+    acc = fma2(w[k], lin, acc);
+  }
+  return add2(s4, acc);
+}
+
+__device__ __forceinline__ void weno9_edges2(const float2 (&s)[9], float2 &qL, float2 &qR, bool2 do_map, bool2 imm_L,
+                                             bool2 imm_R) {
+  using namespace pu_weno9;
+  float2 d[8];
+#pragma unroll
+  for (int m = 0; m < 8; m++) d[m] = sub2(s[m + 1], s[m]);
+  float2 tv[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) {
+    const float2 y3 = d[k + 3];
+    const float2 y2 = fma2(f2(float(TV_L[k][3][2])), d[k + 3], d[k + 2]);
+    const float2 y1 = fma2(f2(float(TV_L[k][3][1])), d[k + 3], fma2(f2(float(TV_L[k][2][1])), d[k + 2], d[k + 1]));
+    const float2 y0 = fma2(f2(float(TV_L[k][3][0])), d[k + 3],
+                           fma2(f2(float(TV_L[k][2][0])), d[k + 2], fma2(f2(float(TV_L[k][1][0])), d[k + 1], d[k])));
+    float2 t = mul2(mul2(f2(float(TV_D[k][3])), y3), y3);
+    t = fma2(mul2(f2(float(TV_D[k][2])), y2), y2, t);
+    t = fma2(mul2(f2(float(TV_D[k][1])), y1), y1, t);
+    tv[k] = fma2(mul2(f2(float(TV_D[k][0])), y0), y0, t);
+  }
+  convexify5x2(tv);
+  if (imm_L.x || imm_L.y || imm_R.x || imm_R.y) {
+    const float mx = fmaxf(fmaxf(fmaxf(fmaxf(tv[0].x, tv[1].x), tv[2].x), tv[3].x), tv[4].x);
+    const float my = fmaxf(fmaxf(fmaxf(fmaxf(tv[0].y, tv[1].y), tv[2].y), tv[3].y), tv[4].y);
+    if (imm_L.x) tv[4].x = mx;
+    if (imm_L.y) tv[4].y = my;
+    if (imm_R.x) tv[0].x = mx;
+    if (imm_R.y) tv[0].y = my;
+  }
+  float2 rk[5];
+#pragma unroll
+  for (int k = 0; k < 5; k++) rk[k] = rcp2(fma2(tv[k], tv[k], f2(1.e-20f)));
+  qL = weno9_edge2<true>(d, s[4], rk, do_map);
+  qR = weno9_edge2<false>(d, s[4], rk, do_map);
+}
+
 // Normalised nonlinear weights of the left edge (after map_rs when do_map),
 // the quantity the learned network is trained to reproduce.
 template <class R>

@@ -1,0 +1,61 @@
+/* C interface of the CPU oracles of the physics modules that run beside the
+ * dycore in the boundary-layer drivers (TEST INFRASTRUCTURE ONLY):
+ *   orc_phys_*  oracle/_build/liboracle.so      -- this project's restatement
+ *   ref_phys_*  oracle/_ref/libporturb_ref.so   -- the reference's own module
+ *                                                 headers compiled against the
+ *                                                 single-rank shim
+ * Modules (model/modules/ of the reference):
+ *   LES_Closure::apply              les_closure.h:30-320
+ *   sponge_layer                    sponge_layer.h:7-62
+ *   geostrophic_wind_forcing        geostrophic_wind_forcing.h:7-42
+ *   apply_surface_fluxes            surface_flux.h:9-125
+ * All arrays are C-order doubles: coupler fields (nz,ny,nx), tracers
+ * (ntr,nz,ny,nx) in coupler order, immersed halo arrays (nz+2,ny+2,nx+2) with
+ * one halo cell on each side (immersed_proportion_halos,
+ * immersed_roughness_halos, immersed_temp_halos of the drivers' init,
+ * sc_init.h:727-768).  The calls update the coupler arrays in place. */
+#pragma once
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_phys_config {
+  int nx, ny, nz;
+  double xlen, ylen, zlen;
+  int ntr;
+  int tracer_positive[16], tracer_adds_mass[16], tracer_diffuse[16];
+  int idWV, idTKE; /* indices of the water_vapor and TKE tracers */
+  double R_d, R_v, cp_d, gamma_d, C0, grav, p0;
+  int enable_gravity;
+  double kinematic_viscosity;
+  int dns;
+  double les_total_mult, les_dissipation_mult, les_shear_prod_mult;
+  int bc_x, bc_y, bc_z; /* ORC_BC_* of oracle_api.h */
+} orc_phys_config;
+
+void *orc_phys_create(const orc_phys_config *cfg, const double *imm_prop_h, const double *imm_rough_h,
+                      const double *imm_temp_h);
+void orc_phys_destroy(void *h);
+int orc_phys_les(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc, double dt);
+int orc_phys_sponge(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc, double dt,
+                    double time_scale, double top_prop);
+int orc_phys_geostrophic(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc, double dt,
+                         double lat_g, double u_g, double v_g);
+int orc_phys_surface_fluxes(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                            double dt);
+
+void *ref_phys_create(const orc_phys_config *cfg, const double *imm_prop_h, const double *imm_rough_h,
+                      const double *imm_temp_h);
+void ref_phys_destroy(void *h);
+int ref_phys_les(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc, double dt);
+int ref_phys_sponge(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc, double dt,
+                    double time_scale, double top_prop);
+int ref_phys_geostrophic(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc, double dt,
+                         double lat_g, double u_g, double v_g);
+int ref_phys_surface_fluxes(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                            double dt);
+
+#ifdef __cplusplus
+}
+#endif

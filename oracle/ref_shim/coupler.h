@@ -50,6 +50,11 @@ class ParallelComm {
   yakl::Array<typename std::remove_cv<T>::type, N, M, S> all_reduce(yakl::Array<T, N, M, S> const &a, MPI_Op) const {
     return a.template copy_as<M>();
   }
+  template <class T, int N, int M, int S>
+  yakl::Array<typename std::remove_cv<T>::type, N, M, S> all_reduce(yakl::Array<T, N, M, S> const &a, MPI_Op,
+                                                                     std::string) const {
+    return a.template copy_as<M>();
+  }
   template <class T>
   T all_reduce(T v, MPI_Op) const { return v; }
 };
@@ -124,6 +129,9 @@ class Coupler {
   int get_nz() const { return nz; }
   size_t get_nx_glob() const { return nx; }
   size_t get_ny_glob() const { return ny; }
+  real get_xlen() const { return xlen; }
+  real get_ylen() const { return ylen; }
+  real get_zlen() const { return zlen; }
   real get_dx() const { return xlen / nx; }
   real get_dy() const { return ylen / ny; }
   real get_dz() const { return zlen / nz; }
@@ -196,6 +204,29 @@ class Coupler {
       out.add_field(r);
     }
     return out;
+  }
+
+  // Periodic x then y exchange of fields that carry hs halos on every side
+  // (coupler.h:785-855 at one rank): the y pass spans the x halos, so the
+  // corner halos wrap in both directions.
+  template <class T>
+  void halo_exchange(MultiField<T, 3> &fields, int hs) const {
+    for (int f = 0; f < fields.get_num_fields(); f++) {
+      auto a = fields.get_field(f);
+      int nzl = a.extent(0) - 2 * hs, nyl = a.extent(1) - 2 * hs, nxl = a.extent(2) - 2 * hs;
+      for (int k = 0; k < nzl; k++)
+        for (int j = 0; j < nyl; j++)
+          for (int ii = 0; ii < hs; ii++) {
+            a(hs + k, hs + j, ii) = a(hs + k, hs + j, nxl + ii);
+            a(hs + k, hs + j, nxl + hs + ii) = a(hs + k, hs + j, hs + ii);
+          }
+      for (int k = 0; k < nzl; k++)
+        for (int jj = 0; jj < hs; jj++)
+          for (int i = 0; i < nxl + 2 * hs; i++) {
+            a(hs + k, jj, i) = a(hs + k, nyl + jj, i);
+            a(hs + k, nyl + hs + jj, i) = a(hs + k, hs + jj, i);
+          }
+    }
   }
 
   template <class T>

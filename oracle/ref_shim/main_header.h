@@ -196,8 +196,22 @@ struct SimpleBounds {
   template <class... I>
   SimpleBounds(I... d) : n{int(d)...} { static_assert(sizeof...(I) == N, "bounds rank"); }
 };
+// Bounds: each dimension is a count n (indices 0..n-1) or an inclusive
+// range {lo, hi} (yakl's LBnd without stride).
+struct LBnd {
+  int l, u;
+  LBnd(int n) : l(0), u(n - 1) {}
+  LBnd(size_t n) : l(0), u(int(n) - 1) {}
+  LBnd(std::initializer_list<int> b) : l(*b.begin()), u(*(b.begin() + 1)) {}
+};
 template <int N>
-using Bounds = SimpleBounds<N>;
+struct Bounds {
+  LBnd b[N];
+  Bounds(LBnd a) : b{a} {}
+  Bounds(LBnd a, LBnd c) : b{a, c} {}
+  Bounds(LBnd a, LBnd c, LBnd d) : b{a, c, d} {}
+  Bounds(LBnd a, LBnd c, LBnd d, LBnd e) : b{a, c, d, e} {}
+};
 
 template <class F>
 void parallel_for(const char *, int n, F const &f) {
@@ -231,6 +245,26 @@ void parallel_for(const char *, SimpleBounds<4> const &b, F const &f) {
 }
 template <class F, int N>
 void parallel_for(SimpleBounds<N> const &b, F const &f) { parallel_for("", b, f); }
+template <class F>
+void parallel_for(const char *, Bounds<1> const &b, F const &f) {
+#pragma omp parallel for
+  for (int i0 = b.b[0].l; i0 <= b.b[0].u; i0++) f(i0);
+}
+template <class F>
+void parallel_for(const char *, Bounds<2> const &b, F const &f) {
+#pragma omp parallel for collapse(2)
+  for (int i0 = b.b[0].l; i0 <= b.b[0].u; i0++)
+    for (int i1 = b.b[1].l; i1 <= b.b[1].u; i1++) f(i0, i1);
+}
+template <class F>
+void parallel_for(const char *, Bounds<3> const &b, F const &f) {
+#pragma omp parallel for collapse(2)
+  for (int i0 = b.b[0].l; i0 <= b.b[0].u; i0++)
+    for (int i1 = b.b[1].l; i1 <= b.b[1].u; i1++)
+      for (int i2 = b.b[2].l; i2 <= b.b[2].u; i2++) f(i0, i1, i2);
+}
+template <class F, int N>
+void parallel_for(Bounds<N> const &b, F const &f) { parallel_for("", b, f); }
 }  // namespace c
 
 namespace intrinsics {

@@ -285,3 +285,26 @@ CONFIGS = {
     "abl_neutral": abl_neutral,
     "urban_canopy": urban_canopy,
 }
+
+
+def immersed_halos(case: Case, roughness: float = 0.1, surface_temp: float = 0.0, immersed_temp: float = 0.0):
+    """The one-cell-halo immersed arrays that the physics modules read
+    (immersed_proportion_halos, immersed_roughness_halos,
+    immersed_temp_halos), built as the drivers' init does (sc_init.h:52-89,
+    727-768): interior proportion from the case, roughness everywhere
+    `roughness`, immersed temperature `immersed_temp`; periodic x/y halos
+    (corners wrap in both); the bottom z halo is the ground (proportion 1,
+    surface roughness, surface temperature), the top z halo is empty.
+    Returns three (nz+2, ny+2, nx+2) arrays."""
+    nz, ny, nx = case.nz, case.ny, case.nx
+    interior = [np.asarray(case.immersed_proportion, dtype=np.float64), np.full((nz, ny, nx), roughness),
+                np.full((nz, ny, nx), immersed_temp)]
+    bottom = [1.0, roughness, surface_temp]
+    out = []
+    for a, b in zip(interior, bottom):
+        h = np.zeros((nz + 2, ny + 2, nx + 2))
+        h[1:-1] = np.pad(a, ((0, 0), (1, 1), (1, 1)), mode="wrap")
+        h[0] = b
+        h[-1] = 0.0
+        out.append(np.ascontiguousarray(h))
+    return tuple(out)

@@ -1,0 +1,93 @@
+/* pu_physics.h -- C ABI of the B200 implementations of the physics modules
+ * that the boundary-layer drivers run beside the dycore every dt_phys
+ * (abl_neutral.cpp:93-104 of the reference):
+ *
+ *   pu_les_apply            modules::LES_Closure::apply          les_closure.h:30-320
+ *   pu_sponge_layer         modules::sponge_layer                sponge_layer.h:7-62
+ *   pu_geostrophic_forcing  modules::geostrophic_wind_forcing    geostrophic_wind_forcing.h:7-42
+ *   pu_surface_fluxes       modules::apply_surface_fluxes        surface_flux.h:9-125
+ *
+ * The reference's modules read their options and the immersed halo arrays
+ * from the coupler; here a pu_physics handle holds them (created once, like
+ * the arrays the drivers' init registers, sc_init.h:727-768) and each call
+ * takes the coupler arrays as a pu_state_view (pu_dycore.h): density_dry,
+ * uvel, vvel, wvel, temp and the tracers in coupler order, C-order
+ * (nz,ny,nx) doubles, host or device memory.  Arithmetic is FP64 as in the
+ * reference.  Every call returns PU_OK or a PU_ERR_* code (pu_last_error()),
+ * where the reference aborts.  Calls on one handle are ordered on its stream
+ * and are asynchronous for device views; pu_physics_synchronize waits.
+ */
+#ifndef PU_PHYSICS_H
+#define PU_PHYSICS_H
+
+#include "pu_dycore.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pu_physics pu_physics;
+
+typedef struct pu_physics_config {
+  int nx, ny, nz;
+  double dx, dy, dz;
+  int ntracers;                            /* coupler tracers, including TKE */
+  int tracer_diffuse[PU_MAX_TRACERS];      /* get_tracer_info(..., diffuse) */
+  int idTKE;                               /* index of the "TKE" tracer (mass-weighted TKE), or -1 */
+  double R_d, gamma_d, C0, grav;           /* coupler options */
+  int enable_gravity;
+  double kinematic_viscosity;              /* option "kinematic_viscosity" (default 0) */
+  int dns;                                 /* option "dns" (default false) */
+  double les_total_mult, les_dissipation_mult, les_shear_prod_mult; /* defaults 1 */
+  int bc_x, bc_y, bc_z;                    /* pu_bc */
+  int device;
+  void *stream;                            /* cudaStream_t, or NULL for the legacy default stream */
+} pu_physics_config;
+
+/* Creates a handle.  imm_prop_h, imm_rough_h, imm_temp_h are the
+ * immersed_proportion_halos, immersed_roughness_halos and immersed_temp_halos
+ * arrays ((nz+2,ny+2,nx+2) doubles with one halo cell per side; mem is
+ * PU_MEM_HOST, PU_MEM_DEVICE or PU_MEM_AUTO); the handle keeps a device copy.
+ * Replaces the options and DataManager reads of the four modules. */
+int pu_physics_create(const pu_physics_config *cfg, const double *imm_prop_h, const double *imm_rough_h,
+                      const double *imm_temp_h, int mem, pu_physics **out);
+int pu_physics_destroy(pu_physics *h);
+
+/* LES_Closure::apply(coupler, dt) (les_closure.h:30-320): TKE closure,
+ * diffusive fluxes of momentum, theta, TKE and diffused tracers, TKE sources;
+ * updates uvel, vvel, wvel, temp, TKE and the diffused tracers in place.  The
+ * update reads neighbours, so the new values go to a device scratch first and
+ * are copied back (pu_les_apply_to avoids the copy). */
+int pu_les_apply(pu_physics *h, pu_state_view *v, double dt);
+/* The same update from `in` into `out` (device views, distinct arrays; the
+ * untouched fields -- density_dry and the non-diffused tracers other than
+ * TKE -- are not written). */
+int pu_les_apply_to(pu_physics *h, const pu_state_view *in, pu_state_view *out, double dt);
+
+/* sponge_layer(coupler, dt, time_scale, top_prop) (sponge_layer.h:7-62):
+ * relaxes u, v, temp toward their level means and w toward 0 in the top
+ * top_prop of the domain.  Level means are FP64 sums with Neumaier
+ * compensation. */
+int pu_sponge_layer(pu_physics *h, pu_state_view *v, double dt, double time_scale, double top_prop);
+
+/* geostrophic_wind_forcing(coupler, dt, lat_g, u_g, v_g)
+ * (geostrophic_wind_forcing.h:7-42). */
+int pu_geostrophic_forcing(pu_physics *h, pu_state_view *v, double dt, double lat_g, double u_g, double v_g);
+
+/* apply_surface_fluxes(coupler, dt) (surface_flux.h:9-125): log-law drag and
+ * heat flux from immersed face neighbours (the ground is the bottom halo). */
+int pu_surface_fluxes(pu_physics *h, pu_state_view *v, double dt);
+
+/* Waits for the handle's work. */
+int pu_physics_synchronize(pu_physics *h);
+
+/* Milliseconds of the last pu_les_apply* kernel (CUDA events on the
+ * handle's stream; the copy-back of pu_les_apply is not included), for
+ * benchmarks.  Synchronises. */
+int pu_physics_last_les_ms(pu_physics *h, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PU_PHYSICS_H */

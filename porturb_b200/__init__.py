@@ -1,5 +1,7 @@
 """B200-native dynamical core with the module API of portUrb's
-Dynamics_Euler_Stratified_WenoFV (order-9 WENO finite volume, SSPRK3).
+Dynamics_Euler_Stratified_WenoFV (order-9 WENO finite volume, SSPRK3), and
+the physics modules that run beside it in the boundary-layer drivers (LES
+closure, sponge layer, geostrophic forcing, surface fluxes).
 
 The compute path is libpu_dycore.so (porturb_b200/csrc, built by
 porturb_b200/build.py); this package holds its ctypes bindings, the host-side
@@ -9,5 +11,7 @@ from . import capi, cases  # noqa: F401
 from .capi import PortUrbError  # noqa: F401
 from .dycore import (Coupler, Dycore, Dynamics_Euler_Stratified_WenoFV, assign_coupler_state,  # noqa: F401
                      case_coupler)
+from .physics import (LES_Closure, Physics, apply_surface_fluxes, geostrophic_wind_forcing,  # noqa: F401
+                      sponge_layer)
 
 __version__ = "0.1.0"

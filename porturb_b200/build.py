@@ -36,7 +36,8 @@ def _sources_mtime() -> float:
     for fn in os.listdir(CSRC):
         if fn.endswith((".cu", ".cuh", ".h")):
             m = max(m, os.path.getmtime(os.path.join(CSRC, fn)))
-    m = max(m, os.path.getmtime(os.path.join(HERE, "..", "include", "pu_dycore.h")))
+    for hdr in ("pu_dycore.h", "pu_physics.h"):
+        m = max(m, os.path.getmtime(os.path.join(HERE, "..", "include", hdr)))
     return m
 
 
@@ -65,7 +66,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_report: bool = False
         cmd = [nvcc()] + NVFLAGS + extra + ["-DPU_REAL=%s" % real, "-DPU_NTR=%d" % ntr, "-DPU_TAG=%s" % tag,
                                             "-c", os.path.join(CSRC, "impl_inst.cu"), "-o", obj]
         jobs.append((obj, cmd))
-    for src in ("pu_dycore", "pu_noalloc"):
+    for src in ("pu_dycore", "pu_noalloc", "physics"):
         jobs.append((os.path.join(OBJDIR, src + ".o"),
                      [nvcc()] + NVFLAGS + extra + ["-c", os.path.join(CSRC, src + ".cu"), "-o",
                                                    os.path.join(OBJDIR, src + ".o")]))

@@ -69,6 +69,18 @@ class pu_learn_stats(C.Structure):
 PU_PROFILE_KINDS = 3
 
 
+class pu_physics_config(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+                ("ntracers", C.c_int), ("tracer_diffuse", C.c_int * PU_MAX_TRACERS), ("idTKE", C.c_int),
+                ("R_d", C.c_double), ("gamma_d", C.c_double), ("C0", C.c_double), ("grav", C.c_double),
+                ("enable_gravity", C.c_int), ("kinematic_viscosity", C.c_double), ("dns", C.c_int),
+                ("les_total_mult", C.c_double), ("les_dissipation_mult", C.c_double),
+                ("les_shear_prod_mult", C.c_double),
+                ("bc_x", C.c_int), ("bc_y", C.c_int), ("bc_z", C.c_int),
+                ("device", C.c_int), ("stream", C.c_void_p)]
+
+
 class pu_profile(C.Structure):
     _fields_ = [("ms", C.c_double * PU_PROFILE_KINDS), ("launches", C.c_longlong * PU_PROFILE_KINDS)]
 
@@ -108,6 +120,16 @@ SIGNATURES = {
     "pu_dycore_profile_read": (_I, [_P, C.POINTER(pu_profile)]),
     "pu_dycore_time_step_noalloc": (_I, [C.POINTER(pu_config), _P, _P, _P, C.POINTER(pu_state_view), _D,
                                          C.POINTER(_I)]),
+    # include/pu_physics.h
+    "pu_physics_create": (_I, [C.POINTER(pu_physics_config), _P, _P, _P, _I, C.POINTER(C.c_void_p)]),
+    "pu_physics_destroy": (_I, [_P]),
+    "pu_les_apply": (_I, [_P, C.POINTER(pu_state_view), _D]),
+    "pu_les_apply_to": (_I, [_P, C.POINTER(pu_state_view), C.POINTER(pu_state_view), _D]),
+    "pu_sponge_layer": (_I, [_P, C.POINTER(pu_state_view), _D, _D, _D]),
+    "pu_geostrophic_forcing": (_I, [_P, C.POINTER(pu_state_view), _D, _D, _D, _D]),
+    "pu_surface_fluxes": (_I, [_P, C.POINTER(pu_state_view), _D]),
+    "pu_physics_synchronize": (_I, [_P]),
+    "pu_physics_last_les_ms": (_I, [_P, C.POINTER(_D)]),
 }
 PU_NOALLOC_SCRATCH_BYTES = 64 << 20
 

@@ -21,6 +21,9 @@ tracers water_vapor + TKE), one JSON line on rank 0.
 * learned: the learned-weight form on the same state and timed region,
   after harvesting 2^21 stencils from it and training the network on the GPU
   (3000 Adam steps, batch 16384); kernel times and the fallback fraction.
+* physics: the modules the boundary-layer driver runs beside the dycore
+  every dt_phys (geostrophic forcing, sponge, surface fluxes, LES closure;
+  FP64 as the reference) on device coupler arrays of the same workload.
 * Multi-GPU: the dycore is not domain-decomposed here; N ranks run N
   independent replicas (ensemble members) with no collective in the data
   path (weak scaling).
@@ -45,6 +48,57 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
 WORKLOAD = dict(nx=256, ny=256, nz=128, dx=10.0)
 DYN_CYCLE = 10
 LEARNED_THRESHOLD = 0.5
+
+
+def physics_modules(case, stream, world, reps=10):
+    """The modules the boundary-layer driver runs beside the dycore every
+    dt_phys (geostrophic forcing, sponge, surface fluxes, LES closure) on
+    device coupler arrays of the same workload: CUDA-event time per call and,
+    for the LES kernel (the out-of-place form, no copy-back), algorithmic
+    HBM bytes over its time."""
+    import torch
+    from porturb_b200.physics import Physics
+    ph = Physics.from_case(case, stream=stream.cuda_stream, device=torch.cuda.current_device())
+    rd, u, v, w, T, trc = [np.ascontiguousarray(a) for a in case.coupler_arrays(perturbed=True)]
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    A = [dev(x) for x in (rd, u, v, w, T)]
+    At = [dev(trc[t]) for t in range(trc.shape[0])]
+    B = [torch.empty_like(x) for x in A]
+    Bt = [torch.empty_like(x) for x in At]
+    dt = 0.1
+    N = case.ncells
+    nd = sum(1 for t in case.tracers if t.diffuse and t.name != "TKE")
+    out = {}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        ph.les_to(tuple(A) + (At,), tuple(B) + (Bt,), dt)
+    ph.synchronize()
+    les_ms = []
+    for _ in range(reps):
+        ph.les_to(tuple(A) + (At,), tuple(B) + (Bt,), dt)
+        les_ms.append(ph.last_les_ms())
+    les_ms = reduce_max(float(np.median(les_ms)), world)
+    # read rho_d, u, v, w, T, TKE, diffused tracers and the immersed proportion;
+    # write u, v, w, T, TKE, diffused tracers (FP64)
+    les_bytes = 8.0 * N * ((7 + nd) + (5 + nd))
+    out["les_kernel_ms"] = les_ms
+    out["les_gbs"] = les_bytes / (les_ms / 1e3) / 1e9
+    calls = (("les", (dt,)), ("sponge", (dt, 100 * dt, 300.0 / case.zlen)),
+             ("geostrophic", (dt, 43.29, 10.0, 0.0)), ("surface_fluxes", (dt,)))
+    for name, args in calls:
+        getattr(ph, name)(*A, At, *args)
+        ph.synchronize()
+        ev0.record(stream)
+        for _ in range(reps):
+            getattr(ph, name)(*A, At, *args)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        out[name + "_ms"] = reduce_max(ev0.elapsed_time(ev1) / reps, world)
+    out["dtype"] = "f64"
+    out["note"] = ("les_ms includes the copy-back of the in-place call; les_kernel_ms is the fused kernel alone; "
+                   "FP64 pow/sqrt/division bound, not HBM bound")
+    ph.close()
+    return out
 
 
 def measured_peaks():
@@ -210,6 +264,7 @@ def main():
     ap.add_argument("--e2e-calls", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-physics", action="store_true")
     args = ap.parse_args()
     world, rank, local = setup_dist()
     if args.impl == "reference":
@@ -281,6 +336,8 @@ def main():
 
     # Learned-weight form: network trained on stencils harvested from this
     # run's own state (GPU training kernels), then the same timed region.
+    physics = None if args.no_physics else physics_modules(case, stream, world)
+
     learned = None
     if not args.no_learned:
         g.learned_harvest(1 << 21, seed=1 + rank)
@@ -356,6 +413,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clk,
             "learned": learned,
+            "physics": physics,
         }
         print(json.dumps(line), flush=True)
     g.close()

@@ -67,13 +67,13 @@ class Physics:
         self.h = h
 
     @classmethod
-    def from_case(cls, case, halos=None, **options):
+    def from_case(cls, case, halos=None, device=0, stream=None, **options):
         from . import cases as _cases
         opts = dict(case.options)
         opts.update(options)
         halos = halos if halos is not None else _cases.immersed_halos(case)
         return cls(case.nx, case.ny, case.nz, case.xlen / case.nx, case.ylen / case.ny, case.zlen / case.nz,
-                   [(t.name, t.diffuse) for t in case.tracers], opts, halos)
+                   [(t.name, t.diffuse) for t in case.tracers], opts, halos, device=device, stream=stream)
 
     def close(self):
         if getattr(self, "h", None):

@@ -5,8 +5,10 @@
 
 Plain mode advances the FP32 (or --precision f64) dycore; --learned first
 harvests stencils from the initial state, trains the network on the GPU and
-then advances with learned weights.  Prints one JSON line with the per-kernel
-CUDA-event times and, in learned mode, the fallback fraction.
+then advances with learned weights; --modules times the physics modules
+(LES closure, sponge, geostrophic forcing, surface fluxes) instead.  Prints
+one JSON line with the per-kernel CUDA-event times and, in learned mode, the
+fallback fraction.
 """
 from __future__ import annotations
 
@@ -26,6 +28,35 @@ CASES = {
 }
 
 
+def run_modules(case, a):
+    """Each physics module `steps` times on device copies of the coupler
+    arrays (FP64); the LES closure out of place (kernel time by CUDA events)."""
+    import torch
+    from .physics import Physics
+    ph = Physics.from_case(case)
+    rd, u, v, w, T, trc = [np.ascontiguousarray(x) for x in case.coupler_arrays(perturbed=True)]
+    dev = lambda x: torch.from_numpy(np.ascontiguousarray(x)).cuda()
+    A = [dev(x) for x in (rd, u, v, w, T)]
+    At = [dev(trc[t]) for t in range(trc.shape[0])]
+    B = [torch.empty_like(x) for x in A]
+    Bt = [torch.empty_like(x) for x in At]
+    dt = 0.1
+    les_ms = []
+    for _ in range(a.steps):
+        ph.les_to(tuple(A) + (At,), tuple(B) + (Bt,), dt)
+        les_ms.append(ph.last_les_ms())
+    out = {"case": a.case, "grid": [a.nx, a.ny, a.nz], "steps": a.steps, "les_kernel_ms": les_ms}
+    for name, args in (("sponge", (dt, 100 * dt, 0.25)), ("geostrophic", (dt, 43.29, 10.0, 0.0)),
+                       ("surface_fluxes", (dt,))):
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            getattr(ph, name)(*A, At, *args)
+        ph.synchronize()
+        out[name + "_ms"] = (time.perf_counter() - t0) * 1e3 / max(a.steps, 1)
+    ph.close()
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=sorted(CASES))
@@ -38,9 +69,15 @@ def main(argv=None):
     ap.add_argument("--harvest", type=int, default=1 << 18)
     ap.add_argument("--train-steps", type=int, default=300)
     ap.add_argument("--threshold", type=float, default=0.5)
+    ap.add_argument("--modules", action="store_true",
+                    help="time the physics modules (LES closure, sponge, geostrophic forcing, surface fluxes) "
+                         "on the case's coupler arrays instead of dycore steps")
     a = ap.parse_args(argv)
 
     case = CASES[a.case](a)
+    if a.modules:
+        print(json.dumps(run_modules(case, a)), flush=True)
+        return
     g = Dycore.from_case(case, precision=a.precision)
     rd, u, v, w, T, trc = [np.ascontiguousarray(x) for x in case.coupler_arrays(perturbed=True)]
     prop = np.ascontiguousarray(case.immersed_proportion)

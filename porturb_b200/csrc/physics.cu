@@ -45,11 +45,13 @@ struct Grid {
   const double *prop;   // immersed_proportion_halos (nz+2, ny+2, nx+2)
 };
 
+// q[t]: the t-th diffused tracer (resolved on the host, so the kernels index
+// it with compile-time constants only).
 struct In {
-  const double *rd, *u, *v, *w, *T, *tke, *q[PU_MAX_TRACERS];
+  const double *rd, *u, *v, *w, *T, *tke, *q[3];
 };
 struct Out {
-  double *u, *v, *w, *T, *tke, *q[PU_MAX_TRACERS];
+  double *u, *v, *w, *T, *tke, *q[3];
 };
 
 __device__ __forceinline__ int wrapi(int i, int n) {
@@ -73,8 +75,7 @@ struct Les {
 // halo of interior rows, solid walls copy the edge level with w = 0 and an
 // isentropic density, periodic z wraps.
 template <int ND>
-__device__ void load_plane(const Grid &G, const In &in, int p, int i0, int j0, const int (&qi)[ND + 1], double *ring,
-                           uint8_t *flag) {
+__device__ void load_plane(const Grid &G, const In &in, int p, int i0, int j0, double *ring, uint8_t *flag) {
   constexpr int F = Les<ND>::F;
   const int nx = G.nx, ny = G.ny, nz = G.nz;
   for (int c = threadIdx.x; c < HP; c += NT) {
@@ -109,7 +110,7 @@ __device__ void load_plane(const Grid &G, const In &in, int p, int i0, int j0, c
     val[iT] = th;
     val[iK] = fmax(0.0, in.tke[q] / rd);
 #pragma unroll
-    for (int t = 0; t < ND; t++) val[6 + t] = in.q[qi[t]][q] / rd;
+    for (int t = 0; t < ND; t++) val[6 + t] = in.q[t][q] / rd;
     if (zhalo) {
       const double g = G.gravity ? G.grav : 0.0;
       const double rho0_gm1 = pow(rd, G.gamma - 1), theta0_g = pow(th, G.gamma);
@@ -233,21 +234,14 @@ __device__ __forceinline__ double tke_source(const Grid &G, const double *ring, 
 __device__ __forceinline__ int slot_of(int p) { return ((p % 3) + 3) % 3; }
 
 template <int ND>
-__global__ void __launch_bounds__(NT) k_les(const Grid G, const In in, const Out out, const int4 qidx, double dt,
-                                            double vhx, double vhy, double vhz) {
+__global__ void __launch_bounds__(NT) k_les(const Grid G, const In in, const Out out, double dt, double vhx,
+                                            double vhy, double vhz) {
   constexpr int F = Les<ND>::F, NF = Les<ND>::NF;
   extern __shared__ __align__(16) unsigned char smem[];
   double *ring = reinterpret_cast<double *>(smem);                        // [3][F][HP]
   double *fx = ring + 3 * F * HP;                                          // [NF][TY][TX+1]
   double *fy = fx + NF * TY * (TX + 1);                                    // [NF][TY+1][TX]
   uint8_t *flag = reinterpret_cast<uint8_t *>(fy + NF * (TY + 1) * TX);   // [3][HP]
-  int qi[ND + 1];
-  {
-    const int qa[4] = {qidx.x, qidx.y, qidx.z, qidx.w};
-#pragma unroll
-    for (int t = 0; t < ND; t++) qi[t] = qa[t];
-    qi[ND] = 0;
-  }
   const int tid = threadIdx.x, tj = tid / TX, ti = tid % TX;
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   const int k0 = blockIdx.z * KC, k1 = min(G.nz, k0 + KC);
@@ -255,7 +249,7 @@ __global__ void __launch_bounds__(NT) k_les(const Grid G, const In in, const Out
   const bool live = i < G.nx && j < G.ny;
   const int oc = (tj + 1) * HX + (ti + 1);   // this column's offset in the halo tile
   for (int p = k0 - 1; p <= k0 + 1; p++)
-    load_plane<ND>(G, in, p, i0, j0, qi, ring + slot_of(p) * F * HP, flag + slot_of(p) * HP);
+    load_plane<ND>(G, in, p, i0, j0, ring + slot_of(p) * F * HP, flag + slot_of(p) * HP);
   __syncthreads();
   double Fb[NF];   // flux through the bottom face of the current cell
   face_flux<ND, 2>(G, ring, flag, slot_of(k0 - 1), tj + 1, ti + 1, slot_of(k0), tj + 1, ti + 1, 0, 0, vhz, Fb);
@@ -284,7 +278,7 @@ __global__ void __launch_bounds__(NT) k_les(const Grid G, const In in, const Out
     for (int f = 0; f < F; f++) cell[f] = ring[(s * F + f) * HP + oc];
     __syncthreads();   // face fluxes visible; plane k-1 no longer read
     // The next level's upper plane (k+2 <= k1 <= nz) into the slot of level k-1.
-    if (k + 1 < k1) load_plane<ND>(G, in, k + 2, i0, j0, qi, ring + slot_of(k + 2) * F * HP, flag + slot_of(k + 2) * HP);
+    if (k + 1 < k1) load_plane<ND>(G, in, k + 2, i0, j0, ring + slot_of(k + 2) * F * HP, flag + slot_of(k + 2) * HP);
     if (live) {
       double tend[NF];
 #pragma unroll
@@ -302,7 +296,7 @@ __global__ void __launch_bounds__(NT) k_les(const Grid G, const In in, const Out
       out.T[q] = G.C0 * pow(cell[iT] * rho + dt * tend[3], G.gamma) / (rho * G.R_d);
       out.tke[q] = fmax(0.0, cell[iK] * rho + dt * tend[4]);
 #pragma unroll
-      for (int t = 0; t < ND; t++) out.q[qi[t]][q] = cell[6 + t] * rho + dt * tend[5 + t];
+      for (int t = 0; t < ND; t++) out.q[t][q] = cell[6 + t] * rho + dt * tend[5 + t];
     }
 #pragma unroll
     for (int v = 0; v < NF; v++) Fb[v] = Ft[v];
@@ -551,9 +545,8 @@ int launch_les(pu_physics &h, const In &in, const Out &out, double dt) {
   dim3 grid((h.cfg.nx + TX - 1) / TX, (h.cfg.ny + TY - 1) / TY, (h.cfg.nz + KC - 1) / KC);
   const double vhx = 0.5 * (0.25 * h.cfg.dx * h.cfg.dx / dt), vhy = 0.5 * (0.25 * h.cfg.dy * h.cfg.dy / dt),
                vhz = 0.5 * (0.25 * h.cfg.dz * h.cfg.dz / dt);
-  const int4 q = make_int4(h.qidx[0], h.qidx[1], h.qidx[2], h.qidx[3]);
   cudaEventRecord(h.e0, h.st);
-  k_les<ND><<<grid, NT, bytes, h.st>>>(G, in, out, q, dt, vhx, vhy, vhz);
+  k_les<ND><<<grid, NT, bytes, h.st>>>(G, in, out, dt, vhx, vhy, vhz);
   cudaEventRecord(h.e1, h.st);
   PH_CK(cudaGetLastError());
   return PU_OK;
@@ -576,7 +569,7 @@ In make_in(const pu_physics &h, double *const (&d)[5 + PU_MAX_TRACERS]) {
   in.w = d[3];
   in.T = d[4];
   in.tke = d[5 + h.cfg.idTKE];
-  for (int t = 0; t < PU_MAX_TRACERS; t++) in.q[t] = t < h.cfg.ntracers ? d[5 + t] : nullptr;
+  for (int t = 0; t < 3; t++) in.q[t] = t < h.nd ? d[5 + h.qidx[t]] : nullptr;
   return in;
 }
 
@@ -587,7 +580,7 @@ Out make_out(const pu_physics &h, double *const (&d)[5 + PU_MAX_TRACERS]) {
   o.w = d[3];
   o.T = d[4];
   o.tke = d[5 + h.cfg.idTKE];
-  for (int t = 0; t < PU_MAX_TRACERS; t++) o.q[t] = t < h.cfg.ntracers ? d[5 + t] : nullptr;
+  for (int t = 0; t < 3; t++) o.q[t] = t < h.nd ? d[5 + h.qidx[t]] : nullptr;
   return o;
 }
 

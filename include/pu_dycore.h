@@ -163,6 +163,16 @@ int pu_dycore_set_hydrostasis(pu_dycore *h, const double *dens_cells, const doub
 /* FP64 compensated global integrals of the resident state.  Synchronous. */
 int pu_dycore_diagnostics(pu_dycore *h, pu_diag *out);
 
+/* The fields the dycore adds to every output/restart file (its write hook,
+ * dynamics_rk.h:1193-1233): density_pert = rho - hy_dens_cells,
+ * theta_pert = rho*theta/rho - hy_theta_cells and
+ * pressure_pert = C0*(rho*theta)^gamma - hy_pressure_cells, formed from the
+ * coupler arrays v as convert_coupler_to_dynamics forms rho and rho*theta
+ * (dynamics_rk.h:1304-1352), FP64, (nz,ny,nx) each; outputs in memory `mem`
+ * (PU_MEM_HOST, PU_MEM_DEVICE or PU_MEM_AUTO).  Synchronous. */
+int pu_dycore_perturbations(pu_dycore *h, const pu_state_view *v, double *density_pert, double *theta_pert,
+                            double *pressure_pert, int mem);
+
 /* Waits for all work of the handle; returns PU_ERR_NONFINITE if a step
  * produced a non-finite value since the last check. */
 int pu_dycore_synchronize(pu_dycore *h);

@@ -106,6 +106,7 @@ SIGNATURES = {
     "pu_dycore_set_hydrostasis": (_I, [_P, _P, _P, _P]),
     "pu_dycore_diagnostics": (_I, [_P, C.POINTER(pu_diag)]),
     "pu_dycore_synchronize": (_I, [_P]),
+    "pu_dycore_perturbations": (_I, [_P, C.POINTER(pu_state_view), _P, _P, _P, _I]),
     "pu_dycore_kernel_launches": (C.c_longlong, [_P]),
     "pu_dycore_learned_harvest": (_I, [_P, C.c_longlong, C.c_ulonglong]),
     "pu_dycore_learned_train": (_I, [_P, _I, _I, _D, C.c_ulonglong, C.POINTER(pu_learn_stats)]),

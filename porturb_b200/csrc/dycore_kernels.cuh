@@ -752,6 +752,30 @@ __global__ void k_store_coupler(CouplerOut co, Thermo th, const double *__restri
   for (int t = 0; t < NTR; t++) co.tr[t][idx] = double(s[(5 + t) * N + idx]);
 }
 
+// The perturbation fields of the dycore's output hook (dynamics_rk.h:1212-1232)
+// from coupler arrays: rho, theta = rho*theta/rho and p = C0 (rho theta)^gamma
+// as convert_coupler_to_dynamics forms them (dynamics_rk.h:1304-1352), minus
+// the hydrostatic cell profiles (cells: [3][nz + 2*HS], density, theta,
+// pressure).  out: [3][N] density_pert, theta_pert, pressure_pert (FP64).
+template <int NTR>
+__global__ void k_perturbations(CouplerPtrs cp, Thermo th, const double *__restrict__ cells, int nzh, size_t N,
+                                size_t NP, double *__restrict__ out) {
+  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= N) return;
+  const int kh = int(idx / NP) + HS;
+  const double rd = cp.rho_d[idx], temp = cp.T[idx];
+  const double rho_v = cp.tr[th.idWV][idx];
+  const double press = rd * th.R_d * temp + rho_v * th.R_v * temp;
+  double rho = rd;
+#pragma unroll
+  for (int t = 0; t < NTR; t++)
+    if ((th.adds_mass >> t) & 1u) rho += cp.tr[t][idx];
+  const double rt = rho * (pow(press / th.C0, 1. / th.gamma) / rho);
+  out[idx] = rho - cells[kh];
+  out[N + idx] = rt / rho - cells[nzh + kh];
+  out[2 * N + idx] = th.C0 * pow(rt, th.gamma) - cells[2 * nzh + kh];
+}
+
 // Absolute conserved variables <-> perturbation storage.
 template <class R, int NTR>
 __global__ void k_get_conserved(const R *__restrict__ s, const double *__restrict__ rho_off,

@@ -336,6 +336,7 @@ struct ImplBase {
   virtual int set_conserved(const double *st, const double *tr, int mem) = 0;
   virtual int set_hydrostasis(const double *r, const double *t, const double *p) = 0;
   virtual int diagnostics(pu_diag *out) = 0;
+  virtual int perturbations(const pu_state_view *v, double *dens, double *theta, double *press, int mem) = 0;
 
   int check_err() {
     int h = 0;
@@ -776,6 +777,25 @@ struct Impl : ImplBase {
     PU_LAUNCHED();
     PU_CK(cudaStreamSynchronize(st));
     ml_n += n;
+    return PU_OK;
+  }
+
+  // density_pert, theta_pert, pressure_pert of the coupler arrays against the
+  // handle's cell profiles (the dycore's output hook).  Host outputs go
+  // through the stage buffer s[1] (idle between steps; S*N values of R hold
+  // 3*N doubles since S*sizeof(R) >= 24).
+  int perturbations(const pu_state_view *v, double *dens, double *theta, double *press, int mem) override {
+    CouplerPtrs cp;
+    PU_TRY(device_view(v, cp));
+    const bool dev = resolve_mem(mem, dens) == PU_MEM_DEVICE;
+    double *out = static_cast<double *>(s[1]);
+    k_perturbations<NTR><<<blocks(N, 256), 256, 0, st>>>(cp, thermo(), cells, nzh, N, NP, out);
+    PU_LAUNCHED();
+    double *dst[3] = {dens, theta, press};
+    for (int a = 0; a < 3; a++)
+      PU_CK(cudaMemcpyAsync(dst[a], out + size_t(a) * N, N * sizeof(double),
+                            dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    PU_CK(cudaStreamSynchronize(st));
     return PU_OK;
   }
 

@@ -238,6 +238,14 @@ int pu_dycore_diagnostics(pu_dycore *h, pu_diag *out) {
   return h->impl->diagnostics(out);
 }
 
+int pu_dycore_perturbations(pu_dycore *h, const pu_state_view *v, double *density_pert, double *theta_pert,
+                            double *pressure_pert, int mem) {
+  if (!h || !v || !density_pert || !theta_pert || !pressure_pert) return fail(PU_ERR_INVALID, "null argument");
+  if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
+  DeviceGuard g(h->device);
+  return h->impl->perturbations(v, density_pert, theta_pert, pressure_pert, mem);
+}
+
 int pu_dycore_synchronize(pu_dycore *h) {
   if (!h) return fail(PU_ERR_INVALID, "null handle");
   DeviceGuard g(h->device);

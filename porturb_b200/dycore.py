@@ -183,6 +183,16 @@ class Dycore:
         out["tracer_mass"] = [d.tracer_mass[t] for t in range(self.ntr)]
         return out
 
+    def perturbations(self, rho_d, u, v, w, T, tracers):
+        """(density_pert, theta_pert, pressure_pert) of coupler arrays against
+        the handle's cell profiles: the dycore's output fields
+        (dynamics_rk.h:1212-1232), float64 numpy arrays."""
+        view = make_view(rho_d, u, v, w, T, tracers)
+        out = [np.empty(self.shape) for _ in range(3)]
+        check(self.lib.pu_dycore_perturbations(self.h, C.byref(view), out[0].ctypes.data, out[1].ctypes.data,
+                                               out[2].ctypes.data, capi.PU_MEM_HOST))
+        return tuple(out)
+
     def kernel_launches(self) -> int:
         return int(self.lib.pu_dycore_kernel_launches(self.h))
 
@@ -262,6 +272,11 @@ class Coupler:
         self.nx = self.ny = self.nz = -1
         self.xlen = self.ylen = self.zlen = -1.0
         self.module_state: Dict[str, object] = {}
+        # output / restart registry (coupler.h:474-531)
+        self.file_counter = 0
+        self.output_vars: List[tuple] = []
+        self.write_output_modules: List = []
+        self.restart_modules: List = []
 
     # grid (coupler.h:132-341, one rank)
     def distribute_mpi_and_allocate_coupled_state(self, nz, ny_glob, nx_glob):
@@ -319,6 +334,24 @@ class Coupler:
             if t[0] == name:
                 return dict(desc=t[1], found=True, positive=t[2], adds_mass=t[3], diffuse=t[4])
         return dict(found=False)
+
+    # output and restart (coupler.h:474-723; porturb_b200/output.py)
+    def register_output_variable(self, name, dims, dtype=np.float64):
+        self.output_vars.append((name, dims, dtype))
+
+    def register_write_output_module(self, f):
+        self.write_output_modules.append(f)
+
+    def register_overwrite_with_restart_module(self, f):
+        self.restart_modules.append(f)
+
+    def write_output_file(self, prefix, verbose=False):
+        from .output import write_output_file
+        return write_output_file(self, prefix, verbose)
+
+    def overwrite_with_restart(self):
+        from .output import overwrite_with_restart
+        overwrite_with_restart(self)
 
     # data manager (DataManager.h:127-299)
     def register_and_allocate(self, name, desc, dims, dtype=np.float64):
@@ -418,6 +451,12 @@ class Dynamics_Euler_Stratified_WenoFV:
             dm[nm] = a.astype(np.float32)
         for nm, a in zip(("hy_dens_edges", "hy_theta_edges", "hy_pressure_edges"), edges):
             dm[nm] = a.astype(np.float32)
+        # Output and restart hooks (dynamics_rk.h:1191-1242).
+        from . import output
+        if coupler.entry_exists("immersed_proportion"):
+            coupler.register_output_variable("immersed_proportion", output.DIMS_3D)
+        coupler.register_write_output_module(output.dycore_write_hook(self._handle))
+        coupler.register_overwrite_with_restart_module(output.dycore_restart_hook(self._handle))
 
     def time_step(self, coupler, dt_phys) -> int:
         """dynamics_rk.h:103-137; returns the number of SSPRK3 cycles taken."""

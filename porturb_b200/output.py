@@ -14,8 +14,8 @@ variables, dimensions and types are the reference's:
   restart is not);
 * registered output variables (``Coupler.register_output_variable``);
 * whatever the registered write modules add (the dycore: ``z_halo``,
-  ``hy_*_cells`` float32, ``density_pert``, ``theta_pert``,
-  ``pressure_pert`` float64).
+  ``hy_*_cells`` float32 -- float64 with ``output_f64`` --, ``density_pert``,
+  ``theta_pert``, ``pressure_pert`` float64).
 
 ``overwrite_with_restart`` reads the state back from the file named by the
 option ``restart_file`` and runs the registered restart modules.
@@ -141,9 +141,13 @@ def dycore_write_hook(handle_of):
         h = handle_of(coupler)
         nzh = coupler.get_nz() + 2 * 4
         nc.create_dim("z_halo", nzh)
-        for name in ("hy_dens_cells", "hy_theta_cells", "hy_pressure_cells"):
-            nc.create_var(name, ("z_halo",), np.float32)
-            nc.write(_host(coupler.get(name)), name)
+        # float32 as the reference stores them; with output_f64 the handle's
+        # own profiles (FP64 in the FP64 build), so that a restart is exact.
+        f64 = coupler.get_option("output_f64", False)
+        cells, _ = h.get_hydrostasis()
+        for name, prof in zip(("hy_dens_cells", "hy_theta_cells", "hy_pressure_cells"), cells):
+            nc.create_var(name, ("z_halo",), np.float64 if f64 else np.float32)
+            nc.write(prof if f64 else _host(coupler.get(name)), name)
         arrays = [coupler.get(n) for n in ("density_dry", "uvel", "vvel", "wvel", "temp")]
         trc = [coupler.get(n) for n in coupler.get_tracer_names()]
         for name, data in zip(("density_pert", "theta_pert", "pressure_pert"), h.perturbations(*arrays, trc)):

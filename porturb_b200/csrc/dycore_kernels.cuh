@@ -26,12 +26,28 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "mlp_infer.cuh"
 #include "weno9.cuh"
 
 namespace pu {
 
+// Packed FP32 limiter (two stencils per FFMA2/FADD2/FMUL2) in the plain x/y
+// kernel; 0 keeps the scalar limiter (results are identical).  The z march
+// keeps the scalar limiter: packing pairs of fields there raises its
+// registers from ~125 to ~165 and the lost occupancy costs more (1.11 against
+// 1.10 ms per launch).
+#ifndef PU_PACKED_LIMITER
+#define PU_PACKED_LIMITER 1
+#endif
+// Minimum resident blocks per SM requested for the plain FP32 x/y kernel: 4
+// (64 registers) keeps 32 warps per SM with the packed limiter (measured on
+// the 256x256x128 boundary layer: 1.80 ms per launch against 2.05 ms uncapped
+// and 1.87 ms with the scalar limiter).
+#ifndef PU_XY_MIN_BLOCKS
+#define PU_XY_MIN_BLOCKS 4
+#endif
 // Minimum resident blocks per SM requested for the learned stencil kernels
 // (caps their registers: the network's operand fragments stay in registers).
 #ifndef PU_LEARNED_XY_MIN_BLOCKS
@@ -200,11 +216,41 @@ __device__ __forceinline__ int recon_learned(const Grid<float> &G, uint32_t *sW,
   return nq;
 }
 
+// Plain reconstruction of `total` stencils, two per thread and iteration
+// (stencils it and it+NT) with the packed FP32 limiter; per stencil the
+// result is bit-identical to weno9_edges.  Used when every stencil takes the
+// nonlinear limiter (weno_all).
+template <int NT, class Load, class Store>
+__device__ __forceinline__ void recon_packed(int total, Load load, Store store) {
+  for (int it = threadIdx.x; it < total; it += 2 * NT) {
+    const int it2 = it + NT;
+    const bool two = it2 < total;
+    float a[9], b[9];
+    unsigned ia, ib;
+    bool xa, xb;
+    load(it, a, ia, xa);
+    if (two) load(it2, b, ib, xb);
+    else {
+#pragma unroll
+      for (int m = 0; m < 9; m++) b[m] = a[m];
+      ib = ia;
+      xb = xa;
+    }
+    float2 s2[9], qL, qR;
+#pragma unroll
+    for (int m = 0; m < 9; m++) s2[m] = make_float2(a[m], b[m]);
+    weno9_edges2(s2, qL, qR, bool2{!xa, !xb}, bool2{((ia >> 3) & 1u) != 0, ((ib >> 3) & 1u) != 0},
+                 bool2{((ia >> 5) & 1u) != 0, ((ib >> 5) & 1u) != 0});
+    store(it, qL.x, qR.x);
+    if (two) store(it2, qL.y, qR.y);
+  }
+}
+
 // x/y fluxes and their divergence for one (x,y) tile of one level.
 // LEARNED (FP32, weno_all only): edges from the network's weights, with the
 // plain limiter as the fallback.
 template <class R, int NTR, int TX, int TY, bool IMM, bool LEARNED = false>
-__global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : 1) k_xy(const Grid<R> G, const R *__restrict__ sin, R *__restrict__ txy) {
+__global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (sizeof(R) == 4 ? PU_XY_MIN_BLOCKS : 1)) k_xy(const Grid<R> G, const R *__restrict__ sin, R *__restrict__ txy) {
   using Sh = XYShape<R, NTR, TX, TY, IMM, LEARNED>;
   constexpr int F = Sh::F, S = Sh::S, NT = Sh::NT, HX = Sh::HX, HY = Sh::HY, EN = Sh::EN, FN = Sh::FN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -270,9 +316,14 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : 1
     ER[f * EN + rem] = qR;
   };
   int n_fb = 0;
+  bool packed = false;
+  if constexpr (std::is_same<R, float>::value && PU_PACKED_LIMITER && !LEARNED) {
+    packed = G.weno_all != 0;
+    if (packed) recon_packed<NT>(F * Sh::EXN, load_x, store_x);
+  }
   if constexpr (LEARNED) {
     n_fb += recon_learned<NT>(G, sW, queue, qn, F * Sh::EXN, load_x, store_x);
-  } else {
+  } else if (!packed) {
     for (int it = tid; it < F * Sh::EXN; it += NT) {
       R s[9];
       unsigned imm;
@@ -343,6 +394,8 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : 1
     if constexpr (LEARNED) {
       __syncthreads();   // step 4 has read the flux buffer that holds the queue
       n_fb += recon_learned<NT>(G, sW, queue, qn + 1, F * Sh::EYN, load_y, store_y);
+    } else if (packed) {
+      if constexpr (std::is_same<R, float>::value) recon_packed<NT>(F * Sh::EYN, load_y, store_y);
     } else {
       for (int it = tid; it < F * Sh::EYN; it += NT) {
         R s[9];
@@ -600,8 +653,7 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : 1)
         n_learned += unsigned(F * 32 - cnt);
         n_fallback += unsigned(cnt);
       } else {
-#pragma unroll 1
-        for (int f = 0; f < F; f++) {
+        auto one_field = [&](int f) {
           R s[9];
 #pragma unroll
           for (int m = 0; m < 9; m++) s[m] = ring[sl[m] + f * NT];
@@ -611,7 +663,9 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : 1)
           else weno9_edges(s, qL, qR, !any10, (imm >> 3) & 1u, (imm >> 5) & 1u);
           eL[f * NT + tid] = qL;
           eRc[f * NT] = qR;
-        }
+        };
+#pragma unroll 1
+        for (int f = 0; f < F; f++) one_field(f);
       }
     }
     if (c > cstart || (wall && c == 0)) {

@@ -364,7 +364,14 @@ inline int resolve_mem(int mem, const void *p) {
 
 template <class R, int NTR>
 struct Impl : ImplBase {
-  static constexpr int XTX_BIG = 16, XTY_BIG = 16;   // x/y tile for ny >= 16
+#ifndef PU_XY_TILE_X
+#define PU_XY_TILE_X 16
+#endif
+#ifndef PU_XY_TILE_Y
+#define PU_XY_TILE_Y 16
+#endif
+  static constexpr int XTX_BIG = PU_XY_TILE_X, XTY_BIG = PU_XY_TILE_Y;   // x/y tile for ny >= 16
+  static constexpr int LTX = 16, LTY = 16;           // x/y tile of the learned form (ny >= 16)
   static constexpr int XTX_SM = 32, XTY_SM = 4;      // x/y tile for thin domains
   static constexpr int ZTX = 32, ZTY = 4;            // z-march columns per block
   LevelTables<R> lt{};
@@ -448,12 +455,10 @@ struct Impl : ImplBase {
     PU_CK(cudaFuncSetAttribute(k_z<R, NTR, ZTX, ZTY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(ZShape<R, NTR, ZTX, ZTY>::bytes)));
     if constexpr (std::is_same<R, float>::value) {
-      PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_BIG, XTY_BIG, false, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(XYShape<R, NTR, XTX_BIG, XTY_BIG, false, true>::bytes)));
-      PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_BIG, XTY_BIG, true, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(XYShape<R, NTR, XTX_BIG, XTY_BIG, true, true>::bytes)));
+      PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, LTX, LTY, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(XYShape<R, NTR, LTX, LTY, false, true>::bytes)));
+      PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, LTX, LTY, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(XYShape<R, NTR, LTX, LTY, true, true>::bytes)));
       PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_SM, XTY_SM, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(XYShape<R, NTR, XTX_SM, XTY_SM, false, true>::bytes)));
       PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_SM, XTY_SM, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -667,10 +672,14 @@ struct Impl : ImplBase {
       using Sh = XYShape<R, NTR, XTX_SM, XTY_SM, IMM, L>;
       dim3 g(blocks(cfg.nx, XTX_SM), blocks(cfg.ny, XTY_SM), cfg.nz);
       k_xy<R, NTR, XTX_SM, XTY_SM, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
+    } else if (L) {
+      using Sh = XYShape<R, NTR, LTX, LTY, IMM, L>;
+      dim3 g(blocks(cfg.nx, LTX), blocks(cfg.ny, LTY), cfg.nz);
+      k_xy<R, NTR, LTX, LTY, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
     } else {
-      using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM, L>;
+      using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM, false>;
       dim3 g(blocks(cfg.nx, XTX_BIG), blocks(cfg.ny, XTY_BIG), cfg.nz);
-      k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
+      k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
     }
     PU_LAUNCHED();
     prof_end(0, e0);

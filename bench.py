@@ -381,11 +381,12 @@ def main():
         alg_xy = 4.0 * S * N
         xy_avg_s = xy_ms / 1e3 / max(xy_n, 1)
         achieved = alg_xy / xy_avg_s / 1e9
-        traffic = None
+        traffic, tinfo = None, {}
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tpath):
             with open(tpath) as f:
-                traffic = json.load(f).get("k_xy_bytes_per_launch")
+                tinfo = json.load(f)
+            traffic = tinfo.get("k_xy_bytes_per_launch")
         cpu = None
         if not args.no_cpu_baseline:
             try:
@@ -404,7 +405,13 @@ def main():
             "roofline": {"kernel": "k_xy (x/y WENO + Riemann + divergence)", "bound": "hbm",
                          "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                          "traffic": traffic, "peak_source": peaks.get("source"),
-                         "note": "FP32-pipe bound; see profiles/ for FP32 pipe utilisation"},
+                         "note": "FP32-FMA-pipe bound (compute_roofline); the HBM fraction is reported from algorithmic bytes"},
+            "compute_roofline": {"kernel": "k_xy", "bound": "fp32 fma pipe",
+                                 "fma_pipe_frac": tinfo.get("k_xy_fma_pipe_frac"),
+                                 "issue_frac": tinfo.get("k_xy_issue_frac"),
+                                 "k_z_fma_pipe_frac": tinfo.get("k_z_fma_pipe_frac"),
+                                 "k_z_issue_frac": tinfo.get("k_z_issue_frac"),
+                                 "source": tinfo.get("source")},
             "kernel_ms": {"k_xy": xy_ms / max(xy_n, 1), "k_z": z_ms / max(z_n, 1),
                           "share_xy": xy_ms / max(xy_ms + z_ms, 1e-12)},
             "cpu_baseline": cpu,

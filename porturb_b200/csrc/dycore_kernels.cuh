@@ -48,6 +48,10 @@ namespace pu {
 #ifndef PU_XY_MIN_BLOCKS
 #define PU_XY_MIN_BLOCKS 4
 #endif
+// Minimum resident blocks per SM requested for the plain z march.
+#ifndef PU_Z_MIN_BLOCKS
+#define PU_Z_MIN_BLOCKS 1
+#endif
 // Minimum resident blocks per SM requested for the learned stencil kernels
 // (caps their registers: the network's operand fragments stay in registers).
 #ifndef PU_LEARNED_XY_MIN_BLOCKS
@@ -522,7 +526,7 @@ __device__ __forceinline__ void prims_of(const Grid<R> &G, const R (&q)[5 + NTR]
 // G.ml_jump, are queued per warp and reconstructed by the plain limiter after
 // the level's field loop, by all lanes of the warp.
 template <class R, int NTR, int TX, int TY, bool IMM, bool LEARNED = false>
-__global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : 1) k_z(const Grid<R> G, const R *__restrict__ sin, const R *sn, R *sout,
+__global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : (sizeof(R) == 4 ? PU_Z_MIN_BLOCKS : 1)) k_z(const Grid<R> G, const R *__restrict__ sin, const R *sn, R *sout,
                                               const R *__restrict__ txy, R a_n, R a_dt, int n_enforce,
                                               int kchunk) {
   constexpr int F = 6 + NTR, S = 5 + NTR, NT = TX * TY;

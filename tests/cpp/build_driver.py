@@ -8,16 +8,24 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 EXE = os.path.join(HERE, "_build", "dropin_driver")
+PHYS_EXE = os.path.join(HERE, "_build", "physics_driver")
 REF_CORE = "/root/reference/model/core"
 
 
+def _compile(src, exe, libdir):
+    cmd = ["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "porturb_b200", "cpp"),
+           "-I", os.path.join(ROOT, "oracle", "ref_shim"), "-I", os.path.join(ROOT, "include"), "-I", REF_CORE,
+           os.path.join(HERE, src), "-o", exe, "-L", libdir, "-lpu_dycore", "-Wl,-rpath," + libdir]
+    subprocess.run(cmd, check=True)
+
+
 def build(libdir):
+    """Builds both drivers (the dycore drop-in alone, and the boundary-layer
+    module chain); returns the dycore driver's path, or None without the
+    reference tree and without a prebuilt binary."""
     if not os.path.isdir(REF_CORE):
         return EXE if os.path.exists(EXE) else None
     os.makedirs(os.path.dirname(EXE), exist_ok=True)
-    cmd = ["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "porturb_b200", "cpp"),
-           "-I", os.path.join(ROOT, "oracle", "ref_shim"), "-I", os.path.join(ROOT, "include"), "-I", REF_CORE,
-           os.path.join(HERE, "dropin_driver.cpp"), "-o", EXE,
-           "-L", libdir, "-lpu_dycore", "-Wl,-rpath," + libdir]
-    subprocess.run(cmd, check=True)
+    _compile("dropin_driver.cpp", EXE, libdir)
+    _compile("physics_driver.cpp", PHYS_EXE, libdir)
     return EXE

@@ -62,3 +62,49 @@ def test_dropin_matches_python_front_end(tmp_path):
         g.time_step(*arrs[:5], trs, dt_phys)
     ref = np.concatenate([np.stack(arrs[:5]), np.stack(trs)])
     assert np.array_equal(out, ref)
+
+
+@pytest.mark.gpu
+def test_physics_dropin_chain_matches_python_front_end(tmp_path):
+    """The drop-in LES closure, sponge, geostrophic forcing and surface-flux
+    headers with the dycore, in the boundary-layer driver's order
+    (abl_neutral.cpp:93-104), give the same arrays as the same chain through
+    the Python API."""
+    from porturb_b200 import Dycore, cases
+    from porturb_b200.physics import Physics
+    build_driver()
+    exe = os.path.join(ROOT, "tests", "cpp", "_build", "physics_driver")
+    case = cases.abl_neutral(nx=32, ny=16, nz=24)
+    halos = cases.immersed_halos(case)
+    g = Dycore.from_case(case, precision="f32")
+    dt = 2 * g.compute_time_step()
+    o = case.options
+    lat_g, u_g, v_g, t_sp, top = 43.29, 10.0, 0.0, 100 * dt, 0.1
+    ncalls = 2
+    base = [np.asarray(a) for a in case.coupler_arrays(perturbed=False)]
+    pert = [np.asarray(a) for a in case.coupler_arrays(perturbed=True)]
+    with open(tmp_path / "in.bin", "wb") as f:
+        np.array([case.nx, case.ny, case.nz, ncalls], np.int32).tofile(f)
+        np.array([case.xlen, case.ylen, case.zlen, dt, o["R_d"], o["R_v"], o["cp_d"], o["gamma_d"], o["C0"],
+                  o["grav"], o["cfl"], lat_g, u_g, v_g, t_sp, top], np.float64).tofile(f)
+        for st in (base, pert):
+            np.concatenate([np.stack(st[:5]).ravel(), st[5][0].ravel()]).astype(np.float64).tofile(f)
+        np.concatenate([h.ravel() for h in halos]).tofile(f)
+    r = subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = np.fromfile(tmp_path / "out.bin", np.float64).reshape(7, case.nz, case.ny, case.nx)
+
+    rd, u, v, w, T, trc = [np.ascontiguousarray(a) for a in base]
+    g.init(rd, u, v, w, T, [np.ascontiguousarray(t) for t in trc], None)
+    a = [np.ascontiguousarray(x.copy()) for x in pert[:5]]
+    trs = [np.ascontiguousarray(t.copy()) for t in pert[5]]
+    ph = Physics.from_case(case, halos=halos)
+    for _ in range(ncalls):
+        ph.geostrophic(*a, trs, dt, lat_g, u_g, v_g)
+        g.time_step(*a, trs, dt)
+        ph.sponge(*a, trs, dt, t_sp, top)
+        ph.surface_fluxes(*a, trs, dt)
+        ph.les(*a, trs, dt)
+    ref = np.concatenate([np.stack(a), np.stack(trs)])
+    assert np.array_equal(out, ref)
+    assert not np.array_equal(ref[6], np.asarray(pert[5][1]))   # the closure changed TKE

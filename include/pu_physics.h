@@ -6,6 +6,11 @@
  *   pu_sponge_layer         modules::sponge_layer                sponge_layer.h:7-62
  *   pu_geostrophic_forcing  modules::geostrophic_wind_forcing    geostrophic_wind_forcing.h:7-42
  *   pu_surface_fluxes       modules::apply_surface_fluxes        surface_flux.h:9-125
+ *   pu_uniform_pg_wind_forcing         modules::uniform_pg_wind_forcing
+ *                                      uniform_pg_wind_forcing.h:6-40
+ *   pu_uniform_pg_wind_forcing_height  modules::uniform_pg_wind_forcing_height
+ *                                      uniform_pg_wind_forcing.h:43-82
+ *                                      (city.cpp:130-136, cubes_periodic.cpp:147-152)
  *
  * The reference's modules read their options and the immersed halo arrays
  * from the coupler; here a pu_physics handle holds them (created once, like
@@ -77,6 +82,37 @@ int pu_geostrophic_forcing(pu_physics *h, pu_state_view *v, double dt, double la
 /* apply_surface_fluxes(coupler, dt) (surface_flux.h:9-125): log-law drag and
  * heat flux from immersed face neighbours (the ground is the bottom halo). */
 int pu_surface_fluxes(pu_physics *h, pu_state_view *v, double dt);
+
+/* What uniform_pg_wind_forcing carries from call to call; the reference keeps
+ * it in the coupler options uniform_pg_wind_forcing_counter, _u0, _v0, _u and
+ * _v.  Zero-initialise it before the first call. */
+typedef struct pu_uniform_pg_state {
+  unsigned long long counter;
+  double u0, v0; /* domain means of u and v taken at counter 0 */
+  double u, v;   /* the latest domain means */
+} pu_uniform_pg_state;
+
+/* uniform_pg_wind_forcing(coupler, dt, tau, update_cycles)
+ * (uniform_pg_wind_forcing.h:6-40): when counter % update_cycles == 0 the
+ * domain means of uvel and vvel are taken into state->u, v (and u0, v0 on the
+ * first call); then every cell gets uvel += dt/tau*(u0-u), vvel +=
+ * dt/tau*(v0-v), and counter is incremented.  The means are FP64 sums with
+ * Neumaier compensation; a call that takes them synchronises the handle's
+ * stream.  PU_ERR_INVALID for update_cycles == 0 or tau <= 0 (the reference
+ * divides by them). */
+int pu_uniform_pg_wind_forcing(pu_physics *h, pu_state_view *v, double dt, double tau,
+                               unsigned long long update_cycles, pu_uniform_pg_state *state);
+
+/* uniform_pg_wind_forcing_height(coupler, dt, height, u0, v0, tau)
+ * (uniform_pg_wind_forcing.h:43-82): the mean wind at `height`, linear
+ * between the level means of the two levels whose centres bracket it, is
+ * relaxed toward (u0, v0): every cell gets uvel += dt/tau*(u0-u(height)),
+ * likewise v.  Above the top level centre the two lowest levels are
+ * extrapolated, as in the reference.  PU_ERR_INVALID when height is below
+ * the first level centre (the reference then reads level -1), nz < 2 or
+ * tau <= 0.  Asynchronous for device views. */
+int pu_uniform_pg_wind_forcing_height(pu_physics *h, pu_state_view *v, double dt, double height, double u0, double v0,
+                                      double tau);
 
 /* Waits for the handle's work. */
 int pu_physics_synchronize(pu_physics *h);

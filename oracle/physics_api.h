@@ -9,11 +9,15 @@
  *   sponge_layer                    sponge_layer.h:7-62
  *   geostrophic_wind_forcing        geostrophic_wind_forcing.h:7-42
  *   apply_surface_fluxes            surface_flux.h:9-125
+ *   uniform_pg_wind_forcing         uniform_pg_wind_forcing.h:6-40
+ *   uniform_pg_wind_forcing_height  uniform_pg_wind_forcing.h:43-82
  * All arrays are C-order doubles: coupler fields (nz,ny,nx), tracers
  * (ntr,nz,ny,nx) in coupler order, immersed halo arrays (nz+2,ny+2,nx+2) with
  * one halo cell on each side (immersed_proportion_halos,
  * immersed_roughness_halos, immersed_temp_halos of the drivers' init,
- * sc_init.h:727-768).  The calls update the coupler arrays in place. */
+ * sc_init.h:727-768).  The calls update the coupler arrays in place.
+ * *_uniform_pg carries st = {counter, u0, v0, u, v} (the coupler options
+ * uniform_pg_wind_forcing_counter, _u0, _v0, _u, _v) from call to call. */
 #pragma once
 
 #ifdef __cplusplus
@@ -44,6 +48,10 @@ int orc_phys_geostrophic(void *h, double *rho_d, double *u, double *v, double *w
                          double lat_g, double u_g, double v_g);
 int orc_phys_surface_fluxes(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
                             double dt);
+int orc_phys_uniform_pg(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc, double dt,
+                        double tau, unsigned long long update_cycles, double *st);
+int orc_phys_uniform_pg_height(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                               double dt, double height, double u0, double v0, double tau);
 
 void *ref_phys_create(const orc_phys_config *cfg, const double *imm_prop_h, const double *imm_rough_h,
                       const double *imm_temp_h);
@@ -55,6 +63,10 @@ int ref_phys_geostrophic(void *h, double *rho_d, double *u, double *v, double *w
                          double lat_g, double u_g, double v_g);
 int ref_phys_surface_fluxes(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
                             double dt);
+int ref_phys_uniform_pg(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc, double dt,
+                        double tau, unsigned long long update_cycles, double *st);
+int ref_phys_uniform_pg_height(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                               double dt, double height, double u0, double v0, double tau);
 
 #ifdef __cplusplus
 }

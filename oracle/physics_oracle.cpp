@@ -9,6 +9,8 @@
 //   sponge_layer                      sponge_layer.h:7-62
 //   geostrophic_wind_forcing          geostrophic_wind_forcing.h:7-42
 //   apply_surface_fluxes              surface_flux.h:9-125
+//   uniform_pg_wind_forcing           uniform_pg_wind_forcing.h:6-40
+//   uniform_pg_wind_forcing_height    uniform_pg_wind_forcing.h:43-82
 // The arithmetic of each quantity is evaluated in the reference's order
 // (the build uses -ffp-contract=off), so the restatement is compared with the
 // reference's own modules bit for bit in the tests.  The code is organised
@@ -417,4 +419,68 @@ int orc_phys_surface_fluxes(void *h, double *, double *u, double *v, double *w, 
   return 0;
 }
 
-}  // extern "C"
+// uniform_pg_wind_forcing (uniform_pg_wind_forcing.h:6-40): every
+// update_cycles calls the domain means of u and v (sums in memory order over
+// all cells, divided by the cell count); u += dt/tau*(u0-u), likewise v.
+int orc_phys_uniform_pg(void *h, double *, double *u, double *v, double *, double *, double *, double dt, double tau,
+                        unsigned long long update_cycles, double *st) {
+  const orc_phys_config &c = static_cast<Phys *>(h)->c;
+  if (update_cycles == 0) return 1;
+  const size_t n = size_t(c.nz) * c.ny * c.nx;
+  const unsigned long long counter = (unsigned long long)st[0];
+  if (counter % update_cycles == 0) {
+    double su = 0, sv = 0;
+    for (size_t q = 0; q < n; q++) su += u[q];
+    for (size_t q = 0; q < n; q++) sv += v[q];
+    st[3] = su / double(n);
+    st[4] = sv / double(n);
+    if (counter == 0) {
+      st[1] = st[3];
+      st[2] = st[4];
+    }
+  }
+  const double fu = dt / tau * (st[1] - st[3]), fv = dt / tau * (st[2] - st[4]);
+  for (size_t q = 0; q < n; q++) {
+    u[q] += fu;
+    v[q] += fv;
+  }
+  st[0] = double(counter + 1);
+  return 0;
+}
+
+// uniform_pg_wind_forcing_height (uniform_pg_wind_forcing.h:43-82): level
+// means of the two levels whose centres bracket `height`, linear in z
+// between them.  Returns 1 where the reference would read outside the levels.
+int orc_phys_uniform_pg_height(void *h, double *, double *u, double *v, double *, double *, double *, double dt,
+                               double height, double u0, double v0, double tau) {
+  const orc_phys_config &c = static_cast<Phys *>(h)->c;
+  const double dz = c.zlen / c.nz;
+  int k1 = 0;
+  for (int k = 0; k < c.nz; k++)
+    if ((k + 0.5) * dz > height) {
+      k1 = k - 1;
+      break;
+    }
+  if (k1 < 0 || k1 + 1 >= c.nz) return 1;
+  const size_t nl = size_t(c.ny) * c.nx;
+  double m[2][2];
+  for (int l = 0; l < 2; l++) {
+    double su = 0, sv = 0;
+    for (size_t q = (k1 + l) * nl; q < (k1 + l + 1) * nl; q++) su += u[q];
+    for (size_t q = (k1 + l) * nl; q < (k1 + l + 1) * nl; q++) sv += v[q];
+    m[l][0] = su / double(nl);
+    m[l][1] = sv / double(nl);
+  }
+  const double z1 = (k1 + 0.5) * dz, z2 = (k1 + 1.5) * dz;
+  const double w1 = (z2 - height) / dz, w2 = (height - z1) / dz;
+  const double um = w1 * m[0][0] + w2 * m[1][0], vm = w1 * m[0][1] + w2 * m[1][1];
+  const double fu = dt / tau * (u0 - um), fv = dt / tau * (v0 - vm);
+  const size_t n = nl * c.nz;
+  for (size_t q = 0; q < n; q++) {
+    u[q] += fu;
+    v[q] += fv;
+  }
+  return 0;
+}
+
+}  // extern "C

@@ -70,7 +70,9 @@ def _lib(kind):
     getattr(lib, pre + "sponge").argtypes = arr + [D, D, D]
     getattr(lib, pre + "geostrophic").argtypes = arr + [D, D, D, D]
     getattr(lib, pre + "surface_fluxes").argtypes = arr + [D]
-    for nm in ("les", "sponge", "geostrophic", "surface_fluxes"):
+    getattr(lib, pre + "uniform_pg").argtypes = arr + [D, D, C.c_ulonglong, P]
+    getattr(lib, pre + "uniform_pg_height").argtypes = arr + [D, D, D, D, D]
+    for nm in ("les", "sponge", "geostrophic", "surface_fluxes", "uniform_pg", "uniform_pg_height"):
         getattr(lib, pre + nm).restype = C.c_int
     return lib
 
@@ -117,6 +119,19 @@ class Physics:
 
     def surface_fluxes(self, state, dt):
         return self._call("surface_fluxes", state, dt)
+
+    def uniform_pg(self, state, dt, tau, update_cycles, st):
+        """st: float64 array [counter, u0, v0, u, v], updated in place."""
+        s = {k: np.array(v, dtype=np.float64, order="C", copy=True) for k, v in state.items()}
+        ptrs = [s[k].ctypes.data for k in ("rho_d", "uvel", "vvel", "wvel", "temp", "tracers")]
+        rc = getattr(self.lib, self.kind + "_phys_uniform_pg")(self.h, *ptrs, float(dt), float(tau), int(update_cycles),
+                                                               st.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("%s_phys_uniform_pg failed" % self.kind)
+        return s
+
+    def uniform_pg_height(self, state, dt, height, u0, v0, tau):
+        return self._call("uniform_pg_height", state, dt, height, u0, v0, tau)
 
 
 def state_of(case, seed=0, wind_noise=0.5, tke_noise=0.05):

@@ -2,7 +2,8 @@
 // INFRASTRUCTURE ONLY).
 //
 // Compiles model/modules/les_closure.h, sponge_layer.h,
-// geostrophic_wind_forcing.h and surface_flux.h of the reference unchanged
+// geostrophic_wind_forcing.h, surface_flux.h and uniform_pg_wind_forcing.h
+// of the reference unchanged
 // against the single-rank shim in oracle/ref_shim and exposes them through
 // the ref_phys_* functions of oracle/physics_api.h.  Each call copies the
 // given coupler arrays into the shim coupler's DataManager, runs the module
@@ -13,6 +14,7 @@
 #include "physics_api.h"
 #include "sponge_layer.h"
 #include "surface_flux.h"
+#include "uniform_pg_wind_forcing.h"
 
 #include <cstdio>
 #include <cstring>
@@ -162,4 +164,40 @@ int ref_phys_surface_fluxes(void *p, double *rho_d, double *u, double *v, double
   });
 }
 
-}  // extern "C"
+int ref_phys_uniform_pg(void *p, double *rho_d, double *u, double *v, double *w, double *T, double *trc, double dt,
+                        double tau, unsigned long long update_cycles, double *st) {
+  PhysHandle &h = *static_cast<PhysHandle *>(p);
+  return guarded([&]() {
+    copy_in(h, rho_d, u, v, w, T, trc);
+    auto &c = h.coupler;
+    const std::string pre = "uniform_pg_wind_forcing_";
+    c.set_option<size_t>(pre + "counter", size_t(st[0]));
+    if (st[0] > 0) {
+      c.set_option<real>(pre + "u0", st[1]);
+      c.set_option<real>(pre + "v0", st[2]);
+      c.set_option<real>(pre + "u", st[3]);
+      c.set_option<real>(pre + "v", st[4]);
+    }
+    modules::uniform_pg_wind_forcing(c, dt, tau, size_t(update_cycles));
+    copy_out(h, rho_d, u, v, w, T, trc);
+    st[0] = double(c.get_option<size_t>(pre + "counter"));
+    st[1] = c.get_option<real>(pre + "u0");
+    st[2] = c.get_option<real>(pre + "v0");
+    st[3] = c.get_option<real>(pre + "u");
+    st[4] = c.get_option<real>(pre + "v");
+    return 0;
+  });
+}
+
+int ref_phys_uniform_pg_height(void *p, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                               double dt, double height, double u0, double v0, double tau) {
+  PhysHandle &h = *static_cast<PhysHandle *>(p);
+  return guarded([&]() {
+    copy_in(h, rho_d, u, v, w, T, trc);
+    modules::uniform_pg_wind_forcing_height(h.coupler, dt, height, u0, v0, tau);
+    copy_out(h, rho_d, u, v, w, T, trc);
+    return 0;
+  });
+}
+
+}  // extern "C

@@ -57,6 +57,8 @@ class ParallelComm {
   }
   template <class T>
   T all_reduce(T v, MPI_Op) const { return v; }
+  template <class T>
+  T all_reduce(T v, MPI_Op, std::string) const { return v; }
 };
 
 class DataManager {

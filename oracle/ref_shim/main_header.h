@@ -10,7 +10,7 @@
 //   * yakl::SArray     -- fixed-size array, C order, (i,j,...) indexing
 //   * yakl::Array      -- reference-counted C-order N-d array with views
 //   * yakl::c::parallel_for over SimpleBounds (OpenMP on the host cores)
-//   * yakl::intrinsics::matmul_cr (column-row matrix products)
+//   * yakl::intrinsics::matmul_cr (column-row matrix products) and sum
 //   * no-op timers and a no-op SimplePNetCDF (output hooks are registered,
 //     never called)
 //   * Kokkos::abort / endrun throwing std::runtime_error.
@@ -268,6 +268,14 @@ void parallel_for(Bounds<N> const &b, F const &f) { parallel_for("", b, f); }
 }  // namespace c
 
 namespace intrinsics {
+// Sum of all elements in memory order (yakl's sum is a parallel reduction
+// whose order is unspecified; one order has to be picked at one rank).
+template <class T, int N, int M, int S>
+typename std::remove_cv<T>::type sum(Array<T, N, M, S> const &a) {
+  typename std::remove_cv<T>::type s = 0;
+  for (size_t i = 0; i < a.size(); i++) s += a.data()[i];
+  return s;
+}
 // Column-row storage: A(col,row).  C = A*B as matrices, C(c,r) = sum_k A(k,r) B(c,k).
 template <class T, size_t CA, size_t RA, size_t CB>
 SArray<T, 2, CB, RA> matmul_cr(SArray<T, 2, CA, RA> const &A, SArray<T, 2, CB, CA> const &B) {

@@ -81,6 +81,11 @@ class pu_physics_config(C.Structure):
                 ("device", C.c_int), ("stream", C.c_void_p)]
 
 
+class pu_uniform_pg_state(C.Structure):
+    _fields_ = [("counter", C.c_ulonglong), ("u0", C.c_double), ("v0", C.c_double),
+                ("u", C.c_double), ("v", C.c_double)]
+
+
 class pu_profile(C.Structure):
     _fields_ = [("ms", C.c_double * PU_PROFILE_KINDS), ("launches", C.c_longlong * PU_PROFILE_KINDS)]
 
@@ -129,6 +134,9 @@ SIGNATURES = {
     "pu_sponge_layer": (_I, [_P, C.POINTER(pu_state_view), _D, _D, _D]),
     "pu_geostrophic_forcing": (_I, [_P, C.POINTER(pu_state_view), _D, _D, _D, _D]),
     "pu_surface_fluxes": (_I, [_P, C.POINTER(pu_state_view), _D]),
+    "pu_uniform_pg_wind_forcing": (_I, [_P, C.POINTER(pu_state_view), _D, _D, C.c_ulonglong,
+                                        C.POINTER(pu_uniform_pg_state)]),
+    "pu_uniform_pg_wind_forcing_height": (_I, [_P, C.POINTER(pu_state_view), _D, _D, _D, _D, _D]),
     "pu_physics_synchronize": (_I, [_P]),
     "pu_physics_last_les_ms": (_I, [_P, C.POINTER(_D)]),
 }

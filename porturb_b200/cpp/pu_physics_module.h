@@ -1,5 +1,6 @@
 // Shared part of the drop-in physics modules (les_closure.h, sponge_layer.h,
-// geostrophic_wind_forcing.h, surface_flux.h in this directory) on top of
+// geostrophic_wind_forcing.h, surface_flux.h, uniform_pg_wind_forcing.h in
+// this directory) on top of
 // libpu_dycore's physics entry points (include/pu_physics.h).
 //
 // The reference's modules read their options and the immersed halo arrays
@@ -13,6 +14,7 @@
 #pragma once
 
 #include <string>
+#include <vector>
 
 #include "coupler.h"
 #include "pu_physics.h"
@@ -32,9 +34,21 @@ inline int physics_bc(std::string const &bc) {
   return -1;
 }
 
-inline pu_physics *physics_handle(core::Coupler &coupler) {
-  if (coupler.option_exists("pu_physics_handle") && coupler.get_option<size_t>("pu_physics_handle") != 0)
-    return reinterpret_cast<pu_physics *>(coupler.get_option<size_t>("pu_physics_handle"));
+inline bool have_immersed_halos(core::Coupler const &coupler) {
+  auto const &dm = coupler.get_data_manager_readonly();
+  return dm.entry_exists("immersed_proportion_halos") && dm.entry_exists("immersed_roughness_halos") &&
+         dm.entry_exists("immersed_temp_halos");
+}
+
+// need_halos = false (modules that read no immersed arrays: the pressure-
+// gradient forcings): without the immersed_*_halos entries the handle is made
+// with no immersed cells and kept under its own option key, so a later module
+// that needs the entries still finds them missing, as in the reference.
+inline pu_physics *physics_handle(core::Coupler &coupler, bool need_halos = true) {
+  const bool plain = !need_halos && !have_immersed_halos(coupler);
+  const char *key = plain ? "pu_physics_handle_no_immersed" : "pu_physics_handle";
+  if (coupler.option_exists(key) && coupler.get_option<size_t>(key) != 0)
+    return reinterpret_cast<pu_physics *>(coupler.get_option<size_t>(key));
   pu_physics_config c{};
   c.nx = coupler.get_nx();
   c.ny = coupler.get_ny();
@@ -68,13 +82,18 @@ inline pu_physics *physics_handle(core::Coupler &coupler) {
   c.bc_z = physics_bc(coupler.get_option<std::string>("bc_z", "solid_wall"));
   c.device = 0;
   c.stream = nullptr;
-  auto const &dm = coupler.get_data_manager_readonly();
-  auto prop = dm.get<real const, 3>("immersed_proportion_halos");
-  auto rough = dm.get<real const, 3>("immersed_roughness_halos");
-  auto temp = dm.get<real const, 3>("immersed_temp_halos");
   pu_physics *h = nullptr;
-  check_physics(pu_physics_create(&c, prop.data(), rough.data(), temp.data(), PU_MEM_AUTO, &h));
-  coupler.set_option<size_t>("pu_physics_handle", reinterpret_cast<size_t>(h));
+  if (plain) {
+    std::vector<double> zero(size_t(c.nz + 2) * (c.ny + 2) * (c.nx + 2), 0.0);
+    check_physics(pu_physics_create(&c, zero.data(), zero.data(), zero.data(), PU_MEM_HOST, &h));
+  } else {
+    auto const &dm = coupler.get_data_manager_readonly();
+    auto prop = dm.get<real const, 3>("immersed_proportion_halos");
+    auto rough = dm.get<real const, 3>("immersed_roughness_halos");
+    auto temp = dm.get<real const, 3>("immersed_temp_halos");
+    check_physics(pu_physics_create(&c, prop.data(), rough.data(), temp.data(), PU_MEM_AUTO, &h));
+  }
+  coupler.set_option<size_t>(key, reinterpret_cast<size_t>(h));
   return h;
 }
 
@@ -95,11 +114,13 @@ inline pu_state_view physics_view(core::Coupler &coupler) {
 
 }  // namespace pu_detail
 
-// Releases the handle the physics modules created on this coupler.
+// Releases the handles the physics modules created on this coupler.
 inline void pu_physics_module_finalize(core::Coupler &coupler) {
-  if (!coupler.option_exists("pu_physics_handle") || coupler.get_option<size_t>("pu_physics_handle") == 0) return;
-  pu_physics_destroy(reinterpret_cast<pu_physics *>(coupler.get_option<size_t>("pu_physics_handle")));
-  coupler.set_option<size_t>("pu_physics_handle", size_t(0));
+  for (const char *key : {"pu_physics_handle", "pu_physics_handle_no_immersed"}) {
+    if (!coupler.option_exists(key) || coupler.get_option<size_t>(key) == 0) continue;
+    pu_physics_destroy(reinterpret_cast<pu_physics *>(coupler.get_option<size_t>(key)));
+    coupler.set_option<size_t>(key, size_t(0));
+  }
 }
 
 }  // namespace modules

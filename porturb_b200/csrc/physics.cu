@@ -11,8 +11,9 @@
 // (neighbouring blocks still read the input).
 // k_level_partial / k_level_final: deterministic level means (Neumaier-
 // compensated FP64 sums in a fixed order) for the sponge and the
-// geostrophic forcing; k_sponge / k_geostrophic / k_surface_fluxes are
-// pointwise updates in place.
+// geostrophic forcing and the pressure-gradient wind forcings; k_sponge /
+// k_geostrophic / k_surface_fluxes / k_add_uv / k_pg_height are pointwise
+// updates in place.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -20,6 +21,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/pu_physics.h"
 
@@ -310,7 +312,7 @@ __global__ void __launch_bounds__(NT) k_les(const Grid G, const In in, const Out
 // ---------------------------------------------------------------------------
 struct CSum {
   double s, c;
-  __device__ void add(double x) {
+  __host__ __device__ void add(double x) {
     const double t = s + x;
     c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
     s = t;
@@ -384,6 +386,27 @@ __global__ void k_geostrophic(double *u, double *v, const double *mean, int nz, 
   const double *m = mean + (e / n) * 3;
   u[e] += dt * (fcor * (m[1] - v_g));
   v[e] += dt * (-fcor * (m[0] - u_g));
+}
+
+// uvel += fu, vvel += fv everywhere (uniform_pg_wind_forcing.h:35-38).
+__global__ void k_add_uv(double *u, double *v, size_t n, double fu, double fv) {
+  const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  u[e] += fu;
+  v[e] += fv;
+}
+
+// The forcing of uniform_pg_wind_forcing_height (uniform_pg_wind_forcing.h:
+// 69-80) from the level means of the two bracketing levels, mean[0..1] and
+// mean[3..4]; each thread forms the same scalars, so no host round trip.
+__global__ void k_pg_height(double *u, double *v, const double *mean, size_t n, double w1, double w2, double dt_tau,
+                            double u0, double v0) {
+  const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const double um = w1 * mean[0] + w2 * mean[3];
+  const double vm = w1 * mean[1] + w2 * mean[4];
+  u[e] += dt_tau * (u0 - um);
+  v[e] += dt_tau * (v0 - vm);
 }
 
 // Log-law drag and heat flux from each immersed face neighbour, in the
@@ -593,8 +616,10 @@ int les_written(const pu_physics &h, int *which) {
   return n;
 }
 
-int level_means(pu_physics &h, const double *a0, const double *a1, const double *a2, int nf, int klo) {
-  const int nlev = h.cfg.nz - klo;
+// Means of levels klo .. klo+nlev-1 (all levels from klo up when nlev < 0)
+// into h.mean[(k - klo) * 3 + f].
+int level_means(pu_physics &h, const double *a0, const double *a1, const double *a2, int nf, int klo, int nlev = -1) {
+  if (nlev < 0) nlev = h.cfg.nz - klo;
   if (nlev <= 0) return PU_OK;
   const double r = 1. / (double(h.cfg.nx) * h.cfg.ny);
   k_level_partial<<<dim3(nlev, PARTS), RED_T, 0, h.st>>>(a0, a1, a2, nf, klo, h.cfg.nx, h.cfg.ny, r, h.partial);
@@ -799,6 +824,81 @@ int pu_surface_fluxes(pu_physics *h, pu_state_view *v, double dt) {
   if (staged) {
     const int which[4] = {1, 2, 3, 4};
     return copy_back(*h, v, d, which, 4);
+  }
+  return PU_OK;
+}
+
+int pu_uniform_pg_wind_forcing(pu_physics *h, pu_state_view *v, double dt, double tau,
+                               unsigned long long update_cycles, pu_uniform_pg_state *state) {
+  if (!h || !v || !state) return fail(PU_ERR_INVALID, "null argument");
+  if (update_cycles == 0 || !(tau > 0)) return fail(PU_ERR_INVALID, "bad uniform_pg_wind_forcing parameters");
+  Dev g(h->cfg.device);
+  double *d[5 + PU_MAX_TRACERS];
+  bool staged;
+  int rc = device_arrays(*h, v, d, staged);
+  if (rc) return rc;
+  if (state->counter % update_cycles == 0) {
+    // Domain mean = mean of the level means (all levels hold nx*ny cells),
+    // summed over the levels with compensation on the host.
+    rc = level_means(*h, d[1], d[2], nullptr, 2, 0);
+    if (rc) return rc;
+    std::vector<double> m(size_t(h->cfg.nz) * 3);
+    PH_CK(cudaMemcpyAsync(m.data(), h->mean, m.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    PH_CK(cudaStreamSynchronize(h->st));
+    double mean[2];
+    for (int f = 0; f < 2; f++) {
+      CSum acc{0.0, 0.0};
+      for (int k = 0; k < h->cfg.nz; k++) acc.add(m[size_t(k) * 3 + f]);
+      mean[f] = (acc.s + acc.c) / h->cfg.nz;
+    }
+    state->u = mean[0];
+    state->v = mean[1];
+    if (state->counter == 0) {
+      state->u0 = mean[0];
+      state->v0 = mean[1];
+    }
+  }
+  k_add_uv<<<unsigned((h->N + 255) / 256), 256, 0, h->st>>>(d[1], d[2], h->N, dt / tau * (state->u0 - state->u),
+                                                            dt / tau * (state->v0 - state->v));
+  PH_CK(cudaGetLastError());
+  state->counter++;
+  if (staged) {
+    const int which[2] = {1, 2};
+    return copy_back(*h, v, d, which, 2);
+  }
+  return PU_OK;
+}
+
+int pu_uniform_pg_wind_forcing_height(pu_physics *h, pu_state_view *v, double dt, double height, double u0, double v0,
+                                      double tau) {
+  if (!h || !v) return fail(PU_ERR_INVALID, "null argument");
+  if (!(tau > 0)) return fail(PU_ERR_INVALID, "bad uniform_pg_wind_forcing_height parameters");
+  const int nz = h->cfg.nz;
+  const double dz = h->cfg.dz;
+  // The lower bracketing level, found as the reference does
+  // (uniform_pg_wind_forcing.h:56-57): 0 when no level centre is above height.
+  int k1 = 0;
+  for (int k = 0; k < nz; k++)
+    if ((k + 0.5) * dz > height) {
+      k1 = k - 1;
+      break;
+    }
+  if (k1 < 0) return fail(PU_ERR_INVALID, "uniform_pg_wind_forcing_height: height below the first level centre");
+  if (k1 + 1 >= nz) return fail(PU_ERR_INVALID, "uniform_pg_wind_forcing_height needs nz >= 2");
+  Dev g(h->cfg.device);
+  double *d[5 + PU_MAX_TRACERS];
+  bool staged;
+  int rc = device_arrays(*h, v, d, staged);
+  if (rc) return rc;
+  rc = level_means(*h, d[1], d[2], nullptr, 2, k1, 2);
+  if (rc) return rc;
+  const double z1 = (k1 + 0.5) * dz, z2 = (k1 + 1.5) * dz;
+  const double w1 = (z2 - height) / dz, w2 = (height - z1) / dz;
+  k_pg_height<<<unsigned((h->N + 255) / 256), 256, 0, h->st>>>(d[1], d[2], h->mean, h->N, w1, w2, dt / tau, u0, v0);
+  PH_CK(cudaGetLastError());
+  if (staged) {
+    const int which[2] = {1, 2};
+    return copy_back(*h, v, d, which, 2);
   }
   return PU_OK;
 }

@@ -3,12 +3,14 @@ run beside the dycore every dt_phys (abl_neutral.cpp:93-104 of the
 reference), on top of include/pu_physics.h:
 
 * :class:`Physics` -- one pu_physics handle (options and immersed halo arrays
-  held on the GPU) with ``les``, ``les_to``, ``sponge``, ``geostrophic`` and
-  ``surface_fluxes`` on coupler arrays (numpy float64 or torch CUDA float64).
+  held on the GPU) with ``les``, ``les_to``, ``sponge``, ``geostrophic``,
+  ``surface_fluxes``, ``uniform_pg`` and ``uniform_pg_height`` on coupler
+  arrays (numpy float64 or torch CUDA float64).
 * The reference's module API on a :class:`~porturb_b200.dycore.Coupler`:
   :class:`LES_Closure` (``init`` adds the TKE tracer, ``apply``),
-  :func:`sponge_layer`, :func:`geostrophic_wind_forcing` and
-  :func:`apply_surface_fluxes`, reading the options and the
+  :func:`sponge_layer`, :func:`geostrophic_wind_forcing`,
+  :func:`apply_surface_fluxes`, :func:`uniform_pg_wind_forcing` and
+  :func:`uniform_pg_wind_forcing_height`, reading the options and the
   ``immersed_*_halos`` entries the drivers' init registers
   (sc_init.h:727-768).
 """
@@ -110,6 +112,18 @@ class Physics:
         view = make_view(rho_d, u, v, w, T, tracers)
         check(self.lib.pu_surface_fluxes(self.h, C.byref(view), float(dt)))
 
+    def uniform_pg(self, rho_d, u, v, w, T, tracers, dt, tau, update_cycles, state: capi.pu_uniform_pg_state):
+        """uniform_pg_wind_forcing on coupler arrays; `state` (counter, u0, v0,
+        u, v) is updated in place."""
+        view = make_view(rho_d, u, v, w, T, tracers)
+        check(self.lib.pu_uniform_pg_wind_forcing(self.h, C.byref(view), float(dt), float(tau), int(update_cycles),
+                                                  C.byref(state)))
+
+    def uniform_pg_height(self, rho_d, u, v, w, T, tracers, dt, height, u0, v0, tau):
+        view = make_view(rho_d, u, v, w, T, tracers)
+        check(self.lib.pu_uniform_pg_wind_forcing_height(self.h, C.byref(view), float(dt), float(height), float(u0),
+                                                         float(v0), float(tau)))
+
     def synchronize(self):
         check(self.lib.pu_physics_synchronize(self.h))
 
@@ -122,8 +136,17 @@ class Physics:
 # ---------------------------------------------------------------------------
 # The reference's module API on a Coupler.
 # ---------------------------------------------------------------------------
-def _handle(coupler) -> Physics:
+_HALO_NAMES = ("immersed_proportion_halos", "immersed_roughness_halos", "immersed_temp_halos")
+
+
+def _handle(coupler, need_halos=True) -> Physics:
+    """The coupler's physics handle.  Modules that read no immersed arrays
+    (the pressure-gradient forcings) get one with no immersed cells when the
+    coupler has none registered; the others need the entries, as in the
+    reference."""
     key = "pu_physics"
+    if not need_halos and not all(coupler.entry_exists(n) for n in _HALO_NAMES):
+        key = "pu_physics_no_immersed"
     h = coupler.module_state.get(key)
     if h is None:
         opts = {k: coupler.get_option(k) for k in ("R_d", "gamma_d", "C0", "grav")}
@@ -131,8 +154,11 @@ def _handle(coupler) -> Physics:
                            ("les_total_mult", 1.0), ("les_dissipation_mult", 1.0), ("les_shear_prod_mult", 1.0),
                            ("bc_x", "periodic"), ("bc_y", "periodic"), ("bc_z", "solid_wall")):
             opts[k] = coupler.get_option(k, default)
-        halos = [coupler.get(n) for n in ("immersed_proportion_halos", "immersed_roughness_halos",
-                                          "immersed_temp_halos")]
+        if key == "pu_physics":
+            halos = [coupler.get(n) for n in _HALO_NAMES]
+        else:
+            shape = (coupler.get_nz() + 2, coupler.get_ny() + 2, coupler.get_nx() + 2)
+            halos = [np.zeros(shape) for _ in _HALO_NAMES]
         tracers = [(t[0], t[4]) for t in coupler.tracers]
         dev = 0
         if coupler.device is not None and ":" in str(coupler.device):
@@ -179,6 +205,33 @@ def apply_surface_fluxes(coupler, dt):
     """modules::apply_surface_fluxes (surface_flux.h:9-125)."""
     rd, u, v, w, T, trc = _arrays(coupler)
     _handle(coupler).surface_fluxes(rd, u, v, w, T, trc, dt)
+
+
+_PG = "uniform_pg_wind_forcing_"
+
+
+def uniform_pg_wind_forcing(coupler, dt, tau=10.0, update_cycles=1):
+    """modules::uniform_pg_wind_forcing (uniform_pg_wind_forcing.h:6-40):
+    relaxes the domain-mean wind toward its value at the first call.  The
+    state lives in the coupler options uniform_pg_wind_forcing_counter, _u0,
+    _v0, _u, _v, as in the reference."""
+    st = capi.pu_uniform_pg_state()
+    st.counter = int(coupler.get_option(_PG + "counter", 0))
+    if st.counter:
+        st.u0, st.v0 = coupler.get_option(_PG + "u0"), coupler.get_option(_PG + "v0")
+        st.u, st.v = coupler.get_option(_PG + "u"), coupler.get_option(_PG + "v")
+    rd, u, v, w, T, trc = _arrays(coupler)
+    _handle(coupler, need_halos=False).uniform_pg(rd, u, v, w, T, trc, dt, tau, update_cycles, st)
+    for k in ("u0", "v0", "u", "v"):
+        coupler.set_option(_PG + k, float(getattr(st, k)))
+    coupler.set_option(_PG + "counter", int(st.counter))
+
+
+def uniform_pg_wind_forcing_height(coupler, dt, height, u0, v0, tau=10.0):
+    """modules::uniform_pg_wind_forcing_height (uniform_pg_wind_forcing.h:43-82):
+    relaxes the mean wind at `height` toward (u0, v0)."""
+    rd, u, v, w, T, trc = _arrays(coupler)
+    _handle(coupler, need_halos=False).uniform_pg_height(rd, u, v, w, T, trc, dt, height, u0, v0, tau)
 
 
 def register_immersed_halos(coupler, case, **kw):

@@ -9,6 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 EXE = os.path.join(HERE, "_build", "dropin_driver")
 PHYS_EXE = os.path.join(HERE, "_build", "physics_driver")
+PG_EXE = os.path.join(HERE, "_build", "pg_driver")
 REF_CORE = "/root/reference/model/core"
 
 
@@ -20,12 +21,13 @@ def _compile(src, exe, libdir):
 
 
 def build(libdir):
-    """Builds both drivers (the dycore drop-in alone, and the boundary-layer
-    module chain); returns the dycore driver's path, or None without the
+    """Builds the drivers (the dycore drop-in alone, the boundary-layer module
+    chain, the pressure-gradient forcings); returns the dycore driver's path, or None without the
     reference tree and without a prebuilt binary."""
     if not os.path.isdir(REF_CORE):
         return EXE if os.path.exists(EXE) else None
     os.makedirs(os.path.dirname(EXE), exist_ok=True)
     _compile("dropin_driver.cpp", EXE, libdir)
     _compile("physics_driver.cpp", PHYS_EXE, libdir)
+    _compile("pg_driver.cpp", PG_EXE, libdir)
     return EXE

@@ -108,3 +108,41 @@ def test_physics_dropin_chain_matches_python_front_end(tmp_path):
     ref = np.concatenate([np.stack(a), np.stack(trs)])
     assert np.array_equal(out, ref)
     assert not np.array_equal(ref[6], np.asarray(pert[5][1]))   # the closure changed TKE
+
+
+@pytest.mark.gpu
+def test_pg_forcing_dropin_matches_python_front_end(tmp_path):
+    """The drop-in uniform_pg_wind_forcing / _height headers on a coupler
+    with no immersed arrays give the same arrays and carried options as the
+    Python module API."""
+    from porturb_b200 import case_coupler, cases, uniform_pg_wind_forcing, uniform_pg_wind_forcing_height
+    build_driver()
+    exe = os.path.join(ROOT, "tests", "cpp", "_build", "pg_driver")
+    case = cases.abl_neutral(nx=24, ny=20, nz=16)
+    rng = np.random.default_rng(3)
+    u = 4.0 + rng.standard_normal((case.nz, case.ny, case.nx))
+    v = -1.0 + rng.standard_normal((case.nz, case.ny, case.nx))
+    dz = case.zlen / case.nz
+    ncalls, cycles, dt, tau = 4, 2, 0.1, 3.0
+    height, u0, v0, tau_h = 5.3 * dz, 7.0, 0.5, 2.0
+    with open(tmp_path / "in.bin", "wb") as f:
+        np.array([case.nx, case.ny, case.nz, ncalls, cycles], np.int32).tofile(f)
+        np.array([case.xlen, case.ylen, case.zlen, dt, tau, height, u0, v0, tau_h, 0.0], np.float64).tofile(f)
+        u.tofile(f)
+        v.tofile(f)
+    r = subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = np.fromfile(tmp_path / "out.bin", np.float64)
+    n = u.size
+    c = case_coupler(case)
+    c.get("uvel")[...] = u
+    c.get("vvel")[...] = v
+    for _ in range(ncalls):
+        uniform_pg_wind_forcing(c, dt, tau, cycles)
+        c.get("uvel")[...] += 0.25
+    st = [c.get_option("uniform_pg_wind_forcing_" + k) for k in ("counter", "u0", "v0", "u", "v")]
+    uniform_pg_wind_forcing_height(c, dt, height, u0, v0, tau_h)
+    assert np.array_equal(out[:n].reshape(u.shape), c.get("uvel"))
+    assert np.array_equal(out[n:2 * n].reshape(v.shape), c.get("vvel"))
+    assert np.array_equal(out[2 * n:], np.array(st, np.float64))
+    assert not np.array_equal(c.get("vvel"), v)

@@ -144,3 +144,80 @@ def test_module_api_on_a_coupler(oracle_lib, gpu_lib):
     got = dict(rho_d=c.get("density_dry"), uvel=c.get("uvel"), vvel=c.get("vvel"), wvel=c.get("wvel"),
                temp=c.get("temp"), tracers=np.stack([c.get(n) for n in c.get_tracer_names()]))
     _check("coupler", got, want, st)
+
+
+def _pg_state(case, seed):
+    st = pyphysics.state_of(case, seed=seed)
+    rng = np.random.default_rng(seed)
+    st["uvel"] = st["uvel"] + 3.0 + rng.standard_normal(st["uvel"].shape)
+    st["vvel"] = st["vvel"] - 1.0 + rng.standard_normal(st["vvel"].shape)
+    return st
+
+
+@pytest.mark.parametrize("update_cycles", [1, 3])
+@pytest.mark.parametrize("device", [False, True])
+def test_uniform_pg_matches_oracle_across_calls(oracle_lib, gpu_lib, update_cycles, device):
+    """uniform_pg_wind_forcing over 7 calls with the wind disturbed between
+    them: the carried state (counter, u0, v0, u, v) and the fields match."""
+    from porturb_b200 import capi
+    case, halos, _ = _case("plain")
+    orc = pyphysics.Physics(case, "orc", halos)
+    ph = Physics.from_case(case, halos=halos)
+    st = _pg_state(case, 5)
+    so, sg = np.zeros(5), capi.pu_uniform_pg_state()
+    rng = np.random.default_rng(9)
+    for call in range(7):
+        want = orc.uniform_pg(st, 0.05, 2.0, update_cycles, so)
+        got = _run_gpu(ph, "uniform_pg", st, (0.05, 2.0, update_cycles, sg), device)
+        _check("uniform_pg/%d" % call, got, want, st)
+        assert sg.counter == so[0]
+        for i, k in enumerate(("u0", "v0", "u", "v")):
+            assert abs(getattr(sg, k) - so[1 + i]) <= 1e-14 * abs(so[1 + i]), (call, k)
+        st = want
+        st["uvel"] = st["uvel"] + 0.3 * rng.standard_normal(st["uvel"].shape)
+        st["vvel"] = st["vvel"] + 0.3 * rng.standard_normal(st["vvel"].shape)
+    ph.close()
+
+
+@pytest.mark.parametrize("device", [False, True])
+def test_uniform_pg_height_matches_oracle(oracle_lib, gpu_lib, device):
+    from porturb_b200.capi import PortUrbError
+    case, halos, _ = _case("plain")
+    dz = case.zlen / case.nz
+    orc = pyphysics.Physics(case, "orc", halos)
+    ph = Physics.from_case(case, halos=halos)
+    st = _pg_state(case, 6)
+    for height in (3.3 * dz, 7.5 * dz, 0.5 * dz, (case.nz + 0.4) * dz):
+        args = (0.05, height, 8.0, 0.5, 3.0)
+        want = orc.uniform_pg_height(st, *args)
+        got = _run_gpu(ph, "uniform_pg_height", st, args, device)
+        _check("uniform_pg_height/%.3f" % height, got, want, st)
+    with pytest.raises(PortUrbError):
+        _run_gpu(ph, "uniform_pg_height", st, (0.05, 0.4 * dz, 8.0, 0.5, 3.0), device)
+    ph.close()
+
+
+def test_uniform_pg_module_api_on_a_coupler(oracle_lib, gpu_lib):
+    """uniform_pg_wind_forcing keeps its state in the coupler options, as the
+    reference does, and needs no immersed arrays on the coupler."""
+    from porturb_b200 import case_coupler, uniform_pg_wind_forcing, uniform_pg_wind_forcing_height
+    case, halos, _ = _case("plain", nx=36, ny=16, nz=18)
+    c = case_coupler(case)
+    st = _pg_state(case, 12)
+    for k, name in (("uvel", "uvel"), ("vvel", "vvel")):
+        c.get(name)[...] = st[k]
+    orc = pyphysics.Physics(case, "orc", halos)
+    so = np.zeros(5)
+    want = dict(st)
+    for _ in range(3):
+        uniform_pg_wind_forcing(c, 0.1, 5.0, 2)
+        want = orc.uniform_pg(want, 0.1, 5.0, 2, so)
+        c.get("uvel")[...] += 0.25
+        want["uvel"] = want["uvel"] + 0.25
+    assert c.get_option("uniform_pg_wind_forcing_counter") == 3
+    assert abs(c.get_option("uniform_pg_wind_forcing_u") - so[3]) <= 1e-14 * abs(so[3])
+    dz = case.zlen / case.nz
+    uniform_pg_wind_forcing_height(c, 0.1, 2.2 * dz, 7.0, 0.0, 4.0)
+    want = orc.uniform_pg_height(want, 0.1, 2.2 * dz, 7.0, 0.0, 4.0)
+    got = dict(want, uvel=c.get("uvel"), vvel=c.get("vvel"))
+    _check("coupler_pg", got, want, st)

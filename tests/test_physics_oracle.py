@@ -77,3 +77,81 @@ def test_les_conserves_and_keeps_tke_positive(oracle_lib):
     assert abs(after - before) <= 1e-12 * abs(before)
     tke = [t.name for t in case.tracers].index("TKE")
     assert out["tracers"][tke].min() >= 0.0
+
+
+def _pg_state(case, seed):
+    st = pyphysics.state_of(case, seed=seed)
+    rng = np.random.default_rng(seed)
+    st["uvel"] = st["uvel"] + 3.0 + rng.standard_normal(st["uvel"].shape)
+    st["vvel"] = st["vvel"] - 1.0 + rng.standard_normal(st["vvel"].shape)
+    return st
+
+
+@pytest.mark.parametrize("update_cycles", [1, 3])
+def test_uniform_pg_matches_reference_across_calls(oracle_lib, update_cycles):
+    """uniform_pg_wind_forcing keeps (counter, u0, v0, u, v) between calls;
+    the wind is disturbed between calls so every update shows."""
+    case, halos, _ = _case("plain")
+    orc = pyphysics.Physics(case, "orc", halos)
+    ref = pyphysics.Physics(case, "ref", halos)
+    st = _pg_state(case, 1)
+    so, sr = np.zeros(5), np.zeros(5)
+    rng = np.random.default_rng(7)
+    for call in range(7):
+        a = orc.uniform_pg(st, 0.05, 2.0, update_cycles, so)
+        b = ref.uniform_pg(st, 0.05, 2.0, update_cycles, sr)
+        assert np.array_equal(so, sr), (call, so, sr)
+        for key in a:
+            assert np.array_equal(a[key], b[key]), (call, key)
+        st = a
+        st["uvel"] = st["uvel"] + 0.3 * rng.standard_normal(st["uvel"].shape)
+        st["vvel"] = st["vvel"] + 0.3 * rng.standard_normal(st["vvel"].shape)
+    assert so[0] == 7
+
+
+def test_uniform_pg_relaxes_the_domain_mean(oracle_lib):
+    """Known answer: the first call records the mean and forces nothing; after
+    a uniform +1 m/s gust the next call removes dt/tau of it."""
+    case, halos, _ = _case("plain")
+    orc = pyphysics.Physics(case, "orc", halos)
+    st = _pg_state(case, 2)
+    so = np.zeros(5)
+    a = orc.uniform_pg(st, 0.1, 4.0, 1, so)
+    assert np.array_equal(a["uvel"], st["uvel"]) and np.array_equal(a["vvel"], st["vvel"])
+    assert so[1] == so[3] and abs(so[1] - st["uvel"].mean()) < 1e-12
+    a["uvel"] = a["uvel"] + 1.0
+    b = orc.uniform_pg(a, 0.1, 4.0, 1, so)
+    assert abs(b["uvel"].mean() - (st["uvel"].mean() + 1.0 - 0.1 / 4.0)) < 1e-12
+    assert abs(b["vvel"].mean() - st["vvel"].mean()) < 1e-12
+
+
+@pytest.mark.parametrize("where", ["between", "on_centre", "above_top", "first_centre"])
+def test_uniform_pg_height_matches_reference(oracle_lib, where):
+    case, halos, _ = _case("plain")
+    dz = case.zlen / case.nz
+    height = {"between": 3.3 * dz, "on_centre": 4.5 * dz, "above_top": (case.nz + 0.2) * dz,
+              "first_centre": 0.5 * dz}[where]
+    st = _pg_state(case, 3)
+    a = pyphysics.Physics(case, "orc", halos).uniform_pg_height(st, 0.05, height, 8.0, 0.5, 3.0)
+    b = pyphysics.Physics(case, "ref", halos).uniform_pg_height(st, 0.05, height, 8.0, 0.5, 3.0)
+    for key in a:
+        assert np.array_equal(a[key], b[key]), key
+    assert not np.array_equal(a["uvel"], st["uvel"])
+
+
+def test_uniform_pg_height_known_answer_and_bad_height(oracle_lib):
+    """Linear interpolation between the bracketing level means; a height
+    below the first level centre is refused (the reference would read level
+    -1, so it is not called there)."""
+    case, halos, _ = _case("plain")
+    dz = case.zlen / case.nz
+    st = _pg_state(case, 4)
+    orc = pyphysics.Physics(case, "orc", halos)
+    height = 2.75 * dz   # between the centres of levels 2 (2.5 dz) and 3 (3.5 dz)
+    a = orc.uniform_pg_height(st, 0.2, height, 6.0, 1.0, 5.0)
+    um = 0.75 * st["uvel"][2].mean() + 0.25 * st["uvel"][3].mean()
+    vm = 0.75 * st["vvel"][2].mean() + 0.25 * st["vvel"][3].mean()
+    assert np.allclose(a["uvel"] - st["uvel"], 0.2 / 5.0 * (6.0 - um), rtol=0, atol=1e-13)
+    assert np.allclose(a["vvel"] - st["vvel"], 0.2 / 5.0 * (1.0 - vm), rtol=0, atol=1e-13)
+    with pytest.raises(RuntimeError):
+        orc.uniform_pg_height(st, 0.2, 0.4 * dz, 6.0, 1.0, 5.0)

@@ -123,6 +123,15 @@ int pu_dycore_destroy(pu_dycore *h);
  * `mem`; NULL = no immersed cells).  Synchronous. */
 int pu_dycore_init(pu_dycore *h, const pu_state_view *coupler, const double *immersed_proportion, int mem);
 
+/* init(coupler) when the coupler also holds windmill_proj_weight
+ * (dynamics_rk.h:1019-1025): the projection weight ((nz,ny,nx) doubles in
+ * `mem`, NULL = none) is added to a copy of immersed_proportion before the
+ * immersed halos, flags and time scales are built.  A projection without
+ * immersed_proportion is PU_ERR_INVALID (the reference aborts on the missing
+ * entry). */
+int pu_dycore_init_windmill(pu_dycore *h, const pu_state_view *coupler, const double *immersed_proportion,
+                            const double *windmill_proj_weight, int mem);
+
 /* compute_time_step(coupler), dynamics_rk.h:57-64: cfl*min(dx,dy,dz)/450. */
 int pu_dycore_compute_time_step(const pu_dycore *h, double *dt);
 

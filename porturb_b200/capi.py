@@ -100,6 +100,7 @@ SIGNATURES = {
     "pu_dycore_create": (_I, [C.POINTER(pu_config), C.POINTER(C.c_void_p)]),
     "pu_dycore_destroy": (_I, [_P]),
     "pu_dycore_init": (_I, [_P, C.POINTER(pu_state_view), _P, _I]),
+    "pu_dycore_init_windmill": (_I, [_P, C.POINTER(pu_state_view), _P, _P, _I]),
     "pu_dycore_compute_time_step": (_I, [_P, C.POINTER(_D)]),
     "pu_dycore_time_step": (_I, [_P, C.POINTER(pu_state_view), _D, C.POINTER(_I)]),
     "pu_dycore_load_state": (_I, [_P, C.POINTER(pu_state_view)]),

@@ -119,7 +119,10 @@ struct Dynamics_Euler_Stratified_WenoFV {
     pu_state_view v = coupler_view(coupler);
     const double *prop = dm.entry_exists("immersed_proportion")
                              ? dm.get<real const, 3>("immersed_proportion").data() : nullptr;
-    check(pu_dycore_init(h, &v, prop, PU_MEM_AUTO));
+    // The optional windmill projection joins the proportion (:1019-1025).
+    const double *proj = dm.entry_exists("windmill_proj_weight")
+                             ? dm.get<real const, 3>("windmill_proj_weight").data() : nullptr;
+    check(pu_dycore_init_windmill(h, &v, prop, proj, PU_MEM_AUTO));
 
     // Entries the reference's init registers for other modules (:951-956, :961-966, :1152-1154).
     const int nz = cfg.nz, nzh = nz + 2 * hs;

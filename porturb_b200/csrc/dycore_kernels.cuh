@@ -731,6 +731,13 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : (s
   }
 }
 
+// a += b elementwise.
+template <class T>
+__global__ void k_add_inplace(T *__restrict__ a, const T *__restrict__ b, size_t n) {
+  const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e < n) a[e] += b[e];
+}
+
 // Enforcement pass on a state in place (the call at the top of
 // time_step_rk_3_3, dynamics_rk.h:301).
 template <class R, int NTR, bool IMM>

@@ -328,7 +328,7 @@ struct ImplBase {
         if (q) cudaFree(q);
   }
   virtual int alloc() = 0;
-  virtual int init(const pu_state_view *v, const double *prop, int mem) = 0;
+  virtual int init(const pu_state_view *v, const double *prop, int mem, const double *proj = nullptr) = 0;
   virtual int load_state(const pu_state_view *v) = 0;
   virtual int store_state(pu_state_view *v) = 0;
   virtual int advance(double dt, int nsteps) = 0;
@@ -548,7 +548,7 @@ struct Impl : ImplBase {
 
   unsigned blocks(size_t n, int bs) const { return unsigned((n + bs - 1) / bs); }
 
-  int init(const pu_state_view *v, const double *prop, int mem) override {
+  int init(const pu_state_view *v, const double *prop, int mem, const double *proj = nullptr) override {
     CouplerPtrs cp;
     PU_TRY(device_view(v, cp));
     const Thermo th = thermo();
@@ -567,15 +567,35 @@ struct Impl : ImplBase {
       if (resolve_mem(mem, prop) == PU_MEM_DEVICE)
         PU_CK(cudaMemcpyAsync(dprop, prop, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
       else PU_CK(cudaMemcpyAsync(dprop, prop, N * sizeof(double), cudaMemcpyHostToDevice, st));
+      int rc = PU_OK;
+      double *dproj = nullptr;
+      if (proj) {
+        // The windmill projection weight joins the proportion before the
+        // halos, flags and time scales are built (dynamics_rk.h:1019-1025).
+        rc = dalloc(dproj, N);
+        if (rc == PU_OK) {
+          cudaMemcpyAsync(dproj, proj, N * sizeof(double),
+                          resolve_mem(mem, proj) == PU_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                          st);
+          k_add_inplace<double><<<blocks(N, 256), 256, 0, st>>>(dprop, dproj, N);
+          const cudaError_t e = cudaGetLastError();
+          if (e != cudaSuccess) {
+            set_error(std::string("kernel launch: ") + cudaGetErrorString(e));
+            rc = PU_ERR_CUDA;
+          } else {
+            launches++;
+          }
+        }
+      }
       uint8_t *d0 = nullptr, *d1 = nullptr, *dz = nullptr;
-      int rc = dalloc(d0, N);
+      if (rc == PU_OK) rc = dalloc(d0, N);
       if (rc == PU_OK) rc = dalloc(d1, N);
       if (rc == PU_OK) rc = dalloc(dz, N);
       int *anyp = nullptr;
       if (rc == PU_OK) rc = dalloc(anyp, 1);
       if (rc == PU_OK) rc = imm_prepare(dprop, d0, d1, dz, anyp);
       cudaStreamSynchronize(st);
-      for (void *p : {(void *)dprop, (void *)d0, (void *)d1, (void *)dz, (void *)anyp})
+      for (void *p : {(void *)dprop, (void *)dproj, (void *)d0, (void *)d1, (void *)dz, (void *)anyp})
         if (p) cudaFree(p);
       if (rc != PU_OK) return rc;
     }

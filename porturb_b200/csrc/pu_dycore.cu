@@ -147,6 +147,15 @@ int pu_dycore_init(pu_dycore *h, const pu_state_view *coupler, const double *imm
   return h->impl->init(coupler, immersed_proportion, mem);
 }
 
+int pu_dycore_init_windmill(pu_dycore *h, const pu_state_view *coupler, const double *immersed_proportion,
+                            const double *windmill_proj_weight, int mem) {
+  if (!h || !coupler) return fail(PU_ERR_INVALID, "null argument");
+  if (windmill_proj_weight && !immersed_proportion)
+    return fail(PU_ERR_INVALID, "windmill_proj_weight needs immersed_proportion");
+  DeviceGuard g(h->device);
+  return h->impl->init(coupler, immersed_proportion, mem, windmill_proj_weight);
+}
+
 int pu_dycore_compute_time_step(const pu_dycore *h, double *dt) {
   if (!h || !dt) return fail(PU_ERR_INVALID, "null argument");
   const pu_config &c = h->impl->cfg;

@@ -120,9 +120,19 @@ class Dycore:
             pass
 
     # -- reference entry points -------------------------------------------
-    def init(self, rho_d, u, v, w, T, tracers, immersed_proportion=None):
+    def init(self, rho_d, u, v, w, T, tracers, immersed_proportion=None, windmill_proj_weight=None):
+        """windmill_proj_weight (optional) is added to immersed_proportion
+        before the immersed arrays are built (dynamics_rk.h:1019-1025)."""
         view = make_view(rho_d, u, v, w, T, tracers)
-        if immersed_proportion is None:
+        if windmill_proj_weight is not None:
+            if immersed_proportion is None:
+                raise ValueError("windmill_proj_weight needs immersed_proportion")
+            p, m = _ptr(immersed_proportion)
+            q, mq = _ptr(windmill_proj_weight)
+            if mq != m:
+                raise ValueError("immersed_proportion and windmill_proj_weight must be in the same memory")
+            check(self.lib.pu_dycore_init_windmill(self.h, C.byref(view), p, q, m))
+        elif immersed_proportion is None:
             check(self.lib.pu_dycore_init(self.h, C.byref(view), None, view.mem))
         else:
             p, m = _ptr(immersed_proportion)
@@ -440,7 +450,8 @@ class Dynamics_Euler_Stratified_WenoFV:
                    specs, opts, precision=self.precision, device=self.device, stream=stream, z_chunk=self.z_chunk)
         (rd, u, v, w, T), trs = self._state_arrays(coupler)
         prop = coupler.get("immersed_proportion") if coupler.entry_exists("immersed_proportion") else None
-        h.init(rd, u, v, w, T, trs, prop)
+        proj = coupler.get("windmill_proj_weight") if coupler.entry_exists("windmill_proj_weight") else None
+        h.init(rd, u, v, w, T, trs, prop, proj)
         coupler.module_state["pu_dycore"] = h
         # The entries other modules read from the data manager (:951-956, :961-966, :1152-1154).
         dm = coupler.dm

@@ -283,6 +283,68 @@ int pu_dycore_time_step_noalloc(const pu_config *cfg, const double *hy_dens_cell
                                 const double *hy_pressure_cells, pu_state_view *coupler, double dt_phys,
                                 int *ncycles);
 
+/* ---------------------------------------------------------------------------
+ * Domain decomposition across GPUs (coupler.h:132-229): a handle can be one
+ * (px, py) tile of an nproc_x x nproc_y grid of tiles over an nx_glob x
+ * ny_glob domain; its cfg.nx, cfg.ny are the tile's sizes and the coupler
+ * arrays it takes are the tile's.  Every stage the tile sends the 5 columns
+ * (rows) of the stage input next to each x (y) edge to the neighbouring tile
+ * and receives the neighbour's, which its x/y kernel reads beyond its edges
+ * (the halo exchange of coupler.h:985-1165 and the edge exchange of
+ * dynamics_rk.h:808-912).  Neighbours wrap periodically; precursor
+ * conditions apply at the global edges only.  Init sums the hydrostatic
+ * profiles over all tiles and builds the immersed flags from a 12-cell halo
+ * of immersed_proportion.  Tiles must be at least 12 cells wide in x and y
+ * (ny_glob == 1: one tile row, ny = 1); tiles in one column of the grid have
+ * the same nx, tiles in one row the same ny.  Plain WENO only (no learned
+ * weights).
+ * ------------------------------------------------------------------------- */
+typedef struct pu_decomp {
+  int nproc_x, nproc_y;      /* tile grid; rank = py*nproc_x + px */
+  int px, py;                /* this tile */
+  long long nx_glob, ny_glob;
+} pu_decomp;
+
+#define PU_NCCL_ID_BYTES 128
+
+/* The process grid the reference's coupler picks for nranks tasks
+ * (coupler.h:148-171): nproc_y is the divisor of nranks whose
+ * nproc_y/(nranks/nproc_y) is closest to ny_glob/nx_glob (the first of equals),
+ * nproc_x = nranks/nproc_y; ny_glob == 1 gives nranks x 1.  Host only. */
+int pu_decomp_process_grid(int nranks, long long nx_glob, long long ny_glob, int *nproc_x, int *nproc_y);
+/* First index and size of tile p of nproc along an axis of n_glob cells
+ * (coupler.h:176-183: beg = round(n_glob/nproc*p), end = round(n_glob/nproc*(p+1))-1).
+ * Host only. */
+int pu_decomp_tile(long long n_glob, int nproc, int p, long long *beg, long long *n);
+/* Ranks of the tiles beyond the x-, x+, y-, y+ edges of tile (px, py)
+ * (coupler.h:203-214).  Host only. */
+int pu_decomp_neighbors(const pu_decomp *d, int nbr[4]);
+
+/* A new NCCL unique id (PU_NCCL_ID_BYTES bytes) for pu_dycore_set_decomposition;
+ * one rank makes it and the host broadcasts it to the others.  NCCL is loaded
+ * from libnccl.so.2 on first use (the copy already in the process, if any). */
+int pu_nccl_get_unique_id(unsigned char *id);
+
+/* Makes the handle a tile of a decomposed domain; call before pu_dycore_init.
+ * With an NCCL id, every tile is a separate rank (one process or thread per
+ * GPU) and this call, init and every time step are collective over the
+ * nproc_x*nproc_y ranks (it creates the NCCL communicator and checks that
+ * the tiles' sizes fit together, failing on every rank alike if they do
+ * not).  With id NULL the tiles of the grid are handles of one process on
+ * one stream, driven by the pu_dycore_group_* calls. */
+int pu_dycore_set_decomposition(pu_dycore *h, const pu_decomp *d, const unsigned char *nccl_id);
+
+/* init, advance and time_step of an in-process group: hs holds the n =
+ * nproc_x*nproc_y tiles (any order) made with pu_dycore_set_decomposition(h,
+ * d, NULL), on one device and one stream; views[i], props[i], projs[i] are
+ * tile i's coupler arrays, immersed_proportion and windmill_proj_weight
+ * (props / projs NULL, or entries NULL, for none).  The tiles advance stage
+ * by stage together (pack, exchange by device copies, x/y and z kernels). */
+int pu_dycore_group_init(pu_dycore *const *hs, int n, const pu_state_view *views, const double *const *props,
+                         const double *const *projs, int mem);
+int pu_dycore_group_advance(pu_dycore *const *hs, int n, double dt, int nsteps);
+int pu_dycore_group_time_step(pu_dycore *const *hs, int n, pu_state_view *views, double dt_phys, int *ncycles);
+
 #ifdef __cplusplus
 }
 #endif

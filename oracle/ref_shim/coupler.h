@@ -59,6 +59,9 @@ class ParallelComm {
   T all_reduce(T v, MPI_Op) const { return v; }
   template <class T>
   T all_reduce(T v, MPI_Op, std::string) const { return v; }
+  // broadcast of one value at one rank: nothing moves (ParallelComm.h:184-188).
+  template <class T>
+  void broadcast(T &, int = 0, std::string = "") const {}
 };
 
 class DataManager {

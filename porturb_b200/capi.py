@@ -81,6 +81,14 @@ class pu_physics_config(C.Structure):
                 ("device", C.c_int), ("stream", C.c_void_p)]
 
 
+class pu_decomp(C.Structure):
+    _fields_ = [("nproc_x", C.c_int), ("nproc_y", C.c_int), ("px", C.c_int), ("py", C.c_int),
+                ("nx_glob", C.c_longlong), ("ny_glob", C.c_longlong)]
+
+
+PU_NCCL_ID_BYTES = 128
+
+
 class pu_uniform_pg_state(C.Structure):
     _fields_ = [("counter", C.c_ulonglong), ("u0", C.c_double), ("v0", C.c_double),
                 ("u", C.c_double), ("v", C.c_double)]
@@ -127,6 +135,14 @@ SIGNATURES = {
     "pu_dycore_profile_read": (_I, [_P, C.POINTER(pu_profile)]),
     "pu_dycore_time_step_noalloc": (_I, [C.POINTER(pu_config), _P, _P, _P, C.POINTER(pu_state_view), _D,
                                          C.POINTER(_I)]),
+    "pu_decomp_process_grid": (_I, [_I, C.c_longlong, C.c_longlong, C.POINTER(_I), C.POINTER(_I)]),
+    "pu_decomp_tile": (_I, [C.c_longlong, _I, _I, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
+    "pu_decomp_neighbors": (_I, [C.POINTER(pu_decomp), C.POINTER(_I)]),
+    "pu_nccl_get_unique_id": (_I, [C.c_char_p]),
+    "pu_dycore_set_decomposition": (_I, [_P, C.POINTER(pu_decomp), C.c_char_p]),
+    "pu_dycore_group_init": (_I, [C.POINTER(_P), _I, C.POINTER(pu_state_view), C.POINTER(_P), C.POINTER(_P), _I]),
+    "pu_dycore_group_advance": (_I, [C.POINTER(_P), _I, _D, _I]),
+    "pu_dycore_group_time_step": (_I, [C.POINTER(_P), _I, C.POINTER(pu_state_view), _D, C.POINTER(_I)]),
     # include/pu_physics.h
     "pu_physics_create": (_I, [C.POINTER(pu_physics_config), _P, _P, _P, _I, C.POINTER(C.c_void_p)]),
     "pu_physics_destroy": (_I, [_P]),

@@ -114,6 +114,20 @@ struct Dynamics_Euler_Stratified_WenoFV {
     pu_dycore *h = nullptr;
     check(pu_dycore_create(&cfg, &h));
     coupler.set_option<size_t>("pu_dycore_handle", reinterpret_cast<size_t>(h));
+    // A coupler distributed over several ranks (coupler.h:132-229): this
+    // rank's handle becomes its tile of the domain, exchanging halos with the
+    // other ranks' tiles over NCCL.  Rank 0 (px = py = 0) makes the NCCL id
+    // and broadcasts it over the coupler's communicator.
+    if (coupler.get_nproc_x() * coupler.get_nproc_y() > 1) {
+      int id[PU_NCCL_ID_BYTES / sizeof(int)] = {};
+      if (coupler.get_px() == 0 && coupler.get_py() == 0)
+        check(pu_nccl_get_unique_id(reinterpret_cast<unsigned char *>(id)));
+      auto comm = coupler.get_parallel_comm();
+      for (auto &w : id) comm.broadcast(w, 0);
+      pu_decomp d{coupler.get_nproc_x(), coupler.get_nproc_y(), coupler.get_px(), coupler.get_py(),
+                  (long long)coupler.get_nx_glob(), (long long)coupler.get_ny_glob()};
+      check(pu_dycore_set_decomposition(h, &d, reinterpret_cast<unsigned char *>(id)));
+    }
 
     auto &dm = coupler.get_data_manager_readwrite();
     pu_state_view v = coupler_view(coupler);

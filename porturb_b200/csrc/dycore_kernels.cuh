@@ -85,6 +85,16 @@ struct Grid {
   const uint8_t *flags;         // FLAG_IMM | FLAG_ANY10 per cell, or null
   const R *imm_mult;            // immersed_proportion^power / tau per cell, or null
   int *err;                     // bit 0: a non-finite value was written
+  // Decomposed tiles (k_xy with DECOMP): the stage input's raw state beyond
+  // the tile's x and y edges, received from the neighbouring tiles, as slabs
+  // [S][nz][ny][HALO_W] (x: hxl below i = 0, hxr from i = nx) and
+  // [S][nz][HALO_W][nx] (y), with their immersed flags ([nz][ny][HALO_W],
+  // [nz][HALO_W][nx]).  gx0/gx1/gy0/gy1: the tile's low/high x/y edge is the
+  // global domain edge (precursor conditions apply only there; 1 for an
+  // undecomposed domain).
+  const R *hxl, *hxr, *hyl, *hyr;
+  const uint8_t *fxl, *fxr, *fyl, *fyr;
+  int gx0, gx1, gy0, gy1;
   // Learned WENO weights (kernels instantiated with LEARNED only).
   const uint32_t *ml_frags;     // per-lane operand fragments of the network
   unsigned long long *ml_counts;  // [0] stencils given learned weights, [1] limiter fallbacks
@@ -106,9 +116,11 @@ __device__ __forceinline__ double pu_expm1(double x) { return expm1(x); }
 // rho', u, v, w, theta', p', tracer mixing ratios.  theta' and p' are formed
 // from the perturbation storage without cancellation:
 //   theta' = (q4 - theta_h q0)/rho,   p' = P0_h*expm1(gamma*log1p(q4/(rho theta)_h)) + (P0_h - p_h).
+// s holds the S raw fields N elements apart (the resident arrays, N = nz*ny*nx,
+// or a halo slab).
 template <class R, int NTR>
-__device__ __forceinline__ void prims(const Grid<R> &G, const R *__restrict__ s, size_t idx, int k, R (&w)[6 + NTR]) {
-  const size_t N = G.N;
+__device__ __forceinline__ void prims_s(const Grid<R> &G, const R *__restrict__ s, size_t N, size_t idx, int k,
+                                        R (&w)[6 + NTR]) {
   const int kh = k + HS;
   R q0 = __ldg(s + idx), q1 = __ldg(s + N + idx), q2 = __ldg(s + 2 * N + idx), q3 = __ldg(s + 3 * N + idx),
     q4 = __ldg(s + 4 * N + idx);
@@ -122,6 +134,79 @@ __device__ __forceinline__ void prims(const Grid<R> &G, const R *__restrict__ s,
   w[5] = fma(__ldg(G.p0_h + kh), pu_expm1(G.gamma * pu_log1p(q4 * __ldg(G.rt_inv + kh))), __ldg(G.dp_h + kh));
 #pragma unroll
   for (int t = 0; t < NTR; t++) w[6 + t] = __ldg(s + (5 + t) * N + idx) * rr;
+}
+
+template <class R, int NTR>
+__device__ __forceinline__ void prims(const Grid<R> &G, const R *__restrict__ s, size_t idx, int k, R (&w)[6 + NTR]) {
+  prims_s<R, NTR>(G, s, G.N, idx, k, w);
+}
+
+// Width of the halo a decomposed tile receives from each neighbour: the
+// order-9 stencils of cells -1 and n reach 5 cells beyond the tile.
+constexpr int HALO_W = 5;
+
+// Where the state and the immersed flags of cell (gi, gj) of level k come
+// from in a decomposed tile: the tile's own arrays, the receive slab beyond
+// an x or a y edge, or -- at a global precursor edge, for the state only --
+// the nearest tile cell (halo_boundary_conditions, dynamics_rk.h:745-790;
+// the immersed halos are exchanged periodically, :1026-1032).  Cells beyond
+// both an x and a y edge, and cells more than HALO_W beyond an edge, are only
+// read by stencils of cells outside the tile, whose results are discarded;
+// they read the nearest valid cell.
+template <class R>
+__device__ __forceinline__ void tile_source(const Grid<R> &G, const R *sin, int gi, int gj, int k, const R *&src,
+                                            size_t &fs, size_t &q, const uint8_t *&fl) {
+  const int nx = G.nx, ny = G.ny;
+  // A 2-D domain (ny == 1) has no y halo: rows beyond it belong to stencils
+  // of rows outside the domain and read row 0, as the periodic wrap does.
+  const bool ox = gi < 0 || gi >= nx, oy = !G.sim2d && (gj < 0 || gj >= ny);
+  if (ox && !oy) {
+    const int col = gi < 0 ? gi + HALO_W : min(gi - nx, HALO_W - 1);
+    const size_t e = (size_t(k) * ny + gj) * HALO_W + col;
+    fl = (gi < 0 ? G.fxl : G.fxr) ? (gi < 0 ? G.fxl : G.fxr) + e : nullptr;
+    if (G.bc_x == BC_PRECURSOR && (gi < 0 ? G.gx0 : G.gx1)) {
+      src = sin;
+      fs = G.N;
+      q = size_t(k) * G.NP + size_t(gj) * nx + clampi(gi, nx);
+    } else {
+      src = gi < 0 ? G.hxl : G.hxr;
+      fs = size_t(G.nz) * ny * HALO_W;
+      q = e;
+    }
+  } else if (oy && !ox) {
+    const int row = gj < 0 ? gj + HALO_W : min(gj - ny, HALO_W - 1);
+    const size_t e = (size_t(k) * HALO_W + row) * nx + gi;
+    fl = (gj < 0 ? G.fyl : G.fyr) ? (gj < 0 ? G.fyl : G.fyr) + e : nullptr;
+    if (G.bc_y == BC_PRECURSOR && (gj < 0 ? G.gy0 : G.gy1)) {
+      src = sin;
+      fs = G.N;
+      q = size_t(k) * G.NP + size_t(clampi(gj, ny)) * nx + gi;
+    } else {
+      src = gj < 0 ? G.hyl : G.hyr;
+      fs = size_t(G.nz) * HALO_W * nx;
+      q = e;
+    }
+  } else {
+    src = sin;
+    fs = G.N;
+    q = size_t(k) * G.NP + size_t(clampi(gj, ny)) * nx + clampi(gi, nx);
+    fl = G.flags ? G.flags + q : nullptr;
+  }
+}
+
+// Copies a bx x by box of each of bz stacked planes between two arrays of
+// planes (x fastest): dst[(p*dyn + dj0 + j)*dxn + di0 + i] =
+// src[(p*syn + sj0 + j)*sxn + si0 + i].  Halo slabs of decomposed tiles are
+// packed, assembled and cropped with it (fields are stacked planes too).
+template <class T>
+__global__ void k_box(const T *__restrict__ src, int sxn, int syn, int si0, int sj0, T *__restrict__ dst, int dxn,
+                      int dyn, int di0, int dj0, int bx, int by, int bz) {
+  const size_t n = size_t(bx) * by * bz;
+  for (size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += size_t(gridDim.x) * blockDim.x) {
+    const int i = int(e % bx), j = int((e / bx) % by);
+    const size_t p = e / (size_t(bx) * by);
+    dst[(p * dyn + dj0 + j) * size_t(dxn) + di0 + i] = src[(p * syn + sj0 + j) * size_t(sxn) + si0 + i];
+  }
 }
 
 // Upwind Riemann flux across one face (dynamics_rk.h:640-706): acoustic
@@ -253,7 +338,7 @@ __device__ __forceinline__ void recon_packed(int total, Load load, Store store) 
 // x/y fluxes and their divergence for one (x,y) tile of one level.
 // LEARNED (FP32, weno_all only): edges from the network's weights, with the
 // plain limiter as the fallback.
-template <class R, int NTR, int TX, int TY, bool IMM, bool LEARNED = false>
+template <class R, int NTR, int TX, int TY, bool IMM, bool LEARNED = false, bool DECOMP = false>
 __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (sizeof(R) == 4 ? PU_XY_MIN_BLOCKS : 1)) k_xy(const Grid<R> G, const R *__restrict__ sin, R *__restrict__ txy) {
   using Sh = XYShape<R, NTR, TX, TY, IMM, LEARNED>;
   constexpr int F = Sh::F, S = Sh::S, NT = Sh::NT, HX = Sh::HX, HY = Sh::HY, EN = Sh::EN, FN = Sh::FN;
@@ -288,13 +373,22 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
       r = rr < 5 ? rr : rr + TY;
     }
     const int gi = i0 - 5 + c, gj = j0 - 5 + r;
-    const int vi = G.bc_x == BC_PRECURSOR ? clampi(gi, nx) : wrapi(gi, nx);
-    const int vj = G.bc_y == BC_PRECURSOR ? clampi(gj, ny) : wrapi(gj, ny);
     R w[F];
-    prims<R, NTR>(G, sin, plane + size_t(vj) * nx + vi, k, w);
+    if constexpr (DECOMP) {
+      const R *src;
+      size_t fs, q;
+      const uint8_t *fl;
+      tile_source(G, sin, gi, gj, k, src, fs, q, fl);
+      prims_s<R, NTR>(G, src, fs, q, k, w);
+      if (IMM) M[r * HX + c] = fl ? __ldg(fl) : uint8_t(0);
+    } else {
+      const int vi = G.bc_x == BC_PRECURSOR ? clampi(gi, nx) : wrapi(gi, nx);
+      const int vj = G.bc_y == BC_PRECURSOR ? clampi(gj, ny) : wrapi(gj, ny);
+      prims<R, NTR>(G, sin, plane + size_t(vj) * nx + vi, k, w);
+      if (IMM) M[r * HX + c] = __ldg(G.flags + plane + size_t(wrapi(gj, ny)) * nx + wrapi(gi, nx));
+    }
 #pragma unroll
     for (int f = 0; f < F; f++) H[(f * HY + r) * HX + c] = w[f];
-    if (IMM) M[r * HX + c] = __ldg(G.flags + plane + size_t(wrapi(gj, ny)) * nx + wrapi(gi, nx));
   }
   __syncthreads();
 
@@ -356,8 +450,8 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
       const int gf = i0 + fi;
 #pragma unroll
       for (int f = 0; f < F; f++) {
-        if (gf == 0) L[f] = Rt[f];
-        if (gf == nx) Rt[f] = L[f];
+        if (gf == 0 && G.gx0) L[f] = Rt[f];
+        if (gf == nx && G.gx1) Rt[f] = L[f];
       }
     }
     R fl[S];
@@ -427,8 +521,8 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
         const int gf = j0 + fj;
 #pragma unroll
         for (int f = 0; f < F; f++) {
-          if (gf == 0) L[f] = Rt[f];
-          if (gf == ny) Rt[f] = L[f];
+          if (gf == 0 && G.gy0) L[f] = Rt[f];
+          if (gf == ny && G.gy1) Rt[f] = L[f];
         }
       }
       R fl[S];

@@ -15,6 +15,7 @@
 #include "../../include/pu_dycore.h"
 #include "dycore_kernels.cuh"
 #include "learned.cuh"
+#include "nccl_dyn.h"
 
 namespace pu {
 
@@ -38,6 +39,46 @@ void set_error(const std::string &msg);
     }                                                                                     \
     launches++;                                                                           \
   } while (0)
+
+// ---------------------------------------------------------------------------
+// Domain decomposition (coupler.h:132-229): a handle can be the (px, py) tile
+// of an nproc_x x nproc_y grid of tiles over the global domain; the halos
+// beyond its x and y edges come from the neighbouring tiles every stage
+// (coupler.h:985-1165, dynamics_rk.h:808-912).
+// ---------------------------------------------------------------------------
+// Buffers of one halo exchange, per direction d = x-, x+, y-, y+: snd[d] holds
+// this tile's cells next to edge d, rcv[d] receives the neighbour's cells
+// beyond edge d (the neighbour's snd[d ^ 1]).
+struct HaloSet {
+  void *snd[4] = {nullptr, nullptr, nullptr, nullptr};
+  void *rcv[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t bytes[4] = {0, 0, 0, 0};
+  void release() {
+    for (int d = 0; d < 4; d++) {
+      if (snd[d]) cudaFree(snd[d]);
+      if (rcv[d]) cudaFree(rcv[d]);
+      snd[d] = rcv[d] = nullptr;
+      bytes[d] = 0;
+    }
+  }
+};
+
+// Width of the immersed-proportion halo gathered at init: the any_immersed10
+// flag of a halo cell next to the tile (the centre of the stencils of cells
+// -1 and n) looks 10 cells further.
+constexpr int INIT_HALO = 12;
+
+struct Decomposition {
+  bool on = false;
+  pu_decomp d{};
+  int rank = 0, nranks = 1;  // rank = py*nproc_x + px (coupler.h:168-171)
+  int nbr[4] = {0, 0, 0, 0}; // ranks beyond the x-, x+, y-, y+ edges, periodic (coupler.h:203-214)
+  ncclComm_t comm = nullptr; // null: an in-process group of tiles (pu_dycore_group_*)
+  HaloSet state;             // the stage input's raw state, HALO_W wide
+  uint8_t *fslab[4] = {nullptr, nullptr, nullptr, nullptr};  // immersed flags of the cells in state.rcv
+  HaloSet ix, iy;            // the immersed proportion at init, INIT_HALO wide (FP64)
+  double *dprop = nullptr, *ext_x = nullptr, *ext = nullptr;  // init scratch
+};
 
 struct ImplBase {
   pu_config cfg{};
@@ -320,7 +361,73 @@ struct ImplBase {
 
   virtual int ml_harvest(long n, unsigned long long seed) = 0;
 
+  // ---- decomposition ----
+  Decomposition dc;
+  bool sim2d() const { return cfg.ny == 1; }
+  HaloSet &halo(int which) { return which == 0 ? dc.state : which == 1 ? dc.ix : dc.iy; }
+  void dec_release() {
+    dc.state.release();
+    dc.ix.release();
+    dc.iy.release();
+    for (auto &f : dc.fslab) {
+      if (f) cudaFree(f);
+      f = nullptr;
+    }
+    for (double **p : {&dc.dprop, &dc.ext_x, &dc.ext}) {
+      if (*p) cudaFree(*p);
+      *p = nullptr;
+    }
+    if (dc.comm && nccl().ok) nccl().CommDestroy(dc.comm);
+    dc.comm = nullptr;
+  }
+  int nccl_fail(ncclResult_t r, const char *what) {
+    set_error(std::string(what) + ": " + (nccl().ok ? nccl().GetErrorString(r) : "NCCL unavailable"));
+    return PU_ERR_CUDA;
+  }
+  // Posts the exchange of one HaloSet with NCCL on the handle's stream.  Per
+  // direction pair the posts are (send snd[lo] to the low neighbour, receive
+  // rcv[hi] from the high one, send snd[hi] to the high neighbour, receive
+  // rcv[lo] from the low one); NCCL matches the sends and receives between
+  // two ranks in the order they are posted, so with one or two tiles across a
+  // direction (both neighbours the same rank) every rank's first message to
+  // the other is its snd[lo], which the other takes into rcv[hi].
+  int nccl_exchange(HaloSet &h, bool x, bool y) {
+    auto &api = nccl();
+    if (!api.ok || !dc.comm) {
+      set_error("NCCL halo exchange without a communicator");
+      return PU_ERR_STATE;
+    }
+    ncclResult_t r = api.GroupStart();
+    if (r != ncclSuccess) return nccl_fail(r, "ncclGroupStart");
+    ncclResult_t first = ncclSuccess;
+    auto note = [&](ncclResult_t q) {
+      if (q != ncclSuccess && first == ncclSuccess) first = q;
+    };
+    for (int a = 0; a < 2; a++) {
+      if ((a == 0 && !x) || (a == 1 && !y)) continue;
+      const int lo = 2 * a, hi = lo + 1;
+      note(api.Send(h.snd[lo], h.bytes[lo], ncclUint8, dc.nbr[lo], dc.comm, st));
+      note(api.Recv(h.rcv[hi], h.bytes[hi], ncclUint8, dc.nbr[hi], dc.comm, st));
+      note(api.Send(h.snd[hi], h.bytes[hi], ncclUint8, dc.nbr[hi], dc.comm, st));
+      note(api.Recv(h.rcv[lo], h.bytes[lo], ncclUint8, dc.nbr[lo], dc.comm, st));
+    }
+    r = api.GroupEnd();
+    if (first != ncclSuccess) return nccl_fail(first, "ncclSend/ncclRecv");
+    if (r != ncclSuccess) return nccl_fail(r, "ncclGroupEnd");
+    return PU_OK;
+  }
+  // Type-dependent parts of the decomposed path (Impl).
+  virtual int dec_alloc() = 0;
+  virtual int dinit_begin(const pu_state_view *v, const double *prop, const double *proj, int mem) = 0;
+  virtual int dinit_hydro(const double *global_sums) = 0;
+  virtual int dinit_mid() = 0;
+  virtual int dinit_end(const pu_state_view *v) = 0;
+  virtual int dec_enforce() = 0;
+  virtual int dec_pack(int stage) = 0;
+  virtual int dec_compute(int stage, double dt, bool last) = 0;
+
   virtual ~ImplBase() {
+    dec_release();
     for (auto e : ev_pool) cudaEventDestroy(e);
     if (owns)
       for (void *q : {(void *)ml_theta, (void *)ml_m, (void *)ml_v, (void *)ml_wq, (void *)ml_grad, (void *)ml_partial,
@@ -450,6 +557,18 @@ struct Impl : ImplBase {
                                int(XYShape<R, NTR, XTX_SM, XTY_SM, false>::bytes)));
     PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_SM, XTY_SM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(XYShape<R, NTR, XTX_SM, XTY_SM, true>::bytes)));
+    PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_BIG, XTY_BIG, false, false, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(XYShape<R, NTR, XTX_BIG, XTY_BIG, false>::bytes)));
+    PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_BIG, XTY_BIG, true, false, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(XYShape<R, NTR, XTX_BIG, XTY_BIG, true>::bytes)));
+    PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_SM, XTY_SM, false, false, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(XYShape<R, NTR, XTX_SM, XTY_SM, false>::bytes)));
+    PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_SM, XTY_SM, true, false, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(XYShape<R, NTR, XTX_SM, XTY_SM, true>::bytes)));
     PU_CK(cudaFuncSetAttribute(k_z<R, NTR, ZTX, ZTY, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(ZShape<R, NTR, ZTX, ZTY>::bytes)));
     PU_CK(cudaFuncSetAttribute(k_z<R, NTR, ZTX, ZTY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -516,6 +635,18 @@ struct Impl : ImplBase {
     G.rt_target = lt.rt_target;
     G.flags = has_imm ? flags : nullptr;
     G.imm_mult = has_imm ? static_cast<const R *>(imm_mult) : nullptr;
+    G.hxl = static_cast<const R *>(dc.state.rcv[0]);
+    G.hxr = static_cast<const R *>(dc.state.rcv[1]);
+    G.hyl = static_cast<const R *>(dc.state.rcv[2]);
+    G.hyr = static_cast<const R *>(dc.state.rcv[3]);
+    G.fxl = has_imm ? dc.fslab[0] : nullptr;
+    G.fxr = has_imm ? dc.fslab[1] : nullptr;
+    G.fyl = has_imm ? dc.fslab[2] : nullptr;
+    G.fyr = has_imm ? dc.fslab[3] : nullptr;
+    G.gx0 = !dc.on || dc.d.px == 0;
+    G.gx1 = !dc.on || dc.d.px == dc.d.nproc_x - 1;
+    G.gy0 = !dc.on || dc.d.py == 0;
+    G.gy1 = !dc.on || dc.d.py == dc.d.nproc_y - 1;
     G.err = err;
     G.ml_frags = ml_frags;
     G.ml_counts = ml_counts;
@@ -549,6 +680,20 @@ struct Impl : ImplBase {
   unsigned blocks(size_t n, int bs) const { return unsigned((n + bs - 1) / bs); }
 
   int init(const pu_state_view *v, const double *prop, int mem, const double *proj = nullptr) override {
+    if (dc.on) {
+      if (!dc.comm) {
+        set_error("the tiles of an in-process group are initialised with pu_dycore_group_init");
+        return PU_ERR_STATE;
+      }
+      PU_TRY(dinit_begin(v, prop, proj, mem));
+      const ncclResult_t r = nccl().AllReduce(sums, sums, size_t(3) * cfg.nz, ncclFloat64, ncclSum, dc.comm, st);
+      if (r != ncclSuccess) return nccl_fail(r, "ncclAllReduce");
+      PU_TRY(dinit_hydro(nullptr));
+      PU_TRY(nccl_exchange(dc.ix, true, false));
+      PU_TRY(dinit_mid());
+      if (!sim2d()) PU_TRY(nccl_exchange(dc.iy, false, true));
+      return dinit_end(v);
+    }
     CouplerPtrs cp;
     PU_TRY(device_view(v, cp));
     const Thermo th = thermo();
@@ -683,15 +828,17 @@ struct Impl : ImplBase {
     return std::is_same<R, float>::value && weno_mode == PU_WENO_LEARNED && ml_ready && cfg.weno_all;
   }
 
-  template <bool IMM, bool LRN>
+  // One SSPRK3 stage: the x/y kernel (DEC: a decomposed tile reading its
+  // received halo slabs), then the z march with the stage combination.
+  template <bool IMM, bool LRN, bool DEC = false>
   int stage(const Grid<R> &G, const R *sin, const R *sn, R *sout, R a_n, R a_dt, int n_enforce) {
-    constexpr bool L = LRN && std::is_same<R, float>::value;
+    constexpr bool L = LRN && std::is_same<R, float>::value && !DEC;
     R *t = static_cast<R *>(txy);
     cudaEvent_t e0 = prof_begin();
     if (small_tile) {
       using Sh = XYShape<R, NTR, XTX_SM, XTY_SM, IMM, L>;
       dim3 g(blocks(cfg.nx, XTX_SM), blocks(cfg.ny, XTY_SM), cfg.nz);
-      k_xy<R, NTR, XTX_SM, XTY_SM, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
+      k_xy<R, NTR, XTX_SM, XTY_SM, IMM, L, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
     } else if (L) {
       using Sh = XYShape<R, NTR, LTX, LTY, IMM, L>;
       dim3 g(blocks(cfg.nx, LTX), blocks(cfg.ny, LTY), cfg.nz);
@@ -699,7 +846,7 @@ struct Impl : ImplBase {
     } else {
       using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM, false>;
       dim3 g(blocks(cfg.nx, XTX_BIG), blocks(cfg.ny, XTY_BIG), cfg.nz);
-      k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
+      k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
     }
     PU_LAUNCHED();
     prof_end(0, e0);
@@ -738,8 +885,272 @@ struct Impl : ImplBase {
 
   int advance(double dt, int nsteps) override {
     if (nsteps <= 0) return PU_OK;
+    if (dc.on) {
+      if (!dc.comm) {
+        set_error("the tiles of an in-process group advance with pu_dycore_group_advance");
+        return PU_ERR_STATE;
+      }
+      PU_TRY(dec_enforce());
+      for (int n = 0; n < nsteps; n++)
+        for (int sg = 0; sg < 3; sg++) {
+          PU_TRY(dec_pack(sg));
+          PU_TRY(nccl_exchange(dc.state, true, !sim2d()));
+          PU_TRY(dec_compute(sg, dt, n == nsteps - 1));
+        }
+      return PU_OK;
+    }
     if (learned_active()) return has_imm ? advance_t<true, true>(dt, nsteps) : advance_t<false, true>(dt, nsteps);
     return has_imm ? advance_t<true, false>(dt, nsteps) : advance_t<false, false>(dt, nsteps);
+  }
+
+  // ---- decomposed tiles ----
+  template <class T>
+  int box(const T *src, int sxn, int syn, int si0, int sj0, T *dst, int dxn, int dyn, int di0, int dj0, int bx,
+          int by, int bz) {
+    const size_t n = size_t(bx) * by * bz;
+    if (!n) return PU_OK;
+    const unsigned nb = unsigned(std::min<size_t>((n + 255) / 256, size_t(148) * 16));
+    k_box<T><<<nb, 256, 0, st>>>(src, sxn, syn, si0, sj0, dst, dxn, dyn, di0, dj0, bx, by, bz);
+    PU_LAUNCHED();
+    return PU_OK;
+  }
+
+  int dec_alloc() override {
+    const size_t W = HALO_W, nz = cfg.nz, nx = cfg.nx, ny = cfg.ny;
+    for (int d = 0; d < (sim2d() ? 2 : 4); d++) {
+      const size_t b = size_t(S) * nz * (d < 2 ? ny * W : W * nx) * sizeof(R);
+      unsigned char *p, *q;
+      PU_TRY(dalloc(p, b));
+      dc.state.snd[d] = p;
+      PU_TRY(dalloc(q, b));
+      dc.state.rcv[d] = q;
+      dc.state.bytes[d] = b;
+    }
+    return PU_OK;
+  }
+
+  // The HALO_W columns (rows) of the stage input next to each x (y) edge.
+  int dec_pack(int sg) override {
+    const R *sin = static_cast<const R *>(s[sg]);
+    const int nx = cfg.nx, ny = cfg.ny, W = HALO_W, P = S * cfg.nz;
+    R **snd = reinterpret_cast<R **>(dc.state.snd);
+    PU_TRY(box(sin, nx, ny, 0, 0, snd[0], W, ny, 0, 0, W, ny, P));
+    PU_TRY(box(sin, nx, ny, nx - W, 0, snd[1], W, ny, 0, 0, W, ny, P));
+    if (!sim2d()) {
+      PU_TRY(box(sin, nx, ny, 0, 0, snd[2], nx, W, 0, 0, nx, W, P));
+      PU_TRY(box(sin, nx, ny, 0, ny - W, snd[3], nx, W, 0, 0, nx, W, P));
+    }
+    return PU_OK;
+  }
+
+  int dec_enforce() override {
+    const Grid<R> G = grid();
+    R *s0 = static_cast<R *>(s[0]);
+    if (has_imm) k_enforce<R, NTR, true><<<blocks(N, 256), 256, 0, st>>>(G, s0);
+    else k_enforce<R, NTR, false><<<blocks(N, 256), 256, 0, st>>>(G, s0);
+    PU_LAUNCHED();
+    return PU_OK;
+  }
+
+  // Stage sg of the Shu-Osher SSPRK(3,3) step, as advance_t runs it.
+  template <bool IMM>
+  int dec_stage(const Grid<R> &G, int sg, double dt, bool last) {
+    R *s0 = static_cast<R *>(s[0]), *s1 = static_cast<R *>(s[1]), *s2 = static_cast<R *>(s[2]);
+    if (sg == 0) return stage<IMM, false, true>(G, s0, nullptr, s1, R(0), R(dt), 1);
+    if (sg == 1) return stage<IMM, false, true>(G, s1, s0, s2, R(3. / 4.), R(1. / 4. * dt), 1);
+    return stage<IMM, false, true>(G, s2, s0, s0, R(1. / 3.), R(2. / 3. * dt), last ? 1 : 2);
+  }
+  int dec_compute(int sg, double dt, bool last) override {
+    const Grid<R> G = grid();
+    return has_imm ? dec_stage<true>(G, sg, dt, last) : dec_stage<false>(G, sg, dt, last);
+  }
+
+  // Init of a tile, in phases between which the tiles exchange:
+  //   begin: column sums of the tile; the immersed proportion (zeros for
+  //          none, plus the windmill projection) and its INIT_HALO columns
+  //          next to each x edge;
+  //   (sum the column sums over the tiles)  hydro: the profiles;
+  //   (x exchange)  mid: the x-extended proportion and its rows next to
+  //          each y edge;
+  //   (y exchange)  end: the extended block, immersed flags and relaxation
+  //          factors on it, cropped to the tile and its halo slabs; the state.
+  int dinit_begin(const pu_state_view *v, const double *prop, const double *proj, int mem) override {
+    if (proj && !prop) {
+      set_error("windmill_proj_weight needs immersed_proportion");
+      return PU_ERR_INVALID;
+    }
+    CouplerPtrs cp;
+    PU_TRY(device_view(v, cp));
+    k_column_sums<NTR><<<cfg.nz, 256, 0, st>>>(cp, thermo(), cfg.nx, cfg.ny, sums);
+    PU_LAUNCHED();
+    PU_TRY(dalloc(dc.dprop, N));
+    if (prop) {
+      PU_CK(cudaMemcpyAsync(dc.dprop, prop, N * sizeof(double),
+                            resolve_mem(mem, prop) == PU_MEM_DEVICE ? cudaMemcpyDeviceToDevice
+                                                                    : cudaMemcpyHostToDevice,
+                            st));
+    } else {
+      PU_CK(cudaMemsetAsync(dc.dprop, 0, N * sizeof(double), st));
+    }
+    if (proj) {
+      double *dproj = nullptr;
+      PU_TRY(dalloc(dproj, N));
+      cudaMemcpyAsync(dproj, proj, N * sizeof(double),
+                      resolve_mem(mem, proj) == PU_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st);
+      k_add_inplace<double><<<blocks(N, 256), 256, 0, st>>>(dc.dprop, dproj, N);
+      const cudaError_t e = cudaGetLastError();
+      cudaStreamSynchronize(st);
+      cudaFree(dproj);
+      if (e != cudaSuccess) {
+        set_error(std::string("kernel launch: ") + cudaGetErrorString(e));
+        return PU_ERR_CUDA;
+      }
+      launches++;
+    }
+    const int E = INIT_HALO, nx = cfg.nx, ny = cfg.ny, nz = cfg.nz;
+    for (int d = 0; d < 2; d++) {
+      const size_t b = size_t(nz) * ny * E * sizeof(double);
+      unsigned char *p, *q;
+      PU_TRY(dalloc(p, b));
+      dc.ix.snd[d] = p;
+      PU_TRY(dalloc(q, b));
+      dc.ix.rcv[d] = q;
+      dc.ix.bytes[d] = b;
+    }
+    double **snd = reinterpret_cast<double **>(dc.ix.snd);
+    PU_TRY(box<double>(dc.dprop, nx, ny, 0, 0, snd[0], E, ny, 0, 0, E, ny, nz));
+    PU_TRY(box<double>(dc.dprop, nx, ny, nx - E, 0, snd[1], E, ny, 0, 0, E, ny, nz));
+    return PU_OK;
+  }
+
+  int dinit_hydro(const double *global_sums) override {
+    if (global_sums) {
+      PU_CK(cudaMemcpyAsync(sums, global_sums, size_t(3) * cfg.nz * sizeof(double), cudaMemcpyHostToDevice, st));
+      PU_CK(cudaStreamSynchronize(st));
+    }
+    HydroOut ho{cells, edges, rho_off, rt_off};
+    const double r = 1. / (double(dc.d.nx_glob) * double(dc.d.ny_glob));
+    k_hydro_finish<R><<<1, 1, 0, st>>>(sums, cfg.nz, r, cfg.gamma_d, cfg.C0, cfg.grav, cfg.dz, sizeof(R) == 4, ho,
+                                       lt);
+    PU_LAUNCHED();
+    return PU_OK;
+  }
+
+  int dinit_mid() override {
+    const int E = INIT_HALO, nx = cfg.nx, ny = cfg.ny, nz = cfg.nz, nxe = nx + 2 * E;
+    PU_TRY(dalloc(dc.ext_x, size_t(nz) * ny * nxe));
+    const double *const *rcv = reinterpret_cast<double *const *>(dc.ix.rcv);
+    PU_TRY(box<double>(dc.dprop, nx, ny, 0, 0, dc.ext_x, nxe, ny, E, 0, nx, ny, nz));
+    PU_TRY(box<double>(rcv[0], E, ny, 0, 0, dc.ext_x, nxe, ny, 0, 0, E, ny, nz));
+    PU_TRY(box<double>(rcv[1], E, ny, 0, 0, dc.ext_x, nxe, ny, E + nx, 0, E, ny, nz));
+    if (sim2d()) return PU_OK;
+    for (int d = 2; d < 4; d++) {
+      const size_t b = size_t(nz) * E * nxe * sizeof(double);
+      unsigned char *p, *q;
+      PU_TRY(dalloc(p, b));
+      dc.iy.snd[d] = p;
+      PU_TRY(dalloc(q, b));
+      dc.iy.rcv[d] = q;
+      dc.iy.bytes[d] = b;
+    }
+    double **snd = reinterpret_cast<double **>(dc.iy.snd);
+    PU_TRY(box<double>(dc.ext_x, nxe, ny, 0, 0, snd[2], nxe, E, 0, 0, nxe, E, nz));
+    PU_TRY(box<double>(dc.ext_x, nxe, ny, 0, ny - E, snd[3], nxe, E, 0, 0, nxe, E, nz));
+    return PU_OK;
+  }
+
+  int dinit_end(const pu_state_view *v) override {
+    const int E = INIT_HALO, W = HALO_W, nx = cfg.nx, ny = cfg.ny, nz = cfg.nz;
+    const int Ey = sim2d() ? 0 : E, nxe = nx + 2 * E, nye = ny + 2 * Ey;
+    const size_t Ne = size_t(nz) * nye * nxe;
+    const double *ext = dc.ext_x;
+    if (!sim2d()) {
+      PU_TRY(dalloc(dc.ext, Ne));
+      const double *const *rcv = reinterpret_cast<double *const *>(dc.iy.rcv);
+      PU_TRY(box<double>(dc.ext_x, nxe, ny, 0, 0, dc.ext, nxe, nye, 0, E, nxe, ny, nz));
+      PU_TRY(box<double>(rcv[2], nxe, E, 0, 0, dc.ext, nxe, nye, 0, 0, nxe, E, nz));
+      PU_TRY(box<double>(rcv[3], nxe, E, 0, 0, dc.ext, nxe, nye, 0, E + ny, nxe, E, nz));
+      ext = dc.ext;
+    }
+    // Flags and factors of the extended block (the distance passes wrap in x
+    // and y over the block; the wrap spans more than 10 cells from any cell
+    // whose flags are kept, so it finds nothing).
+    uint8_t *a = nullptr, *b = nullptr, *dz = nullptr, *fe = nullptr;
+    R *me = nullptr;
+    int rc = dalloc(a, Ne);
+    if (!rc) rc = dalloc(b, Ne);
+    if (!rc) rc = dalloc(dz, Ne);
+    if (!rc) rc = dalloc(fe, Ne);
+    if (!rc) rc = dalloc(me, Ne);
+    if (!rc && !flags) rc = dalloc(flags, N);
+    if (!rc && !imm_mult) {
+      R *m;
+      rc = dalloc(m, N);
+      if (!rc) imm_mult = m;
+    }
+    for (int d = 0; d < (sim2d() ? 2 : 4) && !rc; d++)
+      if (!dc.fslab[d]) rc = dalloc(dc.fslab[d], size_t(nz) * W * (d < 2 ? ny : nx));
+    if (!rc) {
+      k_dist_init<<<blocks(Ne, 256), 256, 0, st>>>(ext, 0, Ne, a, 10);
+      for (int axis = 0; axis < 3; axis++) {
+        k_dist_pass<<<blocks(Ne, 256), 256, 0, st>>>(a, b, nxe, nye, nz, axis, 10);
+        std::swap(a, b);
+      }
+      k_dist_init<<<blocks(Ne, 256), 256, 0, st>>>(ext, 1, Ne, dz, 3);
+      for (int axis = 0; axis < 3; axis++) {
+        k_dist_pass<<<blocks(Ne, 256), 256, 0, st>>>(dz, b, nxe, nye, nz, axis, 3);
+        cudaMemcpyAsync(dz, b, Ne, cudaMemcpyDeviceToDevice, st);
+      }
+      k_imm_finish<R><<<blocks(Ne, 256), 256, 0, st>>>(ext, a, dz, cfg.immersed_power, Ne, fe, me);
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) {
+        set_error(std::string("kernel launch: ") + cudaGetErrorString(e));
+        rc = PU_ERR_CUDA;
+      } else {
+        launches += 9;
+      }
+    }
+    if (!rc) rc = box<uint8_t>(fe, nxe, nye, E, Ey, flags, nx, ny, 0, 0, nx, ny, nz);
+    if (!rc) rc = box<R>(me, nxe, nye, E, Ey, static_cast<R *>(imm_mult), nx, ny, 0, 0, nx, ny, nz);
+    if (!rc) rc = box<uint8_t>(fe, nxe, nye, E - W, Ey, dc.fslab[0], W, ny, 0, 0, W, ny, nz);
+    if (!rc) rc = box<uint8_t>(fe, nxe, nye, E + nx, Ey, dc.fslab[1], W, ny, 0, 0, W, ny, nz);
+    if (!rc && !sim2d()) rc = box<uint8_t>(fe, nxe, nye, E, Ey - W, dc.fslab[2], nx, W, 0, 0, nx, W, nz);
+    if (!rc && !sim2d()) rc = box<uint8_t>(fe, nxe, nye, E, Ey + ny, dc.fslab[3], nx, W, 0, 0, nx, W, nz);
+    // The tile needs the immersed kernels if any of its cells has a flag
+    // (immersed, or immersed cells within 10, its own or its neighbours') or
+    // a halo cell is immersed.
+    if (!rc) {
+      std::vector<uint8_t> hf(N);
+      cudaMemcpyAsync(hf.data(), flags, N, cudaMemcpyDeviceToHost, st);
+      std::vector<uint8_t> hs[4];
+      for (int d = 0; d < (sim2d() ? 2 : 4); d++) {
+        hs[d].resize(size_t(nz) * W * (d < 2 ? ny : nx));
+        cudaMemcpyAsync(hs[d].data(), dc.fslab[d], hs[d].size(), cudaMemcpyDeviceToHost, st);
+      }
+      const cudaError_t e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) {
+        set_error(cudaGetErrorString(e));
+        rc = PU_ERR_CUDA;
+      }
+      has_imm = false;
+      for (size_t q = 0; q < N && !has_imm; q++) has_imm = hf[q] != 0;
+      for (auto &h : hs)
+        for (size_t q = 0; q < h.size() && !has_imm; q++) has_imm = (h[q] & FLAG_IMM) != 0;
+    }
+    cudaStreamSynchronize(st);
+    for (void *p : {(void *)a, (void *)b, (void *)dz, (void *)fe, (void *)me})
+      if (p) cudaFree(p);
+    for (double **p : {&dc.dprop, &dc.ext_x, &dc.ext}) {
+      if (*p) cudaFree(*p);
+      *p = nullptr;
+    }
+    dc.ix.release();
+    dc.iy.release();
+    if (rc) return rc;
+    PU_TRY(load_state(v));
+    PU_CK(cudaStreamSynchronize(st));
+    inited = true;
+    return PU_OK;
   }
 
   int get_conserved(double *stp, double *trp, int mem) override {

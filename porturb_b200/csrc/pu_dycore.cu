@@ -1,9 +1,14 @@
 // C entry points of libpu_dycore (declared in include/pu_dycore.h).
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <cmath>
+#include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <type_traits>
+#include <vector>
 
 #include "impl.cuh"
 
@@ -13,6 +18,39 @@ namespace {
 thread_local std::string g_error;
 }
 void set_error(const std::string &msg) { g_error = msg; }
+
+NcclApi &nccl() {
+  static NcclApi api;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *lib = dlopen("libnccl.so.2", RTLD_NOW | RTLD_LOCAL);
+    if (!lib) {
+      const char *e = dlerror();
+      api.error = std::string("cannot load libnccl.so.2: ") + (e ? e : "unknown error");
+      return;
+    }
+    bool ok = true;
+    auto get = [&](auto &fn, const char *name) {
+      fn = reinterpret_cast<std::remove_reference_t<decltype(fn)>>(dlsym(lib, name));
+      if (!fn && ok) {
+        ok = false;
+        api.error = std::string("libnccl.so.2 has no ") + name;
+      }
+    };
+    get(api.GetUniqueId, "ncclGetUniqueId");
+    get(api.CommInitRank, "ncclCommInitRank");
+    get(api.CommDestroy, "ncclCommDestroy");
+    get(api.GroupStart, "ncclGroupStart");
+    get(api.GroupEnd, "ncclGroupEnd");
+    get(api.Send, "ncclSend");
+    get(api.Recv, "ncclRecv");
+    get(api.AllReduce, "ncclAllReduce");
+    get(api.AllGather, "ncclAllGather");
+    get(api.GetErrorString, "ncclGetErrorString");
+    api.ok = ok;
+  });
+  return api;
+}
 
 #define PU_DECL(tag) ImplBase *make_impl_##tag();
 PU_DECL(f32_1) PU_DECL(f32_2) PU_DECL(f32_3) PU_DECL(f32_4)
@@ -95,6 +133,202 @@ int check_config(const pu_config *c) {
 
 namespace {
 using pu::check_config;
+}  // namespace
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Decomposition geometry (coupler.h:132-229) and the tiles of a group.
+// ---------------------------------------------------------------------------
+// coupler.h:148-171, including its choice rule: each candidate nproc_y is
+// compared through choice/(nranks/best-so-far), the first of equal distances
+// wins, and ny_glob == 1 gives nranks x 1.
+void process_grid(int nranks, long long nx_glob, long long ny_glob, int &npx, int &npy) {
+  if (ny_glob == 1) {
+    npx = nranks;
+    npy = 1;
+    return;
+  }
+  std::vector<double> choices;
+  for (int q = 1; q <= nranks; q++)
+    if (nranks % q == 0) choices.push_back(q);
+  const double aspect_real = double(ny_glob) / double(nx_glob);
+  npy = int(choices.at(0));
+  double aspect = double(npy) / (nranks / npy);
+  double min_dist = std::abs(aspect - aspect_real);
+  for (size_t i = 1; i < choices.size(); i++) {
+    aspect = choices[i] / (nranks / npy);
+    const double dist = std::abs(aspect - aspect_real);
+    if (dist < min_dist) {
+      npy = int(choices[i]);
+      min_dist = dist;
+    }
+  }
+  npx = nranks / npy;
+}
+
+// coupler.h:176-183.
+void tile_range(long long n_glob, int nproc, int p, long long &beg, long long &n) {
+  const double nper = double(n_glob) / nproc;
+  beg = (long long)std::round(nper * p);
+  const long long end = (long long)(std::round(nper * (p + 1)) - 1);
+  n = end - beg + 1;
+}
+
+void neighbors(const pu_decomp &d, int nbr[4]) {
+  auto rank = [&](int px, int py) {
+    px = ((px % d.nproc_x) + d.nproc_x) % d.nproc_x;
+    py = ((py % d.nproc_y) + d.nproc_y) % d.nproc_y;
+    return py * d.nproc_x + px;
+  };
+  nbr[0] = rank(d.px - 1, d.py);
+  nbr[1] = rank(d.px + 1, d.py);
+  nbr[2] = rank(d.px, d.py - 1);
+  nbr[3] = rank(d.px, d.py + 1);
+}
+
+int check_decomp(const pu_decomp *d, const pu_config &c) {
+  if (d->nproc_x < 1 || d->nproc_y < 1 || d->px < 0 || d->px >= d->nproc_x || d->py < 0 || d->py >= d->nproc_y)
+    return fail(PU_ERR_INVALID, "bad tile grid or tile position");
+  if (d->nx_glob < c.nx || d->ny_glob < c.ny) return fail(PU_ERR_INVALID, "the tile is larger than the global grid");
+  if (d->ny_glob == 1) {
+    if (d->nproc_y != 1 || c.ny != 1) return fail(PU_ERR_INVALID, "ny_glob == 1 needs one tile row with ny = 1");
+  } else if (c.ny < pu::INIT_HALO) {
+    return fail(PU_ERR_INVALID, "decomposed tiles need ny >= 12");
+  }
+  if (c.nx < pu::INIT_HALO) return fail(PU_ERR_INVALID, "decomposed tiles need nx >= 12");
+  return PU_OK;
+}
+
+struct TileInfo {
+  int px, py, nx, ny, nz, S, precision;
+};
+
+// Every tile of the grid once; tiles in a column of the grid (same px) of
+// equal nx, in a row of equal ny, adding up to the global grid; nz, the
+// field count and the precision equal.
+bool tiles_fit(const pu_decomp &d, const std::vector<TileInfo> &t, std::string &why) {
+  const int n = d.nproc_x * d.nproc_y;
+  if (int(t.size()) != n) {
+    why = "the group does not hold every tile of the grid";
+    return false;
+  }
+  std::vector<const TileInfo *> at(n, nullptr);
+  for (auto &x : t) {
+    if (x.px < 0 || x.px >= d.nproc_x || x.py < 0 || x.py >= d.nproc_y) {
+      why = "a tile lies outside the grid";
+      return false;
+    }
+    const TileInfo *&slot = at[x.py * d.nproc_x + x.px];
+    if (slot) {
+      why = "two tiles share one grid position";
+      return false;
+    }
+    slot = &x;
+  }
+  long long sx = 0, sy = 0;
+  for (int py = 0; py < d.nproc_y; py++)
+    for (int px = 0; px < d.nproc_x; px++) {
+      const TileInfo &a = *at[py * d.nproc_x + px], &o = *at[0];
+      if (a.nz != o.nz || a.S != o.S || a.precision != o.precision) {
+        why = "tiles differ in nz, tracer count or precision";
+        return false;
+      }
+      if (a.nx != at[px]->nx || a.ny != at[py * d.nproc_x]->ny) {
+        why = "tiles of one grid column differ in nx, or of one grid row in ny";
+        return false;
+      }
+      if (py == 0) sx += a.nx;
+      if (px == 0) sy += a.ny;
+    }
+  if (sx != d.nx_glob || sy != d.ny_glob) {
+    why = "the tile sizes do not add up to the global grid";
+    return false;
+  }
+  return true;
+}
+
+int set_decomposition(pu::ImplBase &I, const pu_decomp &d, const unsigned char *id) {
+  auto &dc = I.dc;
+  dc.d = d;
+  dc.rank = d.py * d.nproc_x + d.px;
+  dc.nranks = d.nproc_x * d.nproc_y;
+  neighbors(d, dc.nbr);
+  int rc = I.dec_alloc();
+  if (rc) return rc;
+  if (id) {
+    auto &api = pu::nccl();
+    if (!api.ok) return fail(PU_ERR_UNSUPPORTED, api.error);
+    ncclUniqueId u;
+    std::memcpy(u.internal, id, sizeof(u.internal));
+    ncclResult_t r = api.CommInitRank(&dc.comm, dc.nranks, u, dc.rank);
+    if (r != ncclSuccess) {
+      dc.comm = nullptr;
+      return fail(PU_ERR_CUDA, std::string("ncclCommInitRank: ") + api.GetErrorString(r));
+    }
+    // Every rank checks the whole table of tiles, so a misfit fails on all
+    // ranks alike before any halo is exchanged.
+    const TileInfo mine{d.px, d.py, I.cfg.nx, I.cfg.ny, I.cfg.nz, I.S, I.cfg.precision};
+    int *buf = nullptr;
+    const size_t ni = sizeof(TileInfo) / sizeof(int);
+    if (cudaMalloc(&buf, ni * (dc.nranks + 1) * sizeof(int)) != cudaSuccess) return fail(PU_ERR_NOMEM, "cudaMalloc");
+    std::vector<TileInfo> all(dc.nranks);
+    cudaMemcpyAsync(buf, &mine, sizeof(TileInfo), cudaMemcpyHostToDevice, I.st);
+    r = api.AllGather(buf, buf + ni, ni, ncclInt32, dc.comm, I.st);
+    cudaMemcpyAsync(all.data(), buf + ni, sizeof(TileInfo) * dc.nranks, cudaMemcpyDeviceToHost, I.st);
+    const cudaError_t e = cudaStreamSynchronize(I.st);
+    cudaFree(buf);
+    if (r != ncclSuccess) return fail(PU_ERR_CUDA, std::string("ncclAllGather: ") + api.GetErrorString(r));
+    if (e != cudaSuccess) return fail(PU_ERR_CUDA, cudaGetErrorString(e));
+    std::string why;
+    if (!tiles_fit(d, all, why)) return fail(PU_ERR_INVALID, why);
+  }
+  dc.on = true;
+  return PU_OK;
+}
+
+// The tiles of an in-process group, indexed by rank; all checks first.
+int group_tiles(pu_dycore *const *hs, int n, std::vector<pu::ImplBase *> &byrank, bool need_init) {
+  if (!hs || n < 1) return fail(PU_ERR_INVALID, "empty group");
+  for (int i = 0; i < n; i++)
+    if (!hs[i] || !hs[i]->impl) return fail(PU_ERR_INVALID, "null handle in the group");
+  const pu::ImplBase &h0 = *hs[0]->impl;
+  std::vector<TileInfo> info;
+  byrank.assign(n, nullptr);
+  for (int i = 0; i < n; i++) {
+    pu::ImplBase &I = *hs[i]->impl;
+    if (!I.dc.on || I.dc.comm)
+      return fail(PU_ERR_STATE, "group tiles are made with pu_dycore_set_decomposition(h, d, NULL)");
+    if (I.dc.d.nproc_x != h0.dc.d.nproc_x || I.dc.d.nproc_y != h0.dc.d.nproc_y ||
+        I.dc.d.nx_glob != h0.dc.d.nx_glob || I.dc.d.ny_glob != h0.dc.d.ny_glob)
+      return fail(PU_ERR_INVALID, "group tiles differ in their tile grid");
+    if (hs[i]->device != hs[0]->device || I.st != h0.st)
+      return fail(PU_ERR_INVALID, "group tiles must share one device and one stream");
+    if (need_init && !I.inited) return fail(PU_ERR_STATE, "pu_dycore_group_init has not been called");
+    if (I.dc.rank < 0 || I.dc.rank >= n || byrank[I.dc.rank]) return fail(PU_ERR_INVALID, "bad or repeated tile");
+    byrank[I.dc.rank] = &I;
+    info.push_back({I.dc.d.px, I.dc.d.py, I.cfg.nx, I.cfg.ny, I.cfg.nz, I.S, I.cfg.precision});
+  }
+  std::string why;
+  if (!tiles_fit(h0.dc.d, info, why)) return fail(PU_ERR_INVALID, why);
+  return PU_OK;
+}
+
+// Every tile's rcv[d] <- its neighbour's snd[d ^ 1] (one stream, in order).
+int local_exchange(std::vector<pu::ImplBase *> &t, int which, bool x, bool y) {
+  for (pu::ImplBase *a : t) {
+    pu::HaloSet &ha = a->halo(which);
+    for (int d = 0; d < 4; d++) {
+      if ((d < 2 && !x) || (d >= 2 && !y)) continue;
+      pu::HaloSet &hb = t[a->dc.nbr[d]]->halo(which);
+      if (ha.bytes[d] != hb.bytes[d ^ 1]) return fail(PU_ERR_INVALID, "neighbouring tiles do not fit");
+      if (cudaMemcpyAsync(ha.rcv[d], hb.snd[d ^ 1], ha.bytes[d], cudaMemcpyDeviceToDevice, a->st) != cudaSuccess)
+        return fail(PU_ERR_CUDA, "halo copy failed");
+    }
+  }
+  return PU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -316,6 +550,7 @@ int pu_dycore_set_weno_mode(pu_dycore *h, int mode) {
   if (!h) return fail(PU_ERR_INVALID, "null handle");
   if (mode != PU_WENO_PLAIN && mode != PU_WENO_LEARNED) return fail(PU_ERR_INVALID, "bad WENO mode");
   if (mode == PU_WENO_LEARNED) {
+    if (h->impl->dc.on) return fail(PU_ERR_UNSUPPORTED, "learned weights do not run on decomposed tiles");
     if (h->impl->cfg.precision != PU_F32) return fail(PU_ERR_UNSUPPORTED, "learned weights run in the FP32 build only");
     if (!h->impl->cfg.weno_all)
       return fail(PU_ERR_UNSUPPORTED, "learned weights replace the limiter of weno_all; this dycore uses linear edges");
@@ -360,6 +595,127 @@ int pu_dycore_profile_read(pu_dycore *h, pu_profile *out) {
   if (!h || !out) return fail(PU_ERR_INVALID, "null argument");
   DeviceGuard g(h->device);
   return h->impl->prof_read(out);
+}
+
+int pu_decomp_process_grid(int nranks, long long nx_glob, long long ny_glob, int *nproc_x, int *nproc_y) {
+  if (nranks < 1 || nx_glob < 1 || ny_glob < 1 || !nproc_x || !nproc_y) return fail(PU_ERR_INVALID, "bad argument");
+  process_grid(nranks, nx_glob, ny_glob, *nproc_x, *nproc_y);
+  return PU_OK;
+}
+
+int pu_decomp_tile(long long n_glob, int nproc, int p, long long *beg, long long *n) {
+  if (n_glob < 1 || nproc < 1 || p < 0 || p >= nproc || !beg || !n) return fail(PU_ERR_INVALID, "bad argument");
+  tile_range(n_glob, nproc, p, *beg, *n);
+  return PU_OK;
+}
+
+int pu_decomp_neighbors(const pu_decomp *d, int nbr[4]) {
+  if (!d || !nbr || d->nproc_x < 1 || d->nproc_y < 1) return fail(PU_ERR_INVALID, "bad argument");
+  neighbors(*d, nbr);
+  return PU_OK;
+}
+
+int pu_nccl_get_unique_id(unsigned char *id) {
+  if (!id) return fail(PU_ERR_INVALID, "null argument");
+  auto &api = pu::nccl();
+  if (!api.ok) return fail(PU_ERR_UNSUPPORTED, api.error);
+  ncclUniqueId u;
+  const ncclResult_t r = api.GetUniqueId(&u);
+  if (r != ncclSuccess) return fail(PU_ERR_CUDA, std::string("ncclGetUniqueId: ") + api.GetErrorString(r));
+  static_assert(sizeof(u.internal) == PU_NCCL_ID_BYTES, "NCCL unique id size");
+  std::memcpy(id, u.internal, PU_NCCL_ID_BYTES);
+  return PU_OK;
+}
+
+int pu_dycore_set_decomposition(pu_dycore *h, const pu_decomp *d, const unsigned char *nccl_id) {
+  if (!h || !d) return fail(PU_ERR_INVALID, "null argument");
+  auto &I = *h->impl;
+  if (I.inited) return fail(PU_ERR_STATE, "pu_dycore_set_decomposition comes before pu_dycore_init");
+  if (I.dc.on) return fail(PU_ERR_STATE, "the handle is already decomposed");
+  if (I.weno_mode == PU_WENO_LEARNED) return fail(PU_ERR_UNSUPPORTED, "learned weights do not run on decomposed tiles");
+  int rc = check_decomp(d, I.cfg);
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  rc = set_decomposition(I, *d, nccl_id);
+  if (rc) I.dec_release();
+  return rc;
+}
+
+int pu_dycore_group_init(pu_dycore *const *hs, int n, const pu_state_view *views, const double *const *props,
+                         const double *const *projs, int mem) {
+  std::vector<pu::ImplBase *> t;
+  int rc = group_tiles(hs, n, t, false);
+  if (rc) return rc;
+  if (!views) return fail(PU_ERR_INVALID, "null views");
+  DeviceGuard g(hs[0]->device);
+  for (int i = 0; i < n; i++) {
+    rc = hs[i]->impl->dinit_begin(&views[i], props ? props[i] : nullptr, projs ? projs[i] : nullptr, mem);
+    if (rc) return rc;
+  }
+  // Profile sums over the tiles in rank order, with compensation.
+  const int nz = t[0]->cfg.nz;
+  std::vector<double> part(size_t(3) * nz), sum(size_t(3) * nz, 0.0), comp(size_t(3) * nz, 0.0);
+  for (pu::ImplBase *a : t) {
+    if (cudaMemcpyAsync(part.data(), a->sums, part.size() * sizeof(double), cudaMemcpyDeviceToHost, a->st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(a->st) != cudaSuccess)
+      return fail(PU_ERR_CUDA, "profile sums copy failed");
+    for (size_t q = 0; q < part.size(); q++) {
+      const double x = part[q], tq = sum[q] + x;
+      comp[q] += std::fabs(sum[q]) >= std::fabs(x) ? (sum[q] - tq) + x : (x - tq) + sum[q];
+      sum[q] = tq;
+    }
+  }
+  for (size_t q = 0; q < sum.size(); q++) sum[q] += comp[q];
+  for (pu::ImplBase *a : t)
+    if ((rc = a->dinit_hydro(sum.data()))) return rc;
+  if ((rc = local_exchange(t, 1, true, false))) return rc;
+  for (pu::ImplBase *a : t)
+    if ((rc = a->dinit_mid())) return rc;
+  if (!t[0]->sim2d() && (rc = local_exchange(t, 2, false, true))) return rc;
+  for (int i = 0; i < n; i++)
+    if ((rc = hs[i]->impl->dinit_end(&views[i]))) return rc;
+  return PU_OK;
+}
+
+int pu_dycore_group_advance(pu_dycore *const *hs, int n, double dt, int nsteps) {
+  std::vector<pu::ImplBase *> t;
+  int rc = group_tiles(hs, n, t, true);
+  if (rc) return rc;
+  if (!(dt > 0)) return fail(PU_ERR_INVALID, "dt must be positive");
+  if (nsteps <= 0) return PU_OK;
+  DeviceGuard g(hs[0]->device);
+  for (pu::ImplBase *a : t)
+    if ((rc = a->dec_enforce())) return rc;
+  for (int s = 0; s < nsteps; s++)
+    for (int sg = 0; sg < 3; sg++) {
+      for (pu::ImplBase *a : t)
+        if ((rc = a->dec_pack(sg))) return rc;
+      if ((rc = local_exchange(t, 0, true, !t[0]->sim2d()))) return rc;
+      for (pu::ImplBase *a : t)
+        if ((rc = a->dec_compute(sg, dt, s == nsteps - 1))) return rc;
+    }
+  return PU_OK;
+}
+
+int pu_dycore_group_time_step(pu_dycore *const *hs, int n, pu_state_view *views, double dt_phys, int *ncycles) {
+  std::vector<pu::ImplBase *> t;
+  int rc = group_tiles(hs, n, t, true);
+  if (rc) return rc;
+  if (!views) return fail(PU_ERR_INVALID, "null views");
+  if (!(dt_phys > 0)) return fail(PU_ERR_INVALID, "dt_phys must be positive");
+  DeviceGuard g(hs[0]->device);
+  double dt_dyn;
+  pu_dycore_compute_time_step(hs[0], &dt_dyn);
+  const int nc = (int)std::ceil(dt_phys / dt_dyn);
+  dt_dyn = dt_phys / nc;
+  for (int i = 0; i < n; i++)
+    if ((rc = hs[i]->impl->load_state(&views[i]))) return rc;
+  if ((rc = pu_dycore_group_advance(hs, n, dt_dyn, nc))) return rc;
+  for (int i = 0; i < n; i++)
+    if ((rc = hs[i]->impl->store_state(&views[i]))) return rc;
+  if (ncycles) *ncycles = nc;
+  return PU_OK;
 }
 
 }  // extern "C"

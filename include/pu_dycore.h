@@ -283,6 +283,17 @@ int pu_dycore_time_step_noalloc(const pu_config *cfg, const double *hy_dens_cell
                                 const double *hy_pressure_cells, pu_state_view *coupler, double dt_phys,
                                 int *ncycles);
 
+/* The FP32 order-9 limiter (WenoLimiter<float,9>::compute_limited_edges,
+ * WenoLimiter.h:349-437, in this library's arithmetic) on n stencils of 9
+ * consecutive floats: the left and right edge values of each.  flags[i]
+ * (NULL: all 1): bit 0 do_map, bit 1 imm_L, bit 2 imm_R.  variant 0: the
+ * scalar form the kernels use; 1: the same without skipping map_rs for
+ * weights already at their ideal values; 2, 3: the packed two-stencil form
+ * with and without that skip.  All four give the same bits.  Host or device
+ * arrays (mem); synchronous, on the current device. */
+int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long long n, int variant, float *qL,
+                       float *qR, int mem);
+
 /* ---------------------------------------------------------------------------
  * Domain decomposition across GPUs (coupler.h:132-229): a handle can be one
  * (px, py) tile of an nproc_x x nproc_y grid of tiles over an nx_glob x

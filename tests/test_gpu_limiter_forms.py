@@ -1,0 +1,95 @@
+"""The FP32 order-9 limiter's forms agree bit for bit (pu_weno9_edges_f32):
+the scalar form and the packed two-stencil form, each with and without
+skipping map_rs when every normalised weight of an edge is within
+map_near(k) of its ideal value (where the map returns the ideal weight
+exactly, csrc/weno9.cuh).  Stencils: random normal, polynomials of degree
+<= 4, constants, smooth data plus noise of amplitude 1e-9 .. 1e-1 (weights
+on both sides of the bounds), steps, with random map and immersed flags.
+The scalar form is also held to the reference's float limiter (the oracle's
+weno9_batch_f32, bit-identical to WenoLimiter<float,9>): within 2e-5 of
+each stencil's range plus 5 % of its magnitude, the effect of the rearranged
+arithmetic (on a constant stencil this form returns the value exactly, the
+reference's polynomial coefficients only to float rounding)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import pyoracle
+from porturb_b200 import capi
+
+pytestmark = pytest.mark.gpu
+
+D = np.array([5, 40, 60, 20, 1]) / 126.0
+T = np.array([2.2928e-2, 8.5599e-2, 9.6490e-2, 5.8021e-2, 6.5359e-3])
+
+
+def _stencils(n, seed=0):
+    rng = np.random.default_rng(seed)
+    x = np.arange(-4, 5, dtype=np.float64)
+    parts = [rng.standard_normal((n, 9))]
+    c = rng.standard_normal((n, 5))
+    poly = sum(c[:, j:j + 1] * (x[None, :] / 4) ** j for j in range(5))
+    parts.append(poly)
+    parts.append(np.repeat(rng.standard_normal((n // 8, 1)), 9, axis=1))
+    amp = 10.0 ** rng.uniform(-9, -1, size=(n, 1))
+    parts.append(poly + amp * rng.standard_normal((n, 9)))
+    step = np.where(x[None, :] >= rng.integers(-4, 5, size=(n, 1)), 1.0, 0.0) + 1e-3 * rng.standard_normal((n, 9))
+    parts.append(step)
+    s = np.concatenate(parts).astype(np.float32)
+    flags = rng.integers(0, 8, size=s.shape[0]).astype(np.uint8)
+    flags[: s.shape[0] // 2] = 1      # half the stencils: do_map, no immersed neighbours
+    return np.ascontiguousarray(s), flags
+
+
+def _near_fraction(s):
+    """Share of stencils (FP64 estimate) whose left-edge weights are all within the bounds."""
+    xs = np.arange(-4, 5)
+    tv = []
+    for k in range(5):
+        cells = np.arange(-4 + k, 1 + k)
+        A = np.array([[((cc + 0.5) ** (j + 1) - (cc - 0.5) ** (j + 1)) / (j + 1) for j in range(5)] for cc in cells])
+        co = s[:, k:k + 5].astype(np.float64) @ np.linalg.inv(A).T
+        a1, a2, a3, a4 = co[:, 1], co[:, 2], co[:, 3], co[:, 4]
+        tv.append(a1 * a1 + 13 / 3 * a2 * a2 + 0.5 * a1 * a3 + 39.1125 * a3 * a3 + 4.2 * a2 * a4 + 625.8 * a4 * a4)
+    tv = np.stack(tv, 1)
+    tot = tv.sum(1, keepdims=True)
+    tv = np.where(tot > 1e-20, tv / np.where(tot > 1e-20, tot, 1), tv)
+    w = D / (tv * tv + 1e-20)
+    w = w / w.sum(1, keepdims=True)
+    return np.all(np.abs(w - D) <= T, axis=1).mean(), np.all(np.abs(w - D) <= 3 * T, axis=1).mean()
+
+
+def _run(lib, s, flags, variant):
+    n = s.shape[0]
+    qL = np.empty(n, np.float32)
+    qR = np.empty(n, np.float32)
+    rc = lib.pu_weno9_edges_f32(s.ctypes.data, flags.ctypes.data, n, variant, qL.ctypes.data, qR.ctypes.data,
+                                capi.PU_MEM_HOST)
+    assert rc == 0, lib.pu_last_error()
+    return qL, qR
+
+
+def test_limiter_forms_agree_bit_for_bit(gpu_lib):
+    s, flags = _stencils(40000)
+    near, near3 = _near_fraction(s)
+    print("stencils with every weight within the bounds: %.3f (within 3x: %.3f)" % (near, near3))
+    assert near > 0.1 and near3 - near > 0.05   # the skip and its surroundings are both exercised
+    out = [_run(gpu_lib, s, flags, v) for v in range(4)]
+    for v in range(1, 4):
+        assert np.array_equal(out[v][0].view(np.uint32), out[0][0].view(np.uint32)), v
+        assert np.array_equal(out[v][1].view(np.uint32), out[0][1].view(np.uint32)), v
+
+
+def test_scalar_form_against_the_reference_limiter(oracle_lib, gpu_lib):
+    s, _ = _stencils(4000, seed=1)
+    flags = np.ones(s.shape[0], np.uint8)
+    qL, qR = _run(gpu_lib, s, flags, 0)
+    rL, rR = pyoracle.weno9_batch_f32(s, do_map=True)
+    # Scale: the stencil's range, plus its magnitude for nearly constant
+    # stencils (the reference forms edge values through polynomial
+    # coefficients that sum to 1 only to float rounding).
+    scale = (s.max(1) - s.min(1)) + 0.05 * np.abs(s).max(1) + 1e-30
+    eL, eR = np.abs(qL - rL) / scale, np.abs(qR - rR) / scale
+    print("max |gpu - reference| / scale: %.2e %.2e" % (eL.max(), eR.max()))
+    assert eL.max() <= 2e-5 and eR.max() <= 2e-5

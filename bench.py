@@ -300,7 +300,6 @@ def main():
     torch.cuda.synchronize()
     clocks.start()
     time.sleep(0.3)
-    g.profile(True)
     launches0 = g.kernel_launches()
     ev0.record(stream)
     for _ in range(args.steps):
@@ -308,6 +307,12 @@ def main():
     ev1.record(stream)
     torch.cuda.synchronize()
     launches = g.kernel_launches() - launches0
+    # Per-kernel CUDA events on the launching stream, in a second pass of the
+    # same number of steps: an event pair around every launch costs ~1.7 % of
+    # the step, so the headline region above runs without them.
+    g.profile(True)
+    for _ in range(args.steps):
+        g.advance(dt, 1)
     prof = g.profile_read()
     g.profile(False)
     clk = clocks.stop()
@@ -413,7 +418,9 @@ def main():
                                  "k_z_issue_frac": tinfo.get("k_z_issue_frac"),
                                  "source": tinfo.get("source")},
             "kernel_ms": {"k_xy": xy_ms / max(xy_n, 1), "k_z": z_ms / max(z_n, 1),
-                          "share_xy": xy_ms / max(xy_ms + z_ms, 1e-12)},
+                          "share_xy": xy_ms / max(xy_ms + z_ms, 1e-12),
+                          "timing": "CUDA events around each launch on its stream, in a second pass of the same "
+                                    "steps right after the headline region"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": bytes_io,
                     "d2h_bytes_per_step": bytes_io, "calls": args.e2e_calls, "dycore_steps_per_call": ncyc // max(1, args.e2e_calls)},

@@ -287,10 +287,9 @@ int pu_dycore_time_step_noalloc(const pu_config *cfg, const double *hy_dens_cell
  * WenoLimiter.h:349-437, in this library's arithmetic) on n stencils of 9
  * consecutive floats: the left and right edge values of each.  flags[i]
  * (NULL: all 1): bit 0 do_map, bit 1 imm_L, bit 2 imm_R.  variant 0: the
- * scalar form the kernels use; 1: the same without skipping map_rs for
- * weights already at their ideal values; 2, 3: the packed two-stencil form
- * with and without that skip.  All four give the same bits.  Host or device
- * arrays (mem); synchronous, on the current device. */
+ * scalar form (the z march, the FP64-free fallbacks); 1: the packed
+ * two-stencil form of the x/y kernel.  Both give the same bits.  Host or
+ * device arrays (mem); synchronous, on the current device. */
 int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long long n, int variant, float *qL,
                        float *qR, int mem);
 

@@ -333,21 +333,20 @@ int local_exchange(std::vector<pu::ImplBase *> &t, int which, bool x, bool y) {
 
 namespace {
 
-// The FP32 limiter on a batch of stencils: VARIANT 0/1 the scalar form with /
-// without the map skip, 2/3 the packed form (stencils 2i and 2i+1 in one
-// thread) with / without it.
+// The FP32 limiter on a batch of stencils: VARIANT 0 the scalar form, 1 the
+// packed form (stencils 2i and 2i+1 in one thread).
 template <int VARIANT>
 __global__ void k_weno9_eval(const float *__restrict__ s, const unsigned char *__restrict__ flags, long long n,
                              float *__restrict__ qL, float *__restrict__ qR) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if constexpr (VARIANT < 2) {
+  if constexpr (VARIANT == 0) {
     if (i >= n) return;
     float st[9];
 #pragma unroll
     for (int m = 0; m < 9; m++) st[m] = s[i * 9 + m];
     const unsigned f = flags ? flags[i] : 1u;
     float a, b;
-    pu::weno9_edges<float, VARIANT == 0>(st, a, b, (f & 1u) != 0, (f & 2u) != 0, (f & 4u) != 0);
+    pu::weno9_edges<float>(st, a, b, (f & 1u) != 0, (f & 2u) != 0, (f & 4u) != 0);
     qL[i] = a;
     qR[i] = b;
   } else {
@@ -359,8 +358,8 @@ __global__ void k_weno9_eval(const float *__restrict__ s, const unsigned char *_
     for (int m = 0; m < 9; m++) st[m] = make_float2(s[a * 9 + m], s[bb * 9 + m]);
     const unsigned fa = flags ? flags[a] : 1u, fb = flags ? flags[bb] : 1u;
     float2 L, R;
-    pu::weno9_edges2<VARIANT == 2>(st, L, R, pu::bool2{(fa & 1u) != 0, (fb & 1u) != 0},
-                                   pu::bool2{(fa & 2u) != 0, (fb & 2u) != 0}, pu::bool2{(fa & 4u) != 0, (fb & 4u) != 0});
+    pu::weno9_edges2(st, L, R, pu::bool2{(fa & 1u) != 0, (fb & 1u) != 0}, pu::bool2{(fa & 2u) != 0, (fb & 2u) != 0},
+                     pu::bool2{(fa & 4u) != 0, (fb & 4u) != 0});
     qL[a] = L.x;
     qR[a] = R.x;
     if (b < n) {
@@ -761,7 +760,7 @@ int pu_dycore_group_time_step(pu_dycore *const *hs, int n, pu_state_view *views,
 
 int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long long n, int variant, float *qL,
                        float *qR, int mem) {
-  if (!stencils || !qL || !qR || n < 0 || variant < 0 || variant > 3) return fail(PU_ERR_INVALID, "bad argument");
+  if (!stencils || !qL || !qR || n < 0 || variant < 0 || variant > 1) return fail(PU_ERR_INVALID, "bad argument");
   if (n == 0) return PU_OK;
   const bool dev = pu::resolve_mem(mem, stencils) == PU_MEM_DEVICE;
   float *ds = const_cast<float *>(stencils), *dl = qL, *dr = qR;
@@ -774,14 +773,10 @@ int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long l
     cudaMemcpy(ds, stencils, size_t(n) * 9 * sizeof(float), cudaMemcpyHostToDevice);
     if (flags) cudaMemcpy(df, flags, size_t(n), cudaMemcpyHostToDevice);
   }
-  const long long threads = variant < 2 ? n : (n + 1) / 2;
+  const long long threads = variant == 0 ? n : (n + 1) / 2;
   const unsigned blocks = unsigned((threads + 255) / 256);
-  switch (variant) {
-    case 0: k_weno9_eval<0><<<blocks, 256>>>(ds, df, n, dl, dr); break;
-    case 1: k_weno9_eval<1><<<blocks, 256>>>(ds, df, n, dl, dr); break;
-    case 2: k_weno9_eval<2><<<blocks, 256>>>(ds, df, n, dl, dr); break;
-    default: k_weno9_eval<3><<<blocks, 256>>>(ds, df, n, dl, dr); break;
-  }
+  if (variant == 0) k_weno9_eval<0><<<blocks, 256>>>(ds, df, n, dl, dr);
+  else k_weno9_eval<1><<<blocks, 256>>>(ds, df, n, dl, dr);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (!dev) {

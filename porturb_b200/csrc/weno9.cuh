@@ -17,8 +17,6 @@
 // the map_rs denominator is at least ideal_k^6 > 2e-13.
 #pragma once
 
-#include <type_traits>
-
 #include "weno9_tables.cuh"
 
 namespace pu {
@@ -33,24 +31,6 @@ __device__ __forceinline__ float fast_rcp<float>(float x) {
   return r;
 }
 
-// Map skip (FP32).  map_rs moves each normalised weight w_k toward its ideal
-// value d_k by t^7 / (t^6 + 2000 (w(1-w))^3), t = w_k - d_k.  While |t| <=
-// map_near(k), that correction is at most a tenth of the float spacing below
-// d_k (T^7 / (2000 min_{|w-d|<=T} (w(1-w))^3) <= 0.1 ulp(d_k); the roundings
-// of t^7, of the denominator and of rcp.approx change it by under 1e-6
-// relative, and w(1-w) >= 1.4e-3 there, so nothing is flushed), and the fma
-// that applies it returns d_k exactly.  So when every weight of an edge is
-// that close, the mapped weights are the ideal ones and the map is not
-// evaluated: the results are bit-identical to evaluating it.  Bounds in the
-// order of IDEAL_L (the right edge uses them reversed, as its ideal weights).
-#ifndef PU_MAP_SKIP
-#define PU_MAP_SKIP 1
-#endif
-
-__host__ __device__ constexpr float map_near(int k) {
-  return k == 0 ? 2.2928e-2f : k == 1 ? 8.5599e-2f : k == 2 ? 9.6490e-2f : k == 3 ? 5.8021e-2f : 6.5359e-3f;
-}
-
 template <class R>
 __device__ __forceinline__ void convexify5(R (&w)[5]) {
   R tot = w[0] + w[1] + w[2] + w[3] + w[4];
@@ -62,8 +42,7 @@ __device__ __forceinline__ void convexify5(R (&w)[5]) {
 }
 
 // One edge: weights from the shared reciprocals rk = 1/(TV_k^2 + 1e-20).
-// SKIP: the map skip above (FP32 only).
-template <class R, bool LEFT, bool SKIP = PU_MAP_SKIP && std::is_same<R, float>::value>
+template <class R, bool LEFT>
 __device__ __forceinline__ R weno9_edge(const R (&d)[8], R s4, const R (&rk)[5], bool do_map) {
   using namespace pu_weno9;
   R w[5];
@@ -71,27 +50,16 @@ __device__ __forceinline__ R weno9_edge(const R (&d)[8], R s4, const R (&rk)[5],
   for (int k = 0; k < 5; k++) w[k] = R(LEFT ? IDEAL_L[k] : IDEAL_R[k]) * rk[k];
   convexify5(w);
   if (do_map) {
-    bool near = SKIP;
-    if constexpr (SKIP) {
 #pragma unroll
-      for (int k = 0; k < 5; k++)
-        near &= fabs(w[k] - R(LEFT ? IDEAL_L[k] : IDEAL_R[k])) <= R(map_near(LEFT ? k : 4 - k));
-    }
-    if (near) {
-#pragma unroll
-      for (int k = 0; k < 5; k++) w[k] = R(LEFT ? IDEAL_L[k] : IDEAL_R[k]);
-    } else {
-#pragma unroll
-      for (int k = 0; k < 5; k++) {
-        const R dk = R(LEFT ? IDEAL_L[k] : IDEAL_R[k]);
-        R t = w[k] - dk;
-        R t2 = t * t;
-        R t6 = t2 * t2 * t2;
-        R u = fma(-w[k], w[k], w[k]);   // w (1 - w)
-        R u3 = u * u * u;
-        R den = fma(R(2000.), u3, t6);
-        w[k] = fma(t6 * t, fast_rcp(den), dk);
-      }
+    for (int k = 0; k < 5; k++) {
+      const R dk = R(LEFT ? IDEAL_L[k] : IDEAL_R[k]);
+      R t = w[k] - dk;
+      R t2 = t * t;
+      R t6 = t2 * t2 * t2;
+      R u = fma(-w[k], w[k], w[k]);   // w (1 - w)
+      R u3 = u * u * u;
+      R den = fma(R(2000.), u3, t6);
+      w[k] = fma(t6 * t, fast_rcp(den), dk);
     }
     convexify5(w);
   }
@@ -106,7 +74,7 @@ __device__ __forceinline__ R weno9_edge(const R (&d)[8], R s4, const R (&rk)[5],
   return s4 + acc;
 }
 
-template <class R, bool SKIP = PU_MAP_SKIP && std::is_same<R, float>::value>
+template <class R>
 __device__ __forceinline__ void weno9_edges(const R (&s)[9], R &qL, R &qR, bool do_map, bool imm_L, bool imm_R) {
   using namespace pu_weno9;
   R d[8];
@@ -133,8 +101,8 @@ __device__ __forceinline__ void weno9_edges(const R (&s)[9], R &qL, R &qR, bool 
   R rk[5];
 #pragma unroll
   for (int k = 0; k < 5; k++) rk[k] = fast_rcp(fma(tv[k], tv[k], R(1.e-20)));
-  qL = weno9_edge<R, true, SKIP>(d, s[4], rk, do_map);
-  qR = weno9_edge<R, false, SKIP>(d, s[4], rk, do_map);
+  qL = weno9_edge<R, true>(d, s[4], rk, do_map);
+  qR = weno9_edge<R, false>(d, s[4], rk, do_map);
 }
 
 // ---------------------------------------------------------------------------
@@ -163,9 +131,7 @@ __device__ __forceinline__ void convexify5x2(float2 (&w)[5]) {
   for (int k = 0; k < 5; k++) w[k] = mul2(w[k], r);
 }
 
-// SKIP: the map skip, taken when both stencils' weights are near their
-// ideal values (a stencil that is near gets exactly d_k from the map too).
-template <bool LEFT, bool SKIP = PU_MAP_SKIP>
+template <bool LEFT>
 __device__ __forceinline__ float2 weno9_edge2(const float2 (&d)[8], float2 s4, const float2 (&rk)[5], bool2 do_map) {
   using namespace pu_weno9;
   float2 w[5];
@@ -174,29 +140,16 @@ __device__ __forceinline__ float2 weno9_edge2(const float2 (&d)[8], float2 s4, c
   convexify5x2(w);
   if (do_map.x || do_map.y) {
     float2 m[5];
-    bool near = SKIP;
-    if constexpr (SKIP) {
 #pragma unroll
-      for (int k = 0; k < 5; k++) {
-        const float dk = float(LEFT ? IDEAL_L[k] : IDEAL_R[k]), bound = map_near(LEFT ? k : 4 - k);
-        near &= fabsf(w[k].x - dk) <= bound && fabsf(w[k].y - dk) <= bound;
-      }
-    }
-    if (near) {
-#pragma unroll
-      for (int k = 0; k < 5; k++) m[k] = f2(float(LEFT ? IDEAL_L[k] : IDEAL_R[k]));
-    } else {
-#pragma unroll
-      for (int k = 0; k < 5; k++) {
-        const float2 dk = f2(float(LEFT ? IDEAL_L[k] : IDEAL_R[k]));
-        const float2 t = sub2(w[k], dk);
-        const float2 t2 = mul2(t, t);
-        const float2 t6 = mul2(mul2(t2, t2), t2);
-        const float2 u = fma2(make_float2(-w[k].x, -w[k].y), w[k], w[k]);
-        const float2 u3 = mul2(mul2(u, u), u);
-        const float2 den = fma2(f2(2000.f), u3, t6);
-        m[k] = fma2(mul2(t6, t), rcp2(den), dk);
-      }
+    for (int k = 0; k < 5; k++) {
+      const float2 dk = f2(float(LEFT ? IDEAL_L[k] : IDEAL_R[k]));
+      const float2 t = sub2(w[k], dk);
+      const float2 t2 = mul2(t, t);
+      const float2 t6 = mul2(mul2(t2, t2), t2);
+      const float2 u = fma2(make_float2(-w[k].x, -w[k].y), w[k], w[k]);
+      const float2 u3 = mul2(mul2(u, u), u);
+      const float2 den = fma2(f2(2000.f), u3, t6);
+      m[k] = fma2(mul2(t6, t), rcp2(den), dk);
     }
     convexify5x2(m);
 #pragma unroll
@@ -213,7 +166,6 @@ __device__ __forceinline__ float2 weno9_edge2(const float2 (&d)[8], float2 s4, c
   return add2(s4, acc);
 }
 
-template <bool SKIP = PU_MAP_SKIP>
 __device__ __forceinline__ void weno9_edges2(const float2 (&s)[9], float2 &qL, float2 &qR, bool2 do_map, bool2 imm_L,
                                              bool2 imm_R) {
   using namespace pu_weno9;
@@ -245,8 +197,8 @@ __device__ __forceinline__ void weno9_edges2(const float2 (&s)[9], float2 &qL, f
   float2 rk[5];
 #pragma unroll
   for (int k = 0; k < 5; k++) rk[k] = rcp2(fma2(tv[k], tv[k], f2(1.e-20f)));
-  qL = weno9_edge2<true, SKIP>(d, s[4], rk, do_map);
-  qR = weno9_edge2<false, SKIP>(d, s[4], rk, do_map);
+  qL = weno9_edge2<true>(d, s[4], rk, do_map);
+  qR = weno9_edge2<false>(d, s[4], rk, do_map);
 }
 
 // Normalised nonlinear weights of the left edge (after map_rs when do_map),

@@ -1,15 +1,14 @@
-"""The FP32 order-9 limiter's forms agree bit for bit (pu_weno9_edges_f32):
-the scalar form and the packed two-stencil form, each with and without
-skipping map_rs when every normalised weight of an edge is within
-map_near(k) of its ideal value (where the map returns the ideal weight
-exactly, csrc/weno9.cuh).  Stencils: random normal, polynomials of degree
-<= 4, constants, smooth data plus noise of amplitude 1e-9 .. 1e-1 (weights
-on both sides of the bounds), steps, with random map and immersed flags.
-The scalar form is also held to the reference's float limiter (the oracle's
-weno9_batch_f32, bit-identical to WenoLimiter<float,9>): within 2e-5 of
-each stencil's range plus 5 % of its magnitude, the effect of the rearranged
-arithmetic (on a constant stencil this form returns the value exactly, the
-reference's polynomial coefficients only to float rounding)."""
+"""The FP32 order-9 limiter's two forms agree bit for bit
+(pu_weno9_edges_f32): the scalar form (z march, fallbacks) and the packed
+two-stencil form of the x/y kernel (FFMA2/FADD2/FMUL2).  Stencils: random
+normal, polynomials of degree <= 4, constants, smooth data plus noise of
+amplitude 1e-9 .. 1e-1 (weights from ideal to far from it), steps, with
+random map and immersed flags.  The scalar form is also held to the
+reference's float limiter (the oracle's weno9_batch_f32, bit-identical to
+WenoLimiter<float,9>): within 2e-5 of each stencil's range plus 5 % of its
+magnitude, the effect of the rearranged arithmetic (on a constant stencil
+this form returns the value exactly, the reference's polynomial
+coefficients only to float rounding)."""
 import ctypes as C
 
 import numpy as np
@@ -19,10 +18,6 @@ import pyoracle
 from porturb_b200 import capi
 
 pytestmark = pytest.mark.gpu
-
-D = np.array([5, 40, 60, 20, 1]) / 126.0
-T = np.array([2.2928e-2, 8.5599e-2, 9.6490e-2, 5.8021e-2, 6.5359e-3])
-
 
 def _stencils(n, seed=0):
     rng = np.random.default_rng(seed)
@@ -42,24 +37,6 @@ def _stencils(n, seed=0):
     return np.ascontiguousarray(s), flags
 
 
-def _near_fraction(s):
-    """Share of stencils (FP64 estimate) whose left-edge weights are all within the bounds."""
-    xs = np.arange(-4, 5)
-    tv = []
-    for k in range(5):
-        cells = np.arange(-4 + k, 1 + k)
-        A = np.array([[((cc + 0.5) ** (j + 1) - (cc - 0.5) ** (j + 1)) / (j + 1) for j in range(5)] for cc in cells])
-        co = s[:, k:k + 5].astype(np.float64) @ np.linalg.inv(A).T
-        a1, a2, a3, a4 = co[:, 1], co[:, 2], co[:, 3], co[:, 4]
-        tv.append(a1 * a1 + 13 / 3 * a2 * a2 + 0.5 * a1 * a3 + 39.1125 * a3 * a3 + 4.2 * a2 * a4 + 625.8 * a4 * a4)
-    tv = np.stack(tv, 1)
-    tot = tv.sum(1, keepdims=True)
-    tv = np.where(tot > 1e-20, tv / np.where(tot > 1e-20, tot, 1), tv)
-    w = D / (tv * tv + 1e-20)
-    w = w / w.sum(1, keepdims=True)
-    return np.all(np.abs(w - D) <= T, axis=1).mean(), np.all(np.abs(w - D) <= 3 * T, axis=1).mean()
-
-
 def _run(lib, s, flags, variant):
     n = s.shape[0]
     qL = np.empty(n, np.float32)
@@ -72,13 +49,10 @@ def _run(lib, s, flags, variant):
 
 def test_limiter_forms_agree_bit_for_bit(gpu_lib):
     s, flags = _stencils(40000)
-    near, near3 = _near_fraction(s)
-    print("stencils with every weight within the bounds: %.3f (within 3x: %.3f)" % (near, near3))
-    assert near > 0.1 and near3 - near > 0.05   # the skip and its surroundings are both exercised
-    out = [_run(gpu_lib, s, flags, v) for v in range(4)]
-    for v in range(1, 4):
-        assert np.array_equal(out[v][0].view(np.uint32), out[0][0].view(np.uint32)), v
-        assert np.array_equal(out[v][1].view(np.uint32), out[0][1].view(np.uint32)), v
+    out = [_run(gpu_lib, s, flags, v) for v in range(2)]
+    assert np.array_equal(out[1][0].view(np.uint32), out[0][0].view(np.uint32))
+    assert np.array_equal(out[1][1].view(np.uint32), out[0][1].view(np.uint32))
+    assert np.all(np.isfinite(out[0][0])) and np.all(np.isfinite(out[0][1]))
 
 
 def test_scalar_form_against_the_reference_limiter(oracle_lib, gpu_lib):

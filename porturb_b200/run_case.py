@@ -2,6 +2,7 @@
 
     python -m porturb_b200.run_case abl_neutral --nx 256 --ny 256 --nz 64 --steps 3
     python -m porturb_b200.run_case abl_neutral --nz 64 --learned --train-steps 300
+    python -m porturb_b200.run_case urban_canopy --nx 1024 --ny 1024 --nz 256 --dx 1 --steps 300 --diag-every 50
 
 Plain mode advances the FP32 (or --precision f64) dycore; --learned first
 harvests stencils from the initial state, trains the network on the GPU and
@@ -21,10 +22,14 @@ import numpy as np
 from . import cases
 from .dycore import Dycore
 
+def _dx(a):
+    return {} if a.dx is None else {"dx": a.dx}
+
+
 CASES = {
-    "abl_neutral": lambda a: cases.abl_neutral(nx=a.nx, ny=a.ny, nz=a.nz),
+    "abl_neutral": lambda a: cases.abl_neutral(nx=a.nx, ny=a.ny, nz=a.nz, **_dx(a)),
     "warm_bubble": lambda a: cases.warm_bubble(nx=a.nx, ny=a.ny, nz=a.nz),
-    "urban_canopy": lambda a: cases.urban_canopy(nx=a.nx, ny=a.ny, nz=a.nz),
+    "urban_canopy": lambda a: cases.urban_canopy(nx=a.nx, ny=a.ny, nz=a.nz, **_dx(a)),
 }
 
 
@@ -64,6 +69,9 @@ def main(argv=None):
     ap.add_argument("--ny", type=int, default=256)
     ap.add_argument("--nz", type=int, default=128)
     ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--dx", type=float, default=None, help="grid spacing in m (the case's default if absent)")
+    ap.add_argument("--diag-every", type=int, default=0,
+                    help="FP64 compensated mass / rho*theta / energy sums every N steps (timed with the steps)")
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--learned", action="store_true")
     ap.add_argument("--harvest", type=int, default=1 << 18)
@@ -92,11 +100,26 @@ def main(argv=None):
         g.learned_set_threshold(a.threshold)
         g.learned_counts()
     g.synchronize()
+    diags = []
+    if a.diag_every > 0:
+        diags.append(dict(step=0, **{k: v for k, v in g.diagnostics().items() if k != "tracer_mass"}))
     g.profile(True)
     t0 = time.perf_counter()
-    g.advance(dt, a.steps)
+    if a.diag_every > 0:
+        done = 0
+        while done < a.steps:
+            n = min(a.diag_every, a.steps - done)
+            g.advance(dt, n)
+            done += n
+            diags.append(dict(step=done, **{k: v for k, v in g.diagnostics().items() if k != "tracer_mass"}))
+    else:
+        g.advance(dt, a.steps)
     g.synchronize()
     wall = time.perf_counter() - t0
+    if diags:
+        out["diagnostics"] = diags
+        out["relative_drift"] = {k: abs(diags[-1][k] - diags[0][k]) / abs(diags[0][k])
+                                 for k in ("mass", "rho_theta", "total_energy")}
     prof = g.profile_read()
     g.profile(False)
     out["ms_per_step"] = wall * 1e3 / max(a.steps, 1)

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "impl.cuh"
+#include "tc_limiter.cuh"
 
 namespace pu {
 
@@ -367,6 +368,65 @@ __global__ void k_weno9_eval(const float *__restrict__ s, const unsigned char *_
       qR[b] = R.y;
     }
   }
+}
+
+// The FP32 limiter with its linear forms on the tensor cores
+// (tc_limiter.cuh): 128 stencils per block and round, one per thread.  The
+// waits on the MMA are bounded; a round whose MMA did not complete sets *err
+// and ends the kernel after releasing the tensor memory.
+__global__ void __launch_bounds__(128) k_weno9_tc(const float *__restrict__ s, const unsigned char *__restrict__ flags,
+                                                  long long n, float *__restrict__ qL, float *__restrict__ qR,
+                                                  int *err) {
+  namespace tc = pu::tc;
+  __shared__ __align__(1024) uint32_t a_hi[tc::TC_A_WORDS], a_lo[tc::TC_A_WORDS];
+  __shared__ __align__(1024) uint32_t b_hi[tc::TC_B_WORDS], b_lo[tc::TC_B_WORDS];
+  __shared__ __align__(8) unsigned long long mbar;
+  __shared__ uint32_t taddr_s;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  tc::fill_coefs(b_hi, b_lo);
+  const uint32_t mb = tc::smem_addr(&mbar);
+  if (tid == 0) tc::mbar_init(mb);
+  if (warp == 0) tc::tmem_alloc(tc::smem_addr(&taddr_s), 32);
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t taddr = taddr_s;
+  uint32_t phase = 0;
+  for (long long b0 = (long long)blockIdx.x * 128; b0 < n; b0 += (long long)gridDim.x * 128) {
+    const long long i = b0 + tid;
+    float st[9];
+#pragma unroll
+    for (int m = 0; m < 9; m++) st[m] = i < n ? s[i * 9 + m] : 0.f;
+    tc::stage_row(st, tid, a_hi, a_lo);
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      tc::issue(taddr, a_hi, a_lo, b_hi, b_lo);
+      tc::commit(mb);
+    }
+    const bool ok = __syncthreads_and(tc::mbar_wait(mb, phase));
+    phase ^= 1u;
+    if (!ok) {
+      if (tid == 0) atomicOr(err, 1);
+      break;
+    }
+    tc::fence_after_sync();
+    uint32_t r[32];
+    tc::tmem_ld32(taddr + (uint32_t(warp * 32) << 16), r);
+    if (i < n) {
+      const unsigned f = flags ? flags[i] : 1u;
+      float a, b;
+      tc::edges_from_row(r, st[4], a, b, (f & 1u) != 0, (f & 2u) != 0, (f & 4u) != 0);
+      qL[i] = a;
+      qR[i] = b;
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(taddr, 32);
 }
 
 }  // namespace
@@ -760,7 +820,7 @@ int pu_dycore_group_time_step(pu_dycore *const *hs, int n, pu_state_view *views,
 
 int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long long n, int variant, float *qL,
                        float *qR, int mem) {
-  if (!stencils || !qL || !qR || n < 0 || variant < 0 || variant > 1) return fail(PU_ERR_INVALID, "bad argument");
+  if (!stencils || !qL || !qR || n < 0 || variant < 0 || variant > 2) return fail(PU_ERR_INVALID, "bad argument");
   if (n == 0) return PU_OK;
   const bool dev = pu::resolve_mem(mem, stencils) == PU_MEM_DEVICE;
   float *ds = const_cast<float *>(stencils), *dl = qL, *dr = qR;
@@ -775,10 +835,23 @@ int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long l
   }
   const long long threads = variant == 0 ? n : (n + 1) / 2;
   const unsigned blocks = unsigned((threads + 255) / 256);
+  int *derr = nullptr;
   if (variant == 0) k_weno9_eval<0><<<blocks, 256>>>(ds, df, n, dl, dr);
-  else k_weno9_eval<1><<<blocks, 256>>>(ds, df, n, dl, dr);
+  else if (variant == 1) k_weno9_eval<1><<<blocks, 256>>>(ds, df, n, dl, dr);
+  else {
+    if (cudaMalloc(&derr, sizeof(int)) == cudaSuccess) {
+      cudaMemset(derr, 0, sizeof(int));
+      const long long nb = (n + 127) / 128;
+      k_weno9_tc<<<unsigned(nb < 148 * 8 ? nb : 148 * 8), 128>>>(ds, df, n, dl, dr, derr);
+    }
+  }
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  int herr = 0;
+  if (derr) {
+    cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(derr);
+  }
   if (!dev) {
     if (e == cudaSuccess) {
       cudaMemcpy(qL, dl, size_t(n) * sizeof(float), cudaMemcpyDeviceToHost);
@@ -790,6 +863,7 @@ int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long l
     if (df) cudaFree(df);
   }
   if (e != cudaSuccess) return fail(PU_ERR_CUDA, cudaGetErrorString(e));
+  if (herr) return fail(PU_ERR_CUDA, "tensor-core limiter: an MMA did not complete in time");
   return PU_OK;
 }
 

@@ -67,3 +67,26 @@ def test_scalar_form_against_the_reference_limiter(oracle_lib, gpu_lib):
     eL, eR = np.abs(qL - rL) / scale, np.abs(qR - rR) / scale
     print("max |gpu - reference| / scale: %.2e %.2e" % (eL.max(), eR.max()))
     assert eL.max() <= 2e-5 and eR.max() <= 2e-5
+
+
+def test_tensor_core_form_matches_the_fp32_forms(oracle_lib, gpu_lib):
+    """The tensor-core form (linear forms by tcgen05.mma in 3xTF32): within
+    the rounding of its reordered sums of the FP32 form, and as close to the
+    reference's float limiter as the FP32 form is (on the same stencils:
+    at most 3x the FP32 form's largest deviation)."""
+    s, flags = _stencils(40000, seed=2)
+    q0 = _run(gpu_lib, s, flags, 0)
+    q2 = _run(gpu_lib, s, flags, 2)
+    scale = (s.max(1) - s.min(1)) + 0.05 * np.abs(s).max(1) + 1e-30
+    eL = np.abs(q2[0] - q0[0]) / scale
+    eR = np.abs(q2[1] - q0[1]) / scale
+    print("max |tensor-core - fp32| / scale: %.2e %.2e" % (eL.max(), eR.max()))
+    assert eL.max() <= 1e-5 and eR.max() <= 1e-5
+    f1 = np.ones(s.shape[0], np.uint8)
+    rL, rR = pyoracle.weno9_batch_f32(s, do_map=True)
+    e = {}
+    for v in (0, 2):
+        qL, qR = _run(gpu_lib, s, f1, v)
+        e[v] = max((np.abs(qL - rL) / scale).max(), (np.abs(qR - rR) / scale).max())
+    print("max deviation from the reference / scale: fp32 %.2e, tensor-core %.2e" % (e[0], e[2]))
+    assert e[2] <= 3 * e[0] + 1e-6

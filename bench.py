@@ -52,7 +52,8 @@ LEARNED_THRESHOLD = 0.5
 
 def physics_modules(case, stream, world, reps=10):
     """The modules the boundary-layer driver runs beside the dycore every
-    dt_phys (geostrophic forcing, sponge, surface fluxes, LES closure) on
+    dt_phys (geostrophic forcing, sponge, surface fluxes, LES closure, time
+    averager) on
     device coupler arrays of the same workload: CUDA-event time per call and,
     for the LES kernel (the out-of-place form, no copy-back), algorithmic
     HBM bytes over its time."""
@@ -94,6 +95,17 @@ def physics_modules(case, stream, world, reps=10):
         ev1.record(stream)
         torch.cuda.synchronize()
         out[name + "_ms"] = reduce_max(ev0.elapsed_time(ev1) / reps, world)
+    # The time averager: reads u, v, w, TKE, reads and writes the 13 averages.
+    avgs = [torch.zeros_like(A[1]) for _ in range(13)]
+    etime = ph.time_average(*A, At, avgs, 0.0, 0.0, dt)
+    ph.synchronize()
+    ev0.record(stream)
+    for r in range(reps):
+        etime = ph.time_average(*A, At, avgs, etime, dt * (r + 1), dt)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    out["time_averager_ms"] = reduce_max(ev0.elapsed_time(ev1) / reps, world)
+    out["time_averager_gbs"] = 8.0 * N * (4 + 2 * 13) / (out["time_averager_ms"] / 1e3) / 1e9
     out["dtype"] = "f64"
     out["note"] = ("les_ms includes the copy-back of the in-place call; les_kernel_ms is the fused kernel alone; "
                    "FP64 pow/sqrt/division bound, not HBM bound")

@@ -11,6 +11,8 @@
  *   pu_uniform_pg_wind_forcing_height  modules::uniform_pg_wind_forcing_height
  *                                      uniform_pg_wind_forcing.h:43-82
  *                                      (city.cpp:130-136, cubes_periodic.cpp:147-152)
+ *   pu_time_averager_accumulate        custom_modules::Time_Averager::accumulate
+ *                                      experiments/examples/custom_modules/time_averager.h:56-110
  *
  * The reference's modules read their options and the immersed halo arrays
  * from the coupler; here a pu_physics handle holds them (created once, like
@@ -113,6 +115,28 @@ int pu_uniform_pg_wind_forcing(pu_physics *h, pu_state_view *v, double dt, doubl
  * tau <= 0.  Asynchronous for device views. */
 int pu_uniform_pg_wind_forcing_height(pu_physics *h, pu_state_view *v, double dt, double height, double u0, double v0,
                                       double tau);
+
+/* The running averages of custom_modules::Time_Averager
+ * (experiments/examples/custom_modules/time_averager.h:7-111, run after the
+ * LES closure in the boundary-layer drivers, abl_neutral.cpp:98-104): the
+ * coupler arrays avg_u .. long_avg_w ((nz,ny,nx) doubles in the memory space
+ * of the state view) and the option time_averager_etime. */
+typedef struct pu_time_averages {
+  double *avg_u, *avg_v, *avg_w, *avg_tke;
+  double *avg_up_up, *avg_up_vp, *avg_up_wp, *avg_vp_vp, *avg_vp_wp, *avg_wp_wp;
+  double *long_avg_u, *long_avg_v, *long_avg_w;
+  double etime; /* time_averager_etime: read, then advanced by dt */
+} pu_time_averages;
+
+/* Time_Averager::accumulate(coupler, dt) (time_averager.h:56-110): with
+ * inertia = etime/(etime+dt) and inertia_long = elapsed_time/(elapsed_time+dt)
+ * (the coupler option elapsed_time), long_avg_u/v/w relax toward u, v, w;
+ * avg_u/v/w/tke toward u, v, w, TKE and avg_up_up .. avg_wp_wp toward the
+ * products of the departures from the new long averages.  FP64 in the
+ * reference's order of operations (no contraction into fma), so results
+ * match the reference bit for bit.  PU_ERR_INVALID without a TKE tracer. */
+int pu_time_averager_accumulate(pu_physics *h, const pu_state_view *v, pu_time_averages *a, double elapsed_time,
+                                double dt);
 
 /* Waits for the handle's work. */
 int pu_physics_synchronize(pu_physics *h);

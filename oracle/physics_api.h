@@ -11,13 +11,18 @@
  *   apply_surface_fluxes            surface_flux.h:9-125
  *   uniform_pg_wind_forcing         uniform_pg_wind_forcing.h:6-40
  *   uniform_pg_wind_forcing_height  uniform_pg_wind_forcing.h:43-82
+ *   Time_Averager::accumulate       experiments/examples/custom_modules/time_averager.h:56-110
  * All arrays are C-order doubles: coupler fields (nz,ny,nx), tracers
  * (ntr,nz,ny,nx) in coupler order, immersed halo arrays (nz+2,ny+2,nx+2) with
  * one halo cell on each side (immersed_proportion_halos,
  * immersed_roughness_halos, immersed_temp_halos of the drivers' init,
  * sc_init.h:727-768).  The calls update the coupler arrays in place.
  * *_uniform_pg carries st = {counter, u0, v0, u, v} (the coupler options
- * uniform_pg_wind_forcing_counter, _u0, _v0, _u, _v) from call to call. */
+ * uniform_pg_wind_forcing_counter, _u0, _v0, _u, _v) from call to call.
+ * *_time_average takes the 13 averages as one [13][nz][ny][nx] block in the
+ * order avg_u, avg_v, avg_w, avg_tke, avg_up_up, avg_up_vp, avg_up_wp,
+ * avg_vp_vp, avg_vp_wp, avg_wp_wp, long_avg_u, long_avg_v, long_avg_w and the
+ * option time_averager_etime in *etime (advanced by dt). */
 #pragma once
 
 #ifdef __cplusplus
@@ -52,6 +57,8 @@ int orc_phys_uniform_pg(void *h, double *rho_d, double *u, double *v, double *w,
                         double tau, unsigned long long update_cycles, double *st);
 int orc_phys_uniform_pg_height(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
                                double dt, double height, double u0, double v0, double tau);
+int orc_phys_time_average(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                          double *avgs, double *etime, double elapsed_time, double dt);
 
 void *ref_phys_create(const orc_phys_config *cfg, const double *imm_prop_h, const double *imm_rough_h,
                       const double *imm_temp_h);
@@ -67,6 +74,8 @@ int ref_phys_uniform_pg(void *h, double *rho_d, double *u, double *v, double *w,
                         double tau, unsigned long long update_cycles, double *st);
 int ref_phys_uniform_pg_height(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
                                double dt, double height, double u0, double v0, double tau);
+int ref_phys_time_average(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                          double *avgs, double *etime, double elapsed_time, double dt);
 
 #ifdef __cplusplus
 }

@@ -11,6 +11,7 @@
 //   apply_surface_fluxes              surface_flux.h:9-125
 //   uniform_pg_wind_forcing           uniform_pg_wind_forcing.h:6-40
 //   uniform_pg_wind_forcing_height    uniform_pg_wind_forcing.h:43-82
+//   Time_Averager::accumulate         experiments/examples/custom_modules/time_averager.h:56-110
 // The arithmetic of each quantity is evaluated in the reference's order
 // (the build uses -ffp-contract=off), so the restatement is compared with the
 // reference's own modules bit for bit in the tests.  The code is organised
@@ -483,4 +484,36 @@ int orc_phys_uniform_pg_height(void *h, double *, double *u, double *v, double *
   return 0;
 }
 
-}  // extern "C
+// Time_Averager::accumulate (time_averager.h:56-110): exponential running
+// averages with inertia etime/(etime+dt) (long ones: elapsed/(elapsed+dt)),
+// the covariances of the departures from the updated long averages.
+int orc_phys_time_average(void *h, double *, double *u, double *v, double *w, double *, double *trc, double *avgs,
+                          double *etime, double elapsed_time, double dt) {
+  const orc_phys_config &c = static_cast<Phys *>(h)->c;
+  if (c.idTKE < 0) return 1;
+  const size_t n = size_t(c.nz) * c.ny * c.nx;
+  const double *tke = trc + size_t(c.idTKE) * n;
+  double *a[13];
+  for (int q = 0; q < 13; q++) a[q] = avgs + size_t(q) * n;
+  const double inertia = *etime / (*etime + dt), inertia_long = elapsed_time / (elapsed_time + dt);
+  for (size_t e = 0; e < n; e++) {
+    a[10][e] = inertia_long * a[10][e] + (1 - inertia_long) * u[e];
+    a[11][e] = inertia_long * a[11][e] + (1 - inertia_long) * v[e];
+    a[12][e] = inertia_long * a[12][e] + (1 - inertia_long) * w[e];
+    const double up = u[e] - a[10][e], vp = v[e] - a[11][e], wp = w[e] - a[12][e];
+    a[0][e] = inertia * a[0][e] + (1 - inertia) * u[e];
+    a[1][e] = inertia * a[1][e] + (1 - inertia) * v[e];
+    a[2][e] = inertia * a[2][e] + (1 - inertia) * w[e];
+    a[3][e] = inertia * a[3][e] + (1 - inertia) * tke[e];
+    a[4][e] = inertia * a[4][e] + (1 - inertia) * up * up;
+    a[5][e] = inertia * a[5][e] + (1 - inertia) * up * vp;
+    a[6][e] = inertia * a[6][e] + (1 - inertia) * up * wp;
+    a[7][e] = inertia * a[7][e] + (1 - inertia) * vp * vp;
+    a[8][e] = inertia * a[8][e] + (1 - inertia) * vp * wp;
+    a[9][e] = inertia * a[9][e] + (1 - inertia) * wp * wp;
+  }
+  *etime = *etime + dt;
+  return 0;
+}
+
+}  // extern "C"

@@ -72,7 +72,8 @@ def _lib(kind):
     getattr(lib, pre + "surface_fluxes").argtypes = arr + [D]
     getattr(lib, pre + "uniform_pg").argtypes = arr + [D, D, C.c_ulonglong, P]
     getattr(lib, pre + "uniform_pg_height").argtypes = arr + [D, D, D, D, D]
-    for nm in ("les", "sponge", "geostrophic", "surface_fluxes", "uniform_pg", "uniform_pg_height"):
+    getattr(lib, pre + "time_average").argtypes = arr + [P, P, D, D]
+    for nm in ("les", "sponge", "geostrophic", "surface_fluxes", "uniform_pg", "uniform_pg_height", "time_average"):
         getattr(lib, pre + nm).restype = C.c_int
     return lib
 
@@ -129,6 +130,18 @@ class Physics:
         if rc != 0:
             raise RuntimeError("%s_phys_uniform_pg failed" % self.kind)
         return s
+
+    def time_average(self, state, avgs, etime, elapsed_time, dt):
+        """avgs: float64 (13, nz, ny, nx) in the order of capi.TAVG_NAMES,
+        updated in place; returns the new etime."""
+        s = {k: np.array(v, dtype=np.float64, order="C", copy=True) for k, v in state.items()}
+        ptrs = [s[k].ctypes.data for k in ("rho_d", "uvel", "vvel", "wvel", "temp", "tracers")]
+        et = np.array([float(etime)])
+        rc = getattr(self.lib, self.kind + "_phys_time_average")(self.h, *ptrs, avgs.ctypes.data, et.ctypes.data,
+                                                                 float(elapsed_time), float(dt))
+        if rc != 0:
+            raise RuntimeError("%s_phys_time_average failed" % self.kind)
+        return float(et[0])
 
     def uniform_pg_height(self, state, dt, height, u0, v0, tau):
         return self._call("uniform_pg_height", state, dt, height, u0, v0, tau)

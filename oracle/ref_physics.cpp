@@ -2,8 +2,9 @@
 // INFRASTRUCTURE ONLY).
 //
 // Compiles model/modules/les_closure.h, sponge_layer.h,
-// geostrophic_wind_forcing.h, surface_flux.h and uniform_pg_wind_forcing.h
-// of the reference unchanged
+// geostrophic_wind_forcing.h, surface_flux.h and uniform_pg_wind_forcing.h,
+// and experiments/examples/custom_modules/time_averager.h, of the reference
+// unchanged
 // against the single-rank shim in oracle/ref_shim and exposes them through
 // the ref_phys_* functions of oracle/physics_api.h.  Each call copies the
 // given coupler arrays into the shim coupler's DataManager, runs the module
@@ -15,6 +16,7 @@
 #include "sponge_layer.h"
 #include "surface_flux.h"
 #include "uniform_pg_wind_forcing.h"
+#include "time_averager.h"
 
 #include <cstdio>
 #include <cstring>
@@ -200,4 +202,29 @@ int ref_phys_uniform_pg_height(void *p, double *rho_d, double *u, double *v, dou
   });
 }
 
-}  // extern "C
+int ref_phys_time_average(void *p, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                          double *avgs, double *etime, double elapsed_time, double dt) {
+  PhysHandle &h = *static_cast<PhysHandle *>(p);
+  return guarded([&]() {
+    static const char *names[13] = {"avg_u",      "avg_v",      "avg_w",     "avg_tke",   "avg_up_up",
+                                    "avg_up_vp",  "avg_up_wp",  "avg_vp_vp", "avg_vp_wp", "avg_wp_wp",
+                                    "long_avg_u", "long_avg_v", "long_avg_w"};
+    auto &c = h.coupler;
+    custom_modules::Time_Averager ta;
+    if (!c.get_data_manager_readonly().entry_exists("avg_u")) ta.init(c);
+    copy_in(h, rho_d, u, v, w, T, trc);
+    const size_t n = ncell(h.cfg);
+    auto &dm = c.get_data_manager_readwrite();
+    for (int q = 0; q < 13; q++) std::memcpy(dm.get<real, 3>(names[q]).data(), avgs + q * n, n * sizeof(double));
+    c.set_option<real>("time_averager_etime", *etime);
+    c.set_option<real>("elapsed_time", elapsed_time);
+    ta.accumulate(c, dt);
+    for (int q = 0; q < 13; q++)
+      std::memcpy(avgs + q * n, dm.get<real const, 3>(names[q]).data(), n * sizeof(double));
+    *etime = c.get_option<real>("time_averager_etime");
+    copy_out(h, rho_d, u, v, w, T, trc);
+    return 0;
+  });
+}
+
+}  // extern "C"

@@ -11,7 +11,8 @@ from . import capi, cases  # noqa: F401
 from .capi import PortUrbError  # noqa: F401
 from .dycore import (Coupler, Dycore, Dynamics_Euler_Stratified_WenoFV, assign_coupler_state,  # noqa: F401
                      case_coupler)
-from .physics import (LES_Closure, Physics, apply_surface_fluxes, geostrophic_wind_forcing,  # noqa: F401
-                      sponge_layer, uniform_pg_wind_forcing, uniform_pg_wind_forcing_height)
+from .physics import (LES_Closure, Physics, Time_Averager, apply_surface_fluxes,  # noqa: F401
+                      geostrophic_wind_forcing, sponge_layer, uniform_pg_wind_forcing,
+                      uniform_pg_wind_forcing_height)
 
 __version__ = "0.1.0"

@@ -94,6 +94,14 @@ class pu_uniform_pg_state(C.Structure):
                 ("u", C.c_double), ("v", C.c_double)]
 
 
+TAVG_NAMES = ("avg_u", "avg_v", "avg_w", "avg_tke", "avg_up_up", "avg_up_vp", "avg_up_wp", "avg_vp_vp", "avg_vp_wp",
+              "avg_wp_wp", "long_avg_u", "long_avg_v", "long_avg_w")
+
+
+class pu_time_averages(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in TAVG_NAMES] + [("etime", C.c_double)]
+
+
 class pu_profile(C.Structure):
     _fields_ = [("ms", C.c_double * PU_PROFILE_KINDS), ("launches", C.c_longlong * PU_PROFILE_KINDS)]
 
@@ -155,6 +163,7 @@ SIGNATURES = {
     "pu_uniform_pg_wind_forcing": (_I, [_P, C.POINTER(pu_state_view), _D, _D, C.c_ulonglong,
                                         C.POINTER(pu_uniform_pg_state)]),
     "pu_uniform_pg_wind_forcing_height": (_I, [_P, C.POINTER(pu_state_view), _D, _D, _D, _D, _D]),
+    "pu_time_averager_accumulate": (_I, [_P, C.POINTER(pu_state_view), C.POINTER(pu_time_averages), _D, _D]),
     "pu_physics_synchronize": (_I, [_P]),
     "pu_physics_last_les_ms": (_I, [_P, C.POINTER(_D)]),
 }

@@ -12,8 +12,8 @@
 // k_level_partial / k_level_final: deterministic level means (Neumaier-
 // compensated FP64 sums in a fixed order) for the sponge and the
 // geostrophic forcing and the pressure-gradient wind forcings; k_sponge /
-// k_geostrophic / k_surface_fluxes / k_add_uv / k_pg_height are pointwise
-// updates in place.
+// k_geostrophic / k_surface_fluxes / k_add_uv / k_pg_height /
+// k_time_average are pointwise updates in place.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -409,6 +409,46 @@ __global__ void k_pg_height(double *u, double *v, const double *mean, size_t n, 
   v[e] += dt_tau * (v0 - vm);
 }
 
+// Time_Averager::accumulate (time_averager.h:88-108), one cell per thread,
+// each product and sum rounded separately in the reference's order.  a[0..12]:
+// avg_u, avg_v, avg_w, avg_tke, avg_up_up, avg_up_vp, avg_up_wp, avg_vp_vp,
+// avg_vp_wp, avg_wp_wp, long_avg_u, long_avg_v, long_avg_w.
+struct TavgArrays {
+  double *a[13];
+};
+
+__global__ void k_time_average(const double *__restrict__ u, const double *__restrict__ v,
+                               const double *__restrict__ w, const double *__restrict__ tke, TavgArrays A, size_t n,
+                               double in, double omi, double inl, double omil) {
+  const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const double U = u[e], V = v[e], W = w[e], K = tke[e];
+  auto relax = [](double inertia, double avg, double om, double x) {
+    return __dadd_rn(__dmul_rn(inertia, avg), __dmul_rn(om, x));
+  };
+  const double lu = relax(inl, A.a[10][e], omil, U);
+  const double lv = relax(inl, A.a[11][e], omil, V);
+  const double lw = relax(inl, A.a[12][e], omil, W);
+  A.a[10][e] = lu;
+  A.a[11][e] = lv;
+  A.a[12][e] = lw;
+  const double up = __dsub_rn(U, lu), vp = __dsub_rn(V, lv), wp = __dsub_rn(W, lw);
+  A.a[0][e] = relax(in, A.a[0][e], omi, U);
+  A.a[1][e] = relax(in, A.a[1][e], omi, V);
+  A.a[2][e] = relax(in, A.a[2][e], omi, W);
+  A.a[3][e] = relax(in, A.a[3][e], omi, K);
+  // (1-inertia)*up*up groups as ((1-inertia)*up)*up.
+  auto relax2 = [](double inertia, double avg, double om, double x, double y) {
+    return __dadd_rn(__dmul_rn(inertia, avg), __dmul_rn(__dmul_rn(om, x), y));
+  };
+  A.a[4][e] = relax2(in, A.a[4][e], omi, up, up);
+  A.a[5][e] = relax2(in, A.a[5][e], omi, up, vp);
+  A.a[6][e] = relax2(in, A.a[6][e], omi, up, wp);
+  A.a[7][e] = relax2(in, A.a[7][e], omi, vp, vp);
+  A.a[8][e] = relax2(in, A.a[8][e], omi, vp, wp);
+  A.a[9][e] = relax2(in, A.a[9][e], omi, wp, wp);
+}
+
 // Log-law drag and heat flux from each immersed face neighbour, in the
 // order x-, x+, y-, y+, z-, z+ (surface_flux.h:40-117).
 __global__ void k_surface_fluxes(double *u, double *v, double *w, double *T, const double *prop, const double *rough,
@@ -458,6 +498,7 @@ struct pu_physics {
   double *stage = nullptr;     // (5 + ntr) * N: host views, and the in-place LES output
   double2 *partial = nullptr;  // level-sum partials
   double *mean = nullptr;      // level means [nz][3]
+  double *tavg_stage = nullptr;  // 13 * N: time averages given in host memory (allocated on first use)
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int nd = 0, qidx[4] = {0, 0, 0, 0};
 };
@@ -698,7 +739,7 @@ int pu_physics_destroy(pu_physics *h) {
     Dev g(h->cfg.device);
     cudaStreamSynchronize(h->st);
     for (void *p : {(void *)h->prop, (void *)h->rough, (void *)h->temp, (void *)h->stage, (void *)h->partial,
-                    (void *)h->mean})
+                    (void *)h->mean, (void *)h->tavg_stage})
       if (p) cudaFree(p);
     if (h->e0) cudaEventDestroy(h->e0);
     if (h->e1) cudaEventDestroy(h->e1);
@@ -900,6 +941,47 @@ int pu_uniform_pg_wind_forcing_height(pu_physics *h, pu_state_view *v, double dt
     const int which[2] = {1, 2};
     return copy_back(*h, v, d, which, 2);
   }
+  return PU_OK;
+}
+
+int pu_time_averager_accumulate(pu_physics *h, const pu_state_view *v, pu_time_averages *a, double elapsed_time,
+                                double dt) {
+  if (!h || !v || !a) return fail(PU_ERR_INVALID, "null argument");
+  if (h->cfg.idTKE < 0) return fail(PU_ERR_INVALID, "the time averager needs the TKE tracer");
+  double *host[13] = {a->avg_u,     a->avg_v,     a->avg_w,     a->avg_tke,    a->avg_up_up,
+                      a->avg_up_vp, a->avg_up_wp, a->avg_vp_vp, a->avg_vp_wp,  a->avg_wp_wp,
+                      a->long_avg_u, a->long_avg_v, a->long_avg_w};
+  for (double *p : host)
+    if (!p) return fail(PU_ERR_INVALID, "null time-average array");
+  Dev g(h->cfg.device);
+  double *d[5 + PU_MAX_TRACERS];
+  bool staged;
+  int rc = device_arrays(*h, v, d, staged);
+  if (rc) return rc;
+  TavgArrays A;
+  if (staged) {
+    if (!h->tavg_stage) PH_CK(cudaMalloc(&h->tavg_stage, 13 * h->N * sizeof(double)));
+    for (int q = 0; q < 13; q++) {
+      A.a[q] = h->tavg_stage + size_t(q) * h->N;
+      PH_CK(cudaMemcpyAsync(A.a[q], host[q], h->N * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    }
+  } else {
+    for (int q = 0; q < 13; q++) A.a[q] = host[q];
+  }
+  // time_averager.h:78-81: inertia from this averager's elapsed time, the
+  // long inertia from the coupler's.
+  const double inertia = a->etime / (a->etime + dt);
+  const double inertia_long = elapsed_time / (elapsed_time + dt);
+  k_time_average<<<unsigned((h->N + 255) / 256), 256, 0, h->st>>>(d[1], d[2], d[3], d[5 + h->cfg.idTKE], A, h->N,
+                                                                   inertia, 1 - inertia, inertia_long,
+                                                                   1 - inertia_long);
+  PH_CK(cudaGetLastError());
+  if (staged) {
+    for (int q = 0; q < 13; q++)
+      PH_CK(cudaMemcpyAsync(host[q], A.a[q], h->N * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    PH_CK(cudaStreamSynchronize(h->st));
+  }
+  a->etime = a->etime + dt;
   return PU_OK;
 }
 

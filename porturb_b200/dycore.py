@@ -291,6 +291,7 @@ class Coupler:
     # grid (coupler.h:132-341, one rank)
     def distribute_mpi_and_allocate_coupled_state(self, nz, ny_glob, nx_glob):
         self.nx, self.ny, self.nz = int(nx_glob), int(ny_glob), int(nz)
+        self.set_option("elapsed_time", 0.0)   # coupler.h:216
 
     def set_grid(self, xlen, ylen, zlen):
         self.xlen, self.ylen, self.zlen = float(xlen), float(ylen), float(zlen)

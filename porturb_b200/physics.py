@@ -9,8 +9,8 @@ reference), on top of include/pu_physics.h:
 * The reference's module API on a :class:`~porturb_b200.dycore.Coupler`:
   :class:`LES_Closure` (``init`` adds the TKE tracer, ``apply``),
   :func:`sponge_layer`, :func:`geostrophic_wind_forcing`,
-  :func:`apply_surface_fluxes`, :func:`uniform_pg_wind_forcing` and
-  :func:`uniform_pg_wind_forcing_height`, reading the options and the
+  :func:`apply_surface_fluxes`, :func:`uniform_pg_wind_forcing`,
+  :func:`uniform_pg_wind_forcing_height` and :class:`Time_Averager`, reading the options and the
   ``immersed_*_halos`` entries the drivers' init registers
   (sc_init.h:727-768).
 """
@@ -124,6 +124,20 @@ class Physics:
         check(self.lib.pu_uniform_pg_wind_forcing_height(self.h, C.byref(view), float(dt), float(height), float(u0),
                                                          float(v0), float(tau)))
 
+    def time_average(self, rho_d, u, v, w, T, tracers, averages, etime, elapsed_time, dt) -> float:
+        """Time_Averager.accumulate on coupler arrays: `averages` holds the 13
+        arrays named in capi.TAVG_NAMES (dict or sequence), updated in place;
+        returns the averager's new elapsed time (etime + dt)."""
+        view = make_view(rho_d, u, v, w, T, tracers)
+        a = capi.pu_time_averages()
+        seq = [averages[n] for n in capi.TAVG_NAMES] if isinstance(averages, dict) else list(averages)
+        for n, arr in zip(capi.TAVG_NAMES, seq):
+            setattr(a, n, _ptr(arr)[0])
+        a.etime = float(etime)
+        check(self.lib.pu_time_averager_accumulate(self.h, C.byref(view), C.byref(a), float(elapsed_time),
+                                                   float(dt)))
+        return a.etime
+
     def synchronize(self):
         check(self.lib.pu_physics_synchronize(self.h))
 
@@ -232,6 +246,38 @@ def uniform_pg_wind_forcing_height(coupler, dt, height, u0, v0, tau=10.0):
     relaxes the mean wind at `height` toward (u0, v0)."""
     rd, u, v, w, T, trc = _arrays(coupler)
     _handle(coupler, need_halos=False).uniform_pg_height(rd, u, v, w, T, trc, dt, height, u0, v0, tau)
+
+
+class Time_Averager:
+    """custom_modules::Time_Averager (experiments/examples/custom_modules/
+    time_averager.h:7-111): running averages of u, v, w, TKE and of the
+    velocity covariances, kept in coupler arrays avg_* / long_avg_* and the
+    option time_averager_etime."""
+
+    def init(self, coupler):
+        """time_averager.h:9-39."""
+        from . import output
+        coupler.set_option("time_averager_etime", 0.0)
+        shape = (coupler.get_nz(), coupler.get_ny(), coupler.get_nx())
+        for n in capi.TAVG_NAMES:
+            coupler.register_and_allocate(n, "", shape)
+            coupler.get(n)[...] = 0
+            coupler.register_output_variable(n, output.DIMS_3D)
+
+    def reset(self, coupler):
+        """time_averager.h:42-54: the short averages restart; the long ones do not."""
+        coupler.set_option("time_averager_etime", 0.0)
+        for n in capi.TAVG_NAMES[:10]:
+            coupler.get(n)[...] = 0
+
+    def accumulate(self, coupler, dt):
+        """time_averager.h:56-110."""
+        rd, u, v, w, T, trc = _arrays(coupler)
+        avgs = {n: coupler.get(n) for n in capi.TAVG_NAMES}
+        etime = _handle(coupler, need_halos=False).time_average(
+            rd, u, v, w, T, trc, avgs, coupler.get_option("time_averager_etime"),
+            coupler.get_option("elapsed_time"), dt)
+        coupler.set_option("time_averager_etime", etime)
 
 
 def register_immersed_halos(coupler, case, **kw):

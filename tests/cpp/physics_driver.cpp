@@ -1,7 +1,8 @@
 // Driver of the C++ drop-in modules in the order of the reference's
-// boundary-layer driver (abl_neutral.cpp:49-104): les_closure.init adds the
-// TKE tracer, dycore.init, then per call geostrophic forcing, dycore
-// time_step, sponge, surface fluxes, LES closure.  The coupler is the
+// boundary-layer driver (abl_neutral.cpp:49-108): les_closure.init adds the
+// TKE tracer, dycore.init, time_averager.init, then per call geostrophic
+// forcing, dycore time_step, sponge, surface fluxes, LES closure, time
+// averager, and elapsed_time advanced by dt.  The coupler is the
 // single-rank stand-in of oracle/ref_shim; the modules are the headers of
 // porturb_b200/cpp on libpu_dycore.so.
 //
@@ -11,7 +12,8 @@
 //           sponge_top; float64 base 6*N and pert 6*N (density_dry, uvel,
 //           vvel, wvel, temp, water_vapor); immersed proportion, roughness and
 //           temperature halo arrays, 3*(nz+2)(ny+2)(nx+2)
-//   output: float64 7*N (the five fields, water_vapor, TKE) after ncalls
+//   output: float64 7*N (the five fields, water_vapor, TKE) and 13*N (the time
+//           averages avg_u .. long_avg_w) after ncalls
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -21,6 +23,7 @@
 #include "les_closure.h"
 #include "sponge_layer.h"
 #include "surface_flux.h"
+#include "time_averager.h"
 
 template <class T>
 static void rd(FILE *f, T *p, size_t n) {
@@ -63,21 +66,30 @@ int main(int argc, char **argv) {
   };
   modules::LES_Closure les;
   modules::Dynamics_Euler_Stratified_WenoFV dycore;
+  custom_modules::Time_Averager tavg;
+  coupler.set_option<real>("elapsed_time", 0);
   load(base);
   les.init(coupler);
   dycore.init(coupler);
+  tavg.init(coupler);
   load(pert);
   const double dt = g[3];
+  double etime = 0;
   for (int c = 0; c < ncalls; c++) {
     modules::geostrophic_wind_forcing(coupler, dt, g[11], g[12], g[13]);
     dycore.time_step(coupler, dt);
     modules::sponge_layer(coupler, dt, g[14], g[15]);
     modules::apply_surface_fluxes(coupler, dt);
     les.apply(coupler, dt);
+    tavg.accumulate(coupler, dt);
+    etime += dt;
+    coupler.set_option<real>("elapsed_time", etime);
   }
   FILE *o = fopen(argv[2], "wb");
   for (int a = 0; a < 6; a++) fwrite(dm.get<real, 3>(sn[a]).data(), sizeof(double), N, o);
   fwrite(dm.get<real, 3>("TKE").data(), sizeof(double), N, o);
+  for (int q = 0; q < custom_modules::Time_Averager::NAVG; q++)
+    fwrite(dm.get<real, 3>(custom_modules::Time_Averager::name(q)).data(), sizeof(double), N, o);
   fclose(o);
   modules::pu_physics_module_finalize(coupler);
   dycore.finalize(coupler);

@@ -66,10 +66,10 @@ def test_dropin_matches_python_front_end(tmp_path):
 
 @pytest.mark.gpu
 def test_physics_dropin_chain_matches_python_front_end(tmp_path):
-    """The drop-in LES closure, sponge, geostrophic forcing and surface-flux
-    headers with the dycore, in the boundary-layer driver's order
-    (abl_neutral.cpp:93-104), give the same arrays as the same chain through
-    the Python API."""
+    """The drop-in LES closure, sponge, geostrophic forcing, surface-flux and
+    time-averager headers with the dycore, in the boundary-layer driver's
+    order (abl_neutral.cpp:93-108), give the same arrays as the same chain
+    through the Python API."""
     from porturb_b200 import Dycore, cases
     from porturb_b200.physics import Physics
     build_driver()
@@ -92,22 +92,27 @@ def test_physics_dropin_chain_matches_python_front_end(tmp_path):
         np.concatenate([h.ravel() for h in halos]).tofile(f)
     r = subprocess.run([exe, str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
-    out = np.fromfile(tmp_path / "out.bin", np.float64).reshape(7, case.nz, case.ny, case.nx)
+    out = np.fromfile(tmp_path / "out.bin", np.float64).reshape(20, case.nz, case.ny, case.nx)
 
     rd, u, v, w, T, trc = [np.ascontiguousarray(a) for a in base]
     g.init(rd, u, v, w, T, [np.ascontiguousarray(t) for t in trc], None)
     a = [np.ascontiguousarray(x.copy()) for x in pert[:5]]
     trs = [np.ascontiguousarray(t.copy()) for t in pert[5]]
     ph = Physics.from_case(case, halos=halos)
+    avgs = np.zeros((13, case.nz, case.ny, case.nx))
+    etime = elapsed = 0.0
     for _ in range(ncalls):
         ph.geostrophic(*a, trs, dt, lat_g, u_g, v_g)
         g.time_step(*a, trs, dt)
         ph.sponge(*a, trs, dt, t_sp, top)
         ph.surface_fluxes(*a, trs, dt)
         ph.les(*a, trs, dt)
-    ref = np.concatenate([np.stack(a), np.stack(trs)])
+        etime = ph.time_average(*a, trs, avgs, etime, elapsed, dt)
+        elapsed += dt
+    ref = np.concatenate([np.stack(a), np.stack(trs), avgs])
     assert np.array_equal(out, ref)
     assert not np.array_equal(ref[6], np.asarray(pert[5][1]))   # the closure changed TKE
+    assert np.abs(avgs[4]).max() > 0                             # the averager saw the fluctuations
 
 
 @pytest.mark.gpu

@@ -221,3 +221,74 @@ def test_uniform_pg_module_api_on_a_coupler(oracle_lib, gpu_lib):
     want = orc.uniform_pg_height(want, 0.1, 2.2 * dz, 7.0, 0.0, 4.0)
     got = dict(want, uvel=c.get("uvel"), vvel=c.get("vvel"))
     _check("coupler_pg", got, want, st)
+
+
+@pytest.mark.parametrize("device", [False, True])
+def test_time_averager_matches_oracle_bit_for_bit(oracle_lib, gpu_lib, device):
+    """pu_time_averager_accumulate over 5 calls with a changing state and a
+    reset: the GPU kernel rounds every product and sum as the reference does,
+    so it equals the oracle (itself equal to the reference's header) exactly."""
+    import torch
+    case, halos, _ = _case("plain")
+    orc = pyphysics.Physics(case, "orc", halos)
+    ph = Physics.from_case(case, halos=halos)
+    st = pyphysics.state_of(case, seed=13)
+    shape = (13,) + st["uvel"].shape
+    ao = np.zeros(shape)
+    ag = torch.zeros(shape, dtype=torch.float64, device="cuda") if device else np.zeros(shape)
+    eo = eg = 0.0
+    elapsed = 0.0
+    rng = np.random.default_rng(5)
+    for call in range(5):
+        if call == 3:
+            eo = eg = 0.0
+            ao[:10] = 0
+            ag[:10] = 0
+        dt = 0.2
+        eo = orc.time_average(st, ao, eo, elapsed, dt)
+        if device:
+            t = {k: torch.from_numpy(np.ascontiguousarray(st[k])).cuda() for k in ("rho_d", "uvel", "vvel", "wvel", "temp")}
+            trc = [torch.from_numpy(np.ascontiguousarray(st["tracers"][i])).cuda() for i in range(st["tracers"].shape[0])]
+            eg = ph.time_average(t["rho_d"], t["uvel"], t["vvel"], t["wvel"], t["temp"], trc, list(ag), eg, elapsed, dt)
+            ph.synchronize()
+            got = ag.cpu().numpy()
+        else:
+            trc = [np.ascontiguousarray(st["tracers"][i]) for i in range(st["tracers"].shape[0])]
+            eg = ph.time_average(st["rho_d"], st["uvel"], st["vvel"], st["wvel"], st["temp"], trc, list(ag), eg,
+                                 elapsed, dt)
+            got = ag
+        assert eg == eo
+        assert np.array_equal(got, ao), (call, np.abs(got - ao).max())
+        elapsed += dt
+        st = dict(st)
+        st["uvel"] = st["uvel"] + 0.3 * rng.standard_normal(st["uvel"].shape)
+    ph.close()
+
+
+def test_time_averager_module_api_on_a_coupler(oracle_lib, gpu_lib):
+    """Time_Averager.init / accumulate / reset on a Coupler keep the arrays and
+    the option time_averager_etime as the reference does."""
+    from porturb_b200 import LES_Closure, Time_Averager, case_coupler
+    case, halos, _ = _case("plain", nx=36, ny=16, nz=18)
+    c = case_coupler(case)
+    st = pyphysics.state_of(case, seed=14)
+    for k, name in (("uvel", "uvel"), ("vvel", "vvel"), ("wvel", "wvel")):
+        c.get(name)[...] = st[k]
+    for t, n in enumerate(c.get_tracer_names()):
+        c.get(n)[...] = st["tracers"][t]
+    ta = Time_Averager()
+    ta.init(c)
+    orc = pyphysics.Physics(case, "orc", halos)
+    avgs = np.zeros((13,) + st["uvel"].shape)
+    etime = 0.0
+    for call in range(3):
+        ta.accumulate(c, 0.5)
+        etime = orc.time_average(st, avgs, etime, c.get_option("elapsed_time"), 0.5)
+        c.set_option("elapsed_time", c.get_option("elapsed_time") + 0.5)
+    from porturb_b200 import capi
+    for q, n in enumerate(capi.TAVG_NAMES):
+        assert np.array_equal(c.get(n), avgs[q]), n
+    assert c.get_option("time_averager_etime") == etime == 1.5
+    ta.reset(c)
+    assert c.get_option("time_averager_etime") == 0.0
+    assert not c.get("avg_u").any() and c.get("long_avg_u").any()

@@ -155,3 +155,33 @@ def test_uniform_pg_height_known_answer_and_bad_height(oracle_lib):
     assert np.allclose(a["vvel"] - st["vvel"], 0.2 / 5.0 * (1.0 - vm), rtol=0, atol=1e-13)
     with pytest.raises(RuntimeError):
         orc.uniform_pg_height(st, 0.2, 0.4 * dz, 6.0, 1.0, 5.0)
+
+
+def test_time_averager_matches_reference_across_calls(oracle_lib):
+    """custom_modules::Time_Averager::accumulate over 6 calls with a changing
+    state and elapsed time, a reset (etime 0, short averages zeroed) midway:
+    the restatement equals the reference's header bit for bit."""
+    case, halos, _ = _case("plain")
+    orc = pyphysics.Physics(case, "orc", halos)
+    ref = pyphysics.Physics(case, "ref", halos)
+    st = pyphysics.state_of(case, seed=9)
+    shape = (13,) + st["uvel"].shape
+    ao, ar = np.zeros(shape), np.zeros(shape)
+    eo = er = 0.0
+    elapsed = 0.0
+    rng = np.random.default_rng(4)
+    for call in range(6):
+        if call == 3:
+            eo = er = 0.0
+            ao[:10] = 0
+            ar[:10] = 0
+        dt = 0.1 + 0.05 * call
+        eo = orc.time_average(st, ao, eo, elapsed, dt)
+        er = ref.time_average(st, ar, er, elapsed, dt)
+        assert eo == er
+        assert np.array_equal(ao, ar), call
+        elapsed += dt
+        st = dict(st)
+        st["uvel"] = st["uvel"] + 0.2 * rng.standard_normal(st["uvel"].shape)
+        st["wvel"] = st["wvel"] + 0.1 * rng.standard_normal(st["wvel"].shape)
+    assert np.abs(ao[4]).max() > 0 and np.abs(ao[10] - st["uvel"]).max() > 0

@@ -50,6 +50,34 @@ DYN_CYCLE = 10
 LEARNED_THRESHOLD = 0.5
 
 
+def decomposed_tiles(case, world, steps, warmup, grid=(2, 2)):
+    """The same workload as a grid of tiles of one process on this GPU
+    (pu_dycore_group_*: per stage a pack of the 5-cell halo slabs, device
+    copies between the tiles, the x/y kernel reading them): the cost of the
+    decomposed path without the interconnect."""
+    import torch
+    from porturb_b200 import decomp
+    grp = decomp.TileGroup(case, *grid, precision="f32")
+    grp.init_case(perturbed=False)
+    for h, c in zip(grp.handles, grp.cases):
+        rd, u, v, w, T, trc = [np.ascontiguousarray(a) for a in c.coupler_arrays(perturbed=True)]
+        h.load_state(rd, u, v, w, T, [np.ascontiguousarray(x) for x in trc])
+    dt = grp.handles[0].compute_time_step()
+    grp.advance(dt, warmup)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    grp.advance(dt, steps)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = reduce_max(ev0.elapsed_time(ev1), world)
+    grp.close()
+    return {"tiles": "%dx%d" % grid, "value": aggregate_value(case.ncells, steps, ms / 1e3, world),
+            "unit": "cell-steps/s", "ms_per_step": ms / steps,
+            "note": "tiles of one process on the legacy default stream: halo slabs packed and copied on the device "
+                    "every stage, no interconnect"}
+
+
 def physics_modules(case, stream, world, reps=10):
     """The modules the boundary-layer driver runs beside the dycore every
     dt_phys (geostrophic forcing, sponge, surface fluxes, LES closure, time
@@ -277,6 +305,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-physics", action="store_true")
+    ap.add_argument("--no-decomposed", action="store_true")
     args = ap.parse_args()
     world, rank, local = setup_dist()
     if args.impl == "reference":
@@ -354,6 +383,7 @@ def main():
     # Learned-weight form: network trained on stencils harvested from this
     # run's own state (GPU training kernels), then the same timed region.
     physics = None if args.no_physics else physics_modules(case, stream, world)
+    decomposed = None if args.no_decomposed else decomposed_tiles(case, world, min(args.steps, 10), args.warmup)
 
     learned = None
     if not args.no_learned:
@@ -440,6 +470,7 @@ def main():
             "clocks": clk,
             "learned": learned,
             "physics": physics,
+            "decomposed": decomposed,
         }
         print(json.dumps(line), flush=True)
     g.close()

@@ -48,9 +48,10 @@ namespace pu {
 #ifndef PU_XY_MIN_BLOCKS
 #define PU_XY_MIN_BLOCKS 4
 #endif
-// Minimum resident blocks per SM requested for the plain z march.
+// Minimum resident blocks per SM requested for the plain z march: 4 blocks
+// of 128 threads (at most 128 registers) measured 0.4 % faster than no cap.
 #ifndef PU_Z_MIN_BLOCKS
-#define PU_Z_MIN_BLOCKS 1
+#define PU_Z_MIN_BLOCKS 4
 #endif
 // Minimum resident blocks per SM requested for the learned stencil kernels
 // (caps their registers: the network's operand fragments stay in registers).

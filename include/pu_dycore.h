@@ -288,9 +288,10 @@ int pu_dycore_time_step_noalloc(const pu_config *cfg, const double *hy_dens_cell
  * consecutive floats: the left and right edge values of each.  flags[i]
  * (NULL: all 1): bit 0 do_map, bit 1 imm_L, bit 2 imm_R.  variant 0: the
  * scalar form (the z march, the FP64-free fallbacks); 1: the packed
- * two-stencil form of the x/y kernel (both give the same bits); 2: the
- * linear forms on the tensor cores (tcgen05.mma kind::tf32, three-term split;
- * agrees with the FP32 forms to rounding, not used by the dycore kernels).
+ * two-stencil form of the x/y kernel (both give the same bits); 2, 3: the
+ * linear forms on the tensor cores (tcgen05.mma kind::tf32, three-term split,
+ * A in shared memory / in tensor memory; the two give the same bits and
+ * agree with the FP32 forms to rounding; not used by the dycore kernels).
  * Host or device arrays (mem); synchronous, on the current device. */
 int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long long n, int variant, float *qL,
                        float *qR, int mem);

@@ -429,6 +429,74 @@ __global__ void __launch_bounds__(128) k_weno9_tc(const float *__restrict__ s, c
   if (warp == 0) tc::tmem_dealloc(taddr, 32);
 }
 
+// As k_weno9_tc with the A operand in tensor memory: 256 threads, two
+// halves of 128 rows on the same 128 lanes, A of half h in columns
+// 16h..16h+15 (hi, lo), its accumulator in columns 32+32h..; 128 columns.
+__global__ void __launch_bounds__(256) k_weno9_tc_ts(const float *__restrict__ s,
+                                                     const unsigned char *__restrict__ flags, long long n,
+                                                     float *__restrict__ qL, float *__restrict__ qR, int *err) {
+  namespace tc = pu::tc;
+  __shared__ __align__(1024) uint32_t b_hi[tc::TC_B_WORDS], b_lo[tc::TC_B_WORDS];
+  __shared__ __align__(8) unsigned long long mbar;
+  __shared__ uint32_t taddr_s;
+  const int tid = threadIdx.x, warp = tid >> 5, half = tid >> 7;
+  tc::fill_coefs(b_hi, b_lo);
+  const uint32_t mb = tc::smem_addr(&mbar);
+  if (tid == 0) tc::mbar_init(mb);
+  if (warp == 0) tc::tmem_alloc(tc::smem_addr(&taddr_s), 128);
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t taddr = taddr_s;
+  const uint32_t lane_base = uint32_t((warp & 3) * 32) << 16;
+  const uint64_t bh = tc::smem_desc(tc::smem_addr(b_hi)), bl = tc::smem_desc(tc::smem_addr(b_lo));
+  uint32_t phase = 0;
+  for (long long b0 = (long long)blockIdx.x * 256; b0 < n; b0 += (long long)gridDim.x * 256) {
+    const long long i = b0 + tid;
+    float st[9];
+#pragma unroll
+    for (int m = 0; m < 9; m++) st[m] = i < n ? s[i * 9 + m] : 0.f;
+    uint32_t v[16];
+    tc::split_row(st, v);
+    tc::tmem_st16(taddr + lane_base + uint32_t(16 * half), v);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const uint32_t a = taddr + uint32_t(16 * h), d = taddr + uint32_t(32 + 32 * h);
+        tc::mma_tf32_ts(d, a + 8, bh, 0u);
+        tc::mma_tf32_ts(d, a, bl, 1u);
+        tc::mma_tf32_ts(d, a, bh, 1u);
+      }
+      tc::commit(mb);
+    }
+    const bool ok = __syncthreads_and(tc::mbar_wait(mb, phase));
+    phase ^= 1u;
+    if (!ok) {
+      if (tid == 0) atomicOr(err, 1);
+      break;
+    }
+    tc::fence_after_sync();
+    uint32_t r[32];
+    tc::tmem_ld32(taddr + lane_base + uint32_t(32 + 32 * half), r);
+    if (i < n) {
+      const unsigned f = flags ? flags[i] : 1u;
+      float a, b;
+      tc::edges_from_row(r, st[4], a, b, (f & 1u) != 0, (f & 2u) != 0, (f & 4u) != 0);
+      qL[i] = a;
+      qR[i] = b;
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(taddr, 128);
+}
+
 }  // namespace
 
 extern "C" {
@@ -820,7 +888,7 @@ int pu_dycore_group_time_step(pu_dycore *const *hs, int n, pu_state_view *views,
 
 int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long long n, int variant, float *qL,
                        float *qR, int mem) {
-  if (!stencils || !qL || !qR || n < 0 || variant < 0 || variant > 2) return fail(PU_ERR_INVALID, "bad argument");
+  if (!stencils || !qL || !qR || n < 0 || variant < 0 || variant > 3) return fail(PU_ERR_INVALID, "bad argument");
   if (n == 0) return PU_OK;
   const bool dev = pu::resolve_mem(mem, stencils) == PU_MEM_DEVICE;
   float *ds = const_cast<float *>(stencils), *dl = qL, *dr = qR;
@@ -842,7 +910,12 @@ int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long l
     if (cudaMalloc(&derr, sizeof(int)) == cudaSuccess) {
       cudaMemset(derr, 0, sizeof(int));
       const long long nb = (n + 127) / 128;
-      k_weno9_tc<<<unsigned(nb < 148 * 8 ? nb : 148 * 8), 128>>>(ds, df, n, dl, dr, derr);
+      if (variant == 2) {
+        k_weno9_tc<<<unsigned(nb < 148 * 8 ? nb : 148 * 8), 128>>>(ds, df, n, dl, dr, derr);
+      } else {
+        const long long nb2 = (n + 255) / 256;
+        k_weno9_tc_ts<<<unsigned(nb2 < 148 * 4 ? nb2 : 148 * 4), 256>>>(ds, df, n, dl, dr, derr);
+      }
     }
   }
   cudaError_t e = cudaGetLastError();

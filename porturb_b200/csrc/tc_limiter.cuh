@@ -83,11 +83,12 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar) {
 }
 
 // Bounded wait for phase `parity` of the barrier; false if it did not come.
+// Polls with test_wait (no suspension of the waiting threads).
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); it++) {
+  for (int it = 0; it < (1 << 24); it++) {
     uint32_t ok;
     asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
         : "=r"(ok)
         : "r"(mbar), "r"(parity)
         : "memory");
@@ -122,6 +123,33 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
         "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
       : "r"(taddr));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// A taken from tensor memory (the "TS" form): lanes are rows, 8 columns of
+// TF32 per operand copy; same descriptor for C, same accumulator.
+__device__ __forceinline__ void mma_tf32_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %3, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %4, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b), "r"(accumulate), "r"(IDESC), "r"(z));
+}
+
+// This warp's lanes, 16 columns from taddr: one row of 16 values per thread.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16};" ::"r"(taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+      "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+      : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// One stencil's differences split into TF32 hi (values 0..7) and lo (8..15).
+__device__ __forceinline__ void split_row(const float (&s)[9], uint32_t (&v)[16]) {
+#pragma unroll
+  for (int m = 0; m < 8; m++) tf32_split(s[m + 1] - s[m], v[m], v[8 + m]);
 }
 
 // Coefficient q of output n (0..31) over difference k (0..7), FP64.

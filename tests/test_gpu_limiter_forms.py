@@ -77,6 +77,9 @@ def test_tensor_core_form_matches_the_fp32_forms(oracle_lib, gpu_lib):
     s, flags = _stencils(40000, seed=2)
     q0 = _run(gpu_lib, s, flags, 0)
     q2 = _run(gpu_lib, s, flags, 2)
+    q3 = _run(gpu_lib, s, flags, 3)
+    assert np.array_equal(q2[0].view(np.uint32), q3[0].view(np.uint32))   # A in shared or tensor memory
+    assert np.array_equal(q2[1].view(np.uint32), q3[1].view(np.uint32))
     scale = (s.max(1) - s.min(1)) + 0.05 * np.abs(s).max(1) + 1e-30
     eL = np.abs(q2[0] - q0[0]) / scale
     eR = np.abs(q2[1] - q0[1]) / scale

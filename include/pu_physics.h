@@ -13,6 +13,8 @@
  *                                      (city.cpp:130-136, cubes_periodic.cpp:147-152)
  *   pu_time_averager_accumulate        custom_modules::Time_Averager::accumulate
  *                                      experiments/examples/custom_modules/time_averager.h:56-110
+ *   pu_edge_sponge_set_column / _apply custom_modules::EdgeSponge::set_column / apply
+ *                                      experiments/examples/custom_modules/edge_sponge.h:14-57
  *
  * The reference's modules read their options and the immersed halo arrays
  * from the coupler; here a pu_physics handle holds them (created once, like
@@ -137,6 +139,23 @@ typedef struct pu_time_averages {
  * match the reference bit for bit.  PU_ERR_INVALID without a TKE tracer. */
 int pu_time_averager_accumulate(pu_physics *h, const pu_state_view *v, pu_time_averages *a, double elapsed_time,
                                 double dt);
+
+/* custom_modules::EdgeSponge (experiments/examples/custom_modules/
+ * edge_sponge.h:8-101; the urban and turbine drivers, city.cpp:97,137).
+ * fields: indices into the state view (0..4 = density_dry, uvel, vvel, wvel,
+ * temp; 5+t = tracer t; the reference's default set is 0..4).
+ * set_column: the horizontal mean of each field per level into column
+ * (nfields*nz doubles, host, field-major), FP64 with Neumaier compensation;
+ * synchronous.  apply: relaxes the fields toward column within the fractions
+ * prop_x1 / prop_x2 / prop_y1 / prop_y2 of the global domain next to its
+ * low-x / high-x / low-y / high-y edges, with weight ((p1-p)/p1)^5 (and the
+ * mirror at the high edges), applied in that order.  i_beg, j_beg, nx_glob,
+ * ny_glob place this tile in the global grid (0, 0, nx, ny on one rank); on
+ * several ranks the caller sums the tiles' column means itself. */
+int pu_edge_sponge_set_column(pu_physics *h, const pu_state_view *v, const int *fields, int nfields, double *column);
+int pu_edge_sponge_apply(pu_physics *h, pu_state_view *v, const int *fields, int nfields, const double *column,
+                         double prop_x1, double prop_x2, double prop_y1, double prop_y2, long long i_beg,
+                         long long j_beg, long long nx_glob, long long ny_glob);
 
 /* Waits for the handle's work. */
 int pu_physics_synchronize(pu_physics *h);

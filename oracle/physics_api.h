@@ -12,6 +12,7 @@
  *   uniform_pg_wind_forcing         uniform_pg_wind_forcing.h:6-40
  *   uniform_pg_wind_forcing_height  uniform_pg_wind_forcing.h:43-82
  *   Time_Averager::accumulate       experiments/examples/custom_modules/time_averager.h:56-110
+ *   EdgeSponge::set_column / apply  experiments/examples/custom_modules/edge_sponge.h:14-72
  * All arrays are C-order doubles: coupler fields (nz,ny,nx), tracers
  * (ntr,nz,ny,nx) in coupler order, immersed halo arrays (nz+2,ny+2,nx+2) with
  * one halo cell on each side (immersed_proportion_halos,
@@ -59,6 +60,12 @@ int orc_phys_uniform_pg_height(void *h, double *rho_d, double *u, double *v, dou
                                double dt, double height, double u0, double v0, double tau);
 int orc_phys_time_average(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
                           double *avgs, double *etime, double elapsed_time, double dt);
+/* Edge sponge on the five state fields (the reference's default set):
+ * column is (5, nz); set_column fills it, apply uses it. */
+int orc_phys_edge_sponge_set_column(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                                    double *column);
+int orc_phys_edge_sponge_apply(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                               const double *column, double px1, double px2, double py1, double py2);
 
 void *ref_phys_create(const orc_phys_config *cfg, const double *imm_prop_h, const double *imm_rough_h,
                       const double *imm_temp_h);
@@ -76,6 +83,10 @@ int ref_phys_uniform_pg_height(void *h, double *rho_d, double *u, double *v, dou
                                double dt, double height, double u0, double v0, double tau);
 int ref_phys_time_average(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
                           double *avgs, double *etime, double elapsed_time, double dt);
+int ref_phys_edge_sponge_set_column(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                                    double *column);
+int ref_phys_edge_sponge_apply(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                               const double *column, double px1, double px2, double py1, double py2);
 
 #ifdef __cplusplus
 }

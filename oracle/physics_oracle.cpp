@@ -12,6 +12,7 @@
 //   uniform_pg_wind_forcing           uniform_pg_wind_forcing.h:6-40
 //   uniform_pg_wind_forcing_height    uniform_pg_wind_forcing.h:43-82
 //   Time_Averager::accumulate         experiments/examples/custom_modules/time_averager.h:56-110
+//   EdgeSponge::set_column / apply    experiments/examples/custom_modules/edge_sponge.h:14-72
 // The arithmetic of each quantity is evaluated in the reference's order
 // (the build uses -ffp-contract=off), so the restatement is compared with the
 // reference's own modules bit for bit in the tests.  The code is organised
@@ -513,6 +514,56 @@ int orc_phys_time_average(void *h, double *, double *u, double *v, double *w, do
     a[9][e] = inertia * a[9][e] + (1 - inertia) * wp * wp;
   }
   *etime = *etime + dt;
+  return 0;
+}
+
+// EdgeSponge::set_column (edge_sponge.h:14-28, 75-96): per field and level
+// the sum over the level in (j, i) order, divided by nx*ny.
+int orc_phys_edge_sponge_set_column(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *,
+                                    double *column) {
+  const orc_phys_config &c = static_cast<Phys *>(h)->c;
+  const double *f[5] = {rho_d, u, v, w, T};
+  const size_t nl = size_t(c.ny) * c.nx;
+  for (int l = 0; l < 5; l++)
+    for (int k = 0; k < c.nz; k++) {
+      double s = 0;
+      for (size_t q = 0; q < nl; q++) s += f[l][size_t(k) * nl + q];
+      column[size_t(l) * c.nz + k] = s / (c.nx * c.ny);
+    }
+  return 0;
+}
+
+// EdgeSponge::apply (edge_sponge.h:31-72): the four edge zones in turn, each
+// blending toward the column profile with weight ((p1-p)/p1)^5.
+int orc_phys_edge_sponge_apply(void *h, double *rho_d, double *u, double *v, double *w, double *T, double *,
+                               const double *column, double px1, double px2, double py1, double py2) {
+  const orc_phys_config &c = static_cast<Phys *>(h)->c;
+  double *f[5] = {rho_d, u, v, w, T};
+  const float pwr = 5;
+  for (int l = 0; l < 5; l++)
+    for (int k = 0; k < c.nz; k++)
+      for (int j = 0; j < c.ny; j++)
+        for (int i = 0; i < c.nx; i++) {
+          double &x = f[l][(size_t(k) * c.ny + j) * c.nx + i];
+          const double col = column[size_t(l) * c.nz + k];
+          const double prop_x = double(i) / c.nx, prop_y = double(j) / c.ny;
+          if (px1 > 0 && prop_x <= px1) {
+            const double wt = std::pow((px1 - prop_x) / px1, pwr);
+            x = wt * col + (1 - wt) * x;
+          }
+          if (px2 > 0 && prop_x >= 1 - px2) {
+            const double wt = std::pow((prop_x - (1 - px2)) / px2, pwr);
+            x = wt * col + (1 - wt) * x;
+          }
+          if (py1 > 0 && prop_y <= py1) {
+            const double wt = std::pow((py1 - prop_y) / py1, pwr);
+            x = wt * col + (1 - wt) * x;
+          }
+          if (py2 > 0 && prop_y >= 1 - py2) {
+            const double wt = std::pow((prop_y - (1 - py2)) / py2, pwr);
+            x = wt * col + (1 - wt) * x;
+          }
+        }
   return 0;
 }
 

@@ -73,7 +73,10 @@ def _lib(kind):
     getattr(lib, pre + "uniform_pg").argtypes = arr + [D, D, C.c_ulonglong, P]
     getattr(lib, pre + "uniform_pg_height").argtypes = arr + [D, D, D, D, D]
     getattr(lib, pre + "time_average").argtypes = arr + [P, P, D, D]
-    for nm in ("les", "sponge", "geostrophic", "surface_fluxes", "uniform_pg", "uniform_pg_height", "time_average"):
+    getattr(lib, pre + "edge_sponge_set_column").argtypes = arr + [P]
+    getattr(lib, pre + "edge_sponge_apply").argtypes = arr + [P, D, D, D, D]
+    for nm in ("les", "sponge", "geostrophic", "surface_fluxes", "uniform_pg", "uniform_pg_height", "time_average",
+               "edge_sponge_set_column", "edge_sponge_apply"):
         getattr(lib, pre + nm).restype = C.c_int
     return lib
 
@@ -142,6 +145,25 @@ class Physics:
         if rc != 0:
             raise RuntimeError("%s_phys_time_average failed" % self.kind)
         return float(et[0])
+
+    def edge_sponge_set_column(self, state):
+        """(5, nz) column profiles of density_dry, uvel, vvel, wvel, temp."""
+        s = {k: np.array(v, dtype=np.float64, order="C", copy=True) for k, v in state.items()}
+        ptrs = [s[k].ctypes.data for k in ("rho_d", "uvel", "vvel", "wvel", "temp", "tracers")]
+        col = np.zeros((5, s["uvel"].shape[0]))
+        if getattr(self.lib, self.kind + "_phys_edge_sponge_set_column")(self.h, *ptrs, col.ctypes.data) != 0:
+            raise RuntimeError("%s_phys_edge_sponge_set_column failed" % self.kind)
+        return col
+
+    def edge_sponge_apply(self, state, column, px1, px2, py1, py2):
+        s = {k: np.array(v, dtype=np.float64, order="C", copy=True) for k, v in state.items()}
+        ptrs = [s[k].ctypes.data for k in ("rho_d", "uvel", "vvel", "wvel", "temp", "tracers")]
+        col = np.ascontiguousarray(column, dtype=np.float64)
+        rc = getattr(self.lib, self.kind + "_phys_edge_sponge_apply")(self.h, *ptrs, col.ctypes.data, float(px1),
+                                                                      float(px2), float(py1), float(py2))
+        if rc != 0:
+            raise RuntimeError("%s_phys_edge_sponge_apply failed" % self.kind)
+        return s
 
     def uniform_pg_height(self, state, dt, height, u0, v0, tau):
         return self._call("uniform_pg_height", state, dt, height, u0, v0, tau)

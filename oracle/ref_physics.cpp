@@ -3,8 +3,8 @@
 //
 // Compiles model/modules/les_closure.h, sponge_layer.h,
 // geostrophic_wind_forcing.h, surface_flux.h and uniform_pg_wind_forcing.h,
-// and experiments/examples/custom_modules/time_averager.h, of the reference
-// unchanged
+// and experiments/examples/custom_modules/time_averager.h and edge_sponge.h,
+// of the reference unchanged
 // against the single-rank shim in oracle/ref_shim and exposes them through
 // the ref_phys_* functions of oracle/physics_api.h.  Each call copies the
 // given coupler arrays into the shim coupler's DataManager, runs the module
@@ -17,6 +17,7 @@
 #include "surface_flux.h"
 #include "uniform_pg_wind_forcing.h"
 #include "time_averager.h"
+#include "edge_sponge.h"
 
 #include <cstdio>
 #include <cstring>
@@ -222,6 +223,37 @@ int ref_phys_time_average(void *p, double *rho_d, double *u, double *v, double *
     for (int q = 0; q < 13; q++)
       std::memcpy(avgs + q * n, dm.get<real const, 3>(names[q]).data(), n * sizeof(double));
     *etime = c.get_option<real>("time_averager_etime");
+    copy_out(h, rho_d, u, v, w, T, trc);
+    return 0;
+  });
+}
+
+int ref_phys_edge_sponge_set_column(void *p, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                                    double *column) {
+  PhysHandle &h = *static_cast<PhysHandle *>(p);
+  return guarded([&]() {
+    copy_in(h, rho_d, u, v, w, T, trc);
+    custom_modules::EdgeSponge es;
+    es.set_column(h.coupler);
+    const int nz = h.cfg.nz;
+    for (int l = 0; l < 5; l++)
+      for (int k = 0; k < nz; k++) column[size_t(l) * nz + k] = es.column(l, k);
+    return 0;
+  });
+}
+
+int ref_phys_edge_sponge_apply(void *p, double *rho_d, double *u, double *v, double *w, double *T, double *trc,
+                               const double *column, double px1, double px2, double py1, double py2) {
+  PhysHandle &h = *static_cast<PhysHandle *>(p);
+  return guarded([&]() {
+    copy_in(h, rho_d, u, v, w, T, trc);
+    custom_modules::EdgeSponge es;
+    es.names = {"density_dry", "uvel", "vvel", "wvel", "temp"};
+    const int nz = h.cfg.nz;
+    es.column = real2d("column", 5, nz);
+    for (int l = 0; l < 5; l++)
+      for (int k = 0; k < nz; k++) es.column(l, k) = column[size_t(l) * nz + k];
+    es.apply(h.coupler, px1, px2, py1, py2);
     copy_out(h, rho_d, u, v, w, T, trc);
     return 0;
   });

@@ -51,7 +51,13 @@ typedef int MPI_Op;
 namespace Kokkos {
 inline void abort(const char *msg) { throw std::runtime_error(std::string("Kokkos::abort: ") + msg); }
 inline void fence() {}
+// One thread: the atomic add is a plain add, in the loop's index order.
+template <class T>
+inline void atomic_add(T *dst, T v) { *dst += v; }
 }  // namespace Kokkos
+
+// A local name for a member the kernel lambda captures by value in yakl.
+#define YAKL_SCOPE(local, expr) auto &local = expr
 
 inline void endrun(std::string msg = "") { throw std::runtime_error("endrun: " + msg); }
 

@@ -11,7 +11,7 @@ from . import capi, cases  # noqa: F401
 from .capi import PortUrbError  # noqa: F401
 from .dycore import (Coupler, Dycore, Dynamics_Euler_Stratified_WenoFV, assign_coupler_state,  # noqa: F401
                      case_coupler)
-from .physics import (LES_Closure, Physics, Time_Averager, apply_surface_fluxes,  # noqa: F401
+from .physics import (EdgeSponge, LES_Closure, Physics, Time_Averager, apply_surface_fluxes,  # noqa: F401
                       geostrophic_wind_forcing, sponge_layer, uniform_pg_wind_forcing,
                       uniform_pg_wind_forcing_height)
 

@@ -164,6 +164,9 @@ SIGNATURES = {
                                         C.POINTER(pu_uniform_pg_state)]),
     "pu_uniform_pg_wind_forcing_height": (_I, [_P, C.POINTER(pu_state_view), _D, _D, _D, _D, _D]),
     "pu_time_averager_accumulate": (_I, [_P, C.POINTER(pu_state_view), C.POINTER(pu_time_averages), _D, _D]),
+    "pu_edge_sponge_set_column": (_I, [_P, C.POINTER(pu_state_view), _P, _I, _P]),
+    "pu_edge_sponge_apply": (_I, [_P, C.POINTER(pu_state_view), _P, _I, _P, _D, _D, _D, _D, C.c_longlong,
+                                  C.c_longlong, C.c_longlong, C.c_longlong]),
     "pu_physics_synchronize": (_I, [_P]),
     "pu_physics_last_les_ms": (_I, [_P, C.POINTER(_D)]),
 }

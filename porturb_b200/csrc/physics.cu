@@ -13,7 +13,7 @@
 // compensated FP64 sums in a fixed order) for the sponge and the
 // geostrophic forcing and the pressure-gradient wind forcings; k_sponge /
 // k_geostrophic / k_surface_fluxes / k_add_uv / k_pg_height /
-// k_time_average are pointwise updates in place.
+// k_time_average / k_edge_sponge are pointwise updates in place.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -449,6 +449,41 @@ __global__ void k_time_average(const double *__restrict__ u, const double *__res
   A.a[9][e] = relax2(in, A.a[9][e], omi, wp, wp);
 }
 
+// EdgeSponge::apply (edge_sponge.h:47-71) on up to 8 fields: the four edge
+// zones in the reference's order, each weight ((p1-p)/p1)^5.
+struct SpongeFields {
+  double *f[8];
+};
+
+__global__ void k_edge_sponge(SpongeFields S, int nfields, const double *__restrict__ column, int nx, int ny, int nz,
+                              long long i_beg, long long j_beg, long long nx_glob, long long ny_glob, double px1,
+                              double px2, double py1, double py2) {
+  const size_t n = size_t(nx) * ny * nz;
+  const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const int i = int(e % nx), j = int((e / nx) % ny), k = int(e / (size_t(nx) * ny));
+  const double prop_x = double(i_beg + i) / double(nx_glob), prop_y = double(j_beg + j) / double(ny_glob);
+  double w[4];
+  bool on[4];
+  on[0] = px1 > 0 && prop_x <= px1;
+  on[1] = px2 > 0 && prop_x >= 1 - px2;
+  on[2] = py1 > 0 && prop_y <= py1;
+  on[3] = py2 > 0 && prop_y >= 1 - py2;
+  if (!(on[0] || on[1] || on[2] || on[3])) return;
+  w[0] = on[0] ? pow((px1 - prop_x) / px1, 5.0) : 0.0;
+  w[1] = on[1] ? pow((prop_x - (1 - px2)) / px2, 5.0) : 0.0;
+  w[2] = on[2] ? pow((py1 - prop_y) / py1, 5.0) : 0.0;
+  w[3] = on[3] ? pow((prop_y - (1 - py2)) / py2, 5.0) : 0.0;
+  for (int l = 0; l < nfields; l++) {
+    double x = S.f[l][e];
+    const double c = column[size_t(l) * nz + k];
+#pragma unroll
+    for (int z = 0; z < 4; z++)
+      if (on[z]) x = w[z] * c + (1 - w[z]) * x;
+    S.f[l][e] = x;
+  }
+}
+
 // Log-law drag and heat flux from each immersed face neighbour, in the
 // order x-, x+, y-, y+, z-, z+ (surface_flux.h:40-117).
 __global__ void k_surface_fluxes(double *u, double *v, double *w, double *T, const double *prop, const double *rough,
@@ -499,6 +534,8 @@ struct pu_physics {
   double2 *partial = nullptr;  // level-sum partials
   double *mean = nullptr;      // level means [nz][3]
   double *tavg_stage = nullptr;  // 13 * N: time averages given in host memory (allocated on first use)
+  double *column = nullptr;      // edge-sponge column profiles, column_cap doubles
+  size_t column_cap = 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int nd = 0, qidx[4] = {0, 0, 0, 0};
 };
@@ -739,7 +776,7 @@ int pu_physics_destroy(pu_physics *h) {
     Dev g(h->cfg.device);
     cudaStreamSynchronize(h->st);
     for (void *p : {(void *)h->prop, (void *)h->rough, (void *)h->temp, (void *)h->stage, (void *)h->partial,
-                    (void *)h->mean, (void *)h->tavg_stage})
+                    (void *)h->mean, (void *)h->tavg_stage, (void *)h->column})
       if (p) cudaFree(p);
     if (h->e0) cudaEventDestroy(h->e0);
     if (h->e1) cudaEventDestroy(h->e1);
@@ -982,6 +1019,72 @@ int pu_time_averager_accumulate(pu_physics *h, const pu_state_view *v, pu_time_a
     PH_CK(cudaStreamSynchronize(h->st));
   }
   a->etime = a->etime + dt;
+  return PU_OK;
+}
+
+int pu_edge_sponge_set_column(pu_physics *h, const pu_state_view *v, const int *fields, int nfields, double *column) {
+  if (!h || !v || !fields || !column) return fail(PU_ERR_INVALID, "null argument");
+  const int S = 5 + h->cfg.ntracers;
+  if (nfields < 1 || nfields > 8) return fail(PU_ERR_INVALID, "edge sponge: 1 to 8 fields");
+  for (int l = 0; l < nfields; l++)
+    if (fields[l] < 0 || fields[l] >= S) return fail(PU_ERR_INVALID, "edge sponge: bad field index");
+  Dev g(h->cfg.device);
+  double *d[5 + PU_MAX_TRACERS];
+  bool staged;
+  int rc = device_arrays(*h, v, d, staged);
+  if (rc) return rc;
+  const int nz = h->cfg.nz;
+  std::vector<double> m(size_t(nz) * 3);
+  for (int l0 = 0; l0 < nfields; l0 += 3) {
+    const int nf = std::min(3, nfields - l0);
+    rc = level_means(*h, d[fields[l0]], nf > 1 ? d[fields[l0 + 1]] : nullptr, nf > 2 ? d[fields[l0 + 2]] : nullptr,
+                     nf, 0);
+    if (rc) return rc;
+    PH_CK(cudaMemcpyAsync(m.data(), h->mean, m.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    PH_CK(cudaStreamSynchronize(h->st));
+    for (int f = 0; f < nf; f++)
+      for (int k = 0; k < nz; k++) column[size_t(l0 + f) * nz + k] = m[size_t(k) * 3 + f];
+  }
+  return PU_OK;
+}
+
+int pu_edge_sponge_apply(pu_physics *h, pu_state_view *v, const int *fields, int nfields, const double *column,
+                         double prop_x1, double prop_x2, double prop_y1, double prop_y2, long long i_beg,
+                         long long j_beg, long long nx_glob, long long ny_glob) {
+  if (!h || !v || !fields || !column) return fail(PU_ERR_INVALID, "null argument");
+  const int S = 5 + h->cfg.ntracers;
+  if (nfields < 1 || nfields > 8) return fail(PU_ERR_INVALID, "edge sponge: 1 to 8 fields");
+  for (int l = 0; l < nfields; l++)
+    if (fields[l] < 0 || fields[l] >= S) return fail(PU_ERR_INVALID, "edge sponge: bad field index");
+  if (nx_glob < h->cfg.nx || ny_glob < h->cfg.ny || i_beg < 0 || j_beg < 0)
+    return fail(PU_ERR_INVALID, "edge sponge: bad tile placement");
+  Dev g(h->cfg.device);
+  double *d[5 + PU_MAX_TRACERS];
+  bool staged;
+  int rc = device_arrays(*h, v, d, staged);
+  if (rc) return rc;
+  const size_t nc = size_t(nfields) * h->cfg.nz;
+  if (h->column_cap < nc) {
+    if (h->column) cudaFree(h->column);
+    h->column = nullptr;
+    h->column_cap = 0;
+    PH_CK(cudaMalloc(&h->column, nc * sizeof(double)));
+    h->column_cap = nc;
+  }
+  PH_CK(cudaMemcpyAsync(h->column, column, nc * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  SpongeFields F{};
+  for (int l = 0; l < nfields; l++) F.f[l] = d[fields[l]];
+  k_edge_sponge<<<unsigned((h->N + 255) / 256), 256, 0, h->st>>>(F, nfields, h->column, h->cfg.nx, h->cfg.ny,
+                                                                 h->cfg.nz, i_beg, j_beg, nx_glob, ny_glob, prop_x1,
+                                                                 prop_x2, prop_y1, prop_y2);
+  PH_CK(cudaGetLastError());
+  // The column is a host array: it must stay valid until the copy is done.
+  PH_CK(cudaStreamSynchronize(h->st));
+  if (staged) {
+    int which[8];
+    for (int l = 0; l < nfields; l++) which[l] = fields[l];
+    return copy_back(*h, v, d, which, nfields);
+  }
   return PU_OK;
 }
 

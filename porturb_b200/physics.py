@@ -10,7 +10,8 @@ reference), on top of include/pu_physics.h:
   :class:`LES_Closure` (``init`` adds the TKE tracer, ``apply``),
   :func:`sponge_layer`, :func:`geostrophic_wind_forcing`,
   :func:`apply_surface_fluxes`, :func:`uniform_pg_wind_forcing`,
-  :func:`uniform_pg_wind_forcing_height` and :class:`Time_Averager`, reading the options and the
+  :func:`uniform_pg_wind_forcing_height`, :class:`Time_Averager` and
+  :class:`EdgeSponge`, reading the options and the
   ``immersed_*_halos`` entries the drivers' init registers
   (sc_init.h:727-768).
 """
@@ -137,6 +138,27 @@ class Physics:
         check(self.lib.pu_time_averager_accumulate(self.h, C.byref(view), C.byref(a), float(elapsed_time),
                                                    float(dt)))
         return a.etime
+
+    def edge_sponge_set_column(self, rho_d, u, v, w, T, tracers, fields=(0, 1, 2, 3, 4)) -> np.ndarray:
+        """EdgeSponge.set_column: (len(fields), nz) horizontal means of the
+        state-view fields (0..4 = density_dry, uvel, vvel, wvel, temp; 5+t
+        tracer t)."""
+        view = make_view(rho_d, u, v, w, T, tracers)
+        idx = np.ascontiguousarray(fields, dtype=np.int32)
+        col = np.zeros((len(idx), self.shape[0]))
+        check(self.lib.pu_edge_sponge_set_column(self.h, C.byref(view), idx.ctypes.data, len(idx), col.ctypes.data))
+        return col
+
+    def edge_sponge(self, rho_d, u, v, w, T, tracers, column, prop_x1=0.1, prop_x2=0.1, prop_y1=0.1, prop_y2=0.1,
+                    fields=(0, 1, 2, 3, 4)):
+        """EdgeSponge.apply on one rank (the tile is the whole domain)."""
+        view = make_view(rho_d, u, v, w, T, tracers)
+        idx = np.ascontiguousarray(fields, dtype=np.int32)
+        col = np.ascontiguousarray(column, dtype=np.float64)
+        nz, ny, nx = self.shape
+        check(self.lib.pu_edge_sponge_apply(self.h, C.byref(view), idx.ctypes.data, len(idx), col.ctypes.data,
+                                            float(prop_x1), float(prop_x2), float(prop_y1), float(prop_y2), 0, 0,
+                                            nx, ny))
 
     def synchronize(self):
         check(self.lib.pu_physics_synchronize(self.h))
@@ -278,6 +300,37 @@ class Time_Averager:
             rd, u, v, w, T, trc, avgs, coupler.get_option("time_averager_etime"),
             coupler.get_option("elapsed_time"), dt)
         coupler.set_option("time_averager_etime", etime)
+
+
+_STATE_FIELDS = ("density_dry", "uvel", "vvel", "wvel", "temp")
+
+
+class EdgeSponge:
+    """custom_modules::EdgeSponge (experiments/examples/custom_modules/
+    edge_sponge.h:8-101): set_column records the horizontal-mean profile of
+    the named coupler fields; apply relaxes them toward it near the lateral
+    edges of the domain."""
+
+    def __init__(self):
+        self.names = []
+        self.column = None
+
+    def _fields(self, coupler):
+        trc = list(coupler.get_tracer_names())
+        return [(_STATE_FIELDS.index(n) if n in _STATE_FIELDS else 5 + trc.index(n)) for n in self.names]
+
+    def set_column(self, coupler, names_in=_STATE_FIELDS):
+        """edge_sponge.h:14-28."""
+        self.names = list(names_in)
+        rd, u, v, w, T, trc = _arrays(coupler)
+        self.column = _handle(coupler, need_halos=False).edge_sponge_set_column(rd, u, v, w, T, trc,
+                                                                                self._fields(coupler))
+
+    def apply(self, coupler, prop_x1=0.1, prop_x2=0.1, prop_y1=0.1, prop_y2=0.1):
+        """edge_sponge.h:31-72."""
+        rd, u, v, w, T, trc = _arrays(coupler)
+        _handle(coupler, need_halos=False).edge_sponge(rd, u, v, w, T, trc, self.column, prop_x1, prop_x2, prop_y1,
+                                                       prop_y2, self._fields(coupler))
 
 
 def register_immersed_halos(coupler, case, **kw):

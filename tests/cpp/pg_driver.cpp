@@ -1,18 +1,22 @@
 // Driver of the C++ drop-in pressure-gradient forcings
-// (porturb_b200/cpp/uniform_pg_wind_forcing.h) on the single-rank stand-in
-// coupler of oracle/ref_shim, with no immersed arrays registered: ncalls of
-// uniform_pg_wind_forcing with +0.25 m/s added to uvel after each, then one
-// uniform_pg_wind_forcing_height.
+// (porturb_b200/cpp/uniform_pg_wind_forcing.h) and edge sponge
+// (porturb_b200/cpp/edge_sponge.h) on the single-rank stand-in coupler of
+// oracle/ref_shim, with no immersed arrays registered: the edge sponge
+// records its column profile, then ncalls of uniform_pg_wind_forcing with
+// +0.25 m/s added to uvel after each, then one
+// uniform_pg_wind_forcing_height, then the edge sponge (city.cpp:137).
 //
 // Usage: pg_driver <input.bin> <output.bin>
 //   input : int32 nx, ny, nz, ncalls, update_cycles; float64 xlen, ylen, zlen,
 //           dt, tau, height, u0, v0, tau_height; float64 uvel N, vvel N
 //   output: float64 uvel N, vvel N, then counter, u0, v0, u, v of the
-//           coupler options after the uniform forcing calls
+//           coupler options after the uniform forcing calls, then the five
+//           state fields after the edge sponge (5 N)
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
 
+#include "edge_sponge.h"
 #include "uniform_pg_wind_forcing.h"
 
 template <class T>
@@ -42,6 +46,8 @@ int main(int argc, char **argv) {
   for (auto nm : {"density_dry", "uvel", "vvel", "wvel", "temp"}) dm.register_and_allocate<real>(nm, "", {nz, ny, nx});
   std::copy(u.begin(), u.end(), dm.get<real, 3>("uvel").data());
   std::copy(v.begin(), v.end(), dm.get<real, 3>("vvel").data());
+  custom_modules::EdgeSponge edge_sponge;
+  edge_sponge.set_column(coupler);
   for (int c = 0; c < ncalls; c++) {
     modules::uniform_pg_wind_forcing(coupler, g[3], g[4], size_t(cycles));
     auto uu = dm.get<real, 3>("uvel");
@@ -56,6 +62,8 @@ int main(int argc, char **argv) {
   fwrite(dm.get<real, 3>("uvel").data(), sizeof(double), N, o);
   fwrite(dm.get<real, 3>("vvel").data(), sizeof(double), N, o);
   fwrite(st, sizeof(double), 5, o);
+  edge_sponge.apply(coupler, 0.2, 0.1, 0.15, 0.25);
+  for (auto nm : {"density_dry", "uvel", "vvel", "wvel", "temp"}) fwrite(dm.get<real, 3>(nm).data(), sizeof(double), N, o);
   fclose(o);
   modules::pu_physics_module_finalize(coupler);
   printf("pg driver ok\n");

@@ -117,10 +117,10 @@ def test_physics_dropin_chain_matches_python_front_end(tmp_path):
 
 @pytest.mark.gpu
 def test_pg_forcing_dropin_matches_python_front_end(tmp_path):
-    """The drop-in uniform_pg_wind_forcing / _height headers on a coupler
-    with no immersed arrays give the same arrays and carried options as the
-    Python module API."""
-    from porturb_b200 import case_coupler, cases, uniform_pg_wind_forcing, uniform_pg_wind_forcing_height
+    """The drop-in uniform_pg_wind_forcing / _height and edge-sponge headers on
+    a coupler with no immersed arrays give the same arrays and carried options
+    as the Python module API."""
+    from porturb_b200 import EdgeSponge, case_coupler, cases, uniform_pg_wind_forcing, uniform_pg_wind_forcing_height
     build_driver()
     exe = os.path.join(ROOT, "tests", "cpp", "_build", "pg_driver")
     case = cases.abl_neutral(nx=24, ny=20, nz=16)
@@ -142,6 +142,11 @@ def test_pg_forcing_dropin_matches_python_front_end(tmp_path):
     c = case_coupler(case)
     c.get("uvel")[...] = u
     c.get("vvel")[...] = v
+    c.get("density_dry")[...] = 0.0   # as the driver's freshly allocated arrays
+    c.get("wvel")[...] = 0.0
+    c.get("temp")[...] = 0.0
+    es = EdgeSponge()
+    es.set_column(c)
     for _ in range(ncalls):
         uniform_pg_wind_forcing(c, dt, tau, cycles)
         c.get("uvel")[...] += 0.25
@@ -149,5 +154,8 @@ def test_pg_forcing_dropin_matches_python_front_end(tmp_path):
     uniform_pg_wind_forcing_height(c, dt, height, u0, v0, tau_h)
     assert np.array_equal(out[:n].reshape(u.shape), c.get("uvel"))
     assert np.array_equal(out[n:2 * n].reshape(v.shape), c.get("vvel"))
-    assert np.array_equal(out[2 * n:], np.array(st, np.float64))
+    assert np.array_equal(out[2 * n:2 * n + 5], np.array(st, np.float64))
     assert not np.array_equal(c.get("vvel"), v)
+    es.apply(c, 0.2, 0.1, 0.15, 0.25)
+    for q, nm in enumerate(("density_dry", "uvel", "vvel", "wvel", "temp")):
+        assert np.array_equal(out[2 * n + 5 + q * n:2 * n + 5 + (q + 1) * n].reshape(u.shape), c.get(nm)), nm

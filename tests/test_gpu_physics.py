@@ -292,3 +292,52 @@ def test_time_averager_module_api_on_a_coupler(oracle_lib, gpu_lib):
     ta.reset(c)
     assert c.get_option("time_averager_etime") == 0.0
     assert not c.get("avg_u").any() and c.get("long_avg_u").any()
+
+
+@pytest.mark.parametrize("device", [False, True])
+def test_edge_sponge_matches_oracle(oracle_lib, gpu_lib, device):
+    """pu_edge_sponge_set_column / _apply against the oracle (itself equal to
+    the reference's header): column means within 1e-14 of each field's
+    magnitude (each value scaled by 1/(nx ny) before a compensated parallel
+    sum, against the reference's sequential sum divided once), relaxed
+    fields within the _check bound."""
+    case, halos, _ = _case("plain")
+    orc = pyphysics.Physics(case, "orc", halos)
+    ph = Physics.from_case(case, halos=halos)
+    st0 = pyphysics.state_of(case, seed=23)
+    want_col = orc.edge_sponge_set_column(st0)
+    trc0 = [np.ascontiguousarray(st0["tracers"][i]) for i in range(st0["tracers"].shape[0])]
+    col = ph.edge_sponge_set_column(st0["rho_d"], st0["uvel"], st0["vvel"], st0["wvel"], st0["temp"], trc0)
+    mags = np.array([np.abs(st0[k]).max() for k in ("rho_d", "uvel", "vvel", "wvel", "temp")])
+    assert np.all(np.abs(col - want_col) <= 1e-14 * mags[:, None])
+    st = pyphysics.state_of(case, seed=24)
+    for props in ((0.1, 0.1, 0.1, 0.1), (0.3, 0.0, 0.0, 0.25)):
+        want = orc.edge_sponge_apply(st, want_col, *props)
+        got = _run_gpu(ph, "edge_sponge", st, (want_col,) + props, device)
+        _check("edge_sponge/%s" % (props,), got, want, st)
+    ph.close()
+
+
+def test_edge_sponge_module_api_on_a_coupler(oracle_lib, gpu_lib):
+    """EdgeSponge.set_column / apply on a Coupler, as the urban driver calls
+    them (city.cpp:97, 137)."""
+    from porturb_b200 import EdgeSponge, case_coupler
+    case, halos, _ = _case("plain", nx=36, ny=16, nz=18)
+    c = case_coupler(case)
+    st = pyphysics.state_of(case, seed=25)
+    for k, name in (("rho_d", "density_dry"), ("uvel", "uvel"), ("vvel", "vvel"), ("wvel", "wvel"), ("temp", "temp")):
+        c.get(name)[...] = st[k]
+    es = EdgeSponge()
+    es.set_column(c)
+    orc = pyphysics.Physics(case, "orc", halos)
+    col = orc.edge_sponge_set_column(st)
+    mags = np.array([np.abs(st[k]).max() for k in ("rho_d", "uvel", "vvel", "wvel", "temp")])
+    assert np.all(np.abs(es.column - col) <= 1e-14 * mags[:, None])
+    st2 = pyphysics.state_of(case, seed=26)
+    for k, name in (("rho_d", "density_dry"), ("uvel", "uvel"), ("vvel", "vvel"), ("wvel", "wvel"), ("temp", "temp")):
+        c.get(name)[...] = st2[k]
+    es.apply(c, 0.01, 0.01, 0.01, 0.01)
+    want = orc.edge_sponge_apply(st2, es.column, 0.01, 0.01, 0.01, 0.01)
+    got = dict(want, rho_d=c.get("density_dry"), uvel=c.get("uvel"), vvel=c.get("vvel"), wvel=c.get("wvel"),
+               temp=c.get("temp"))
+    _check("coupler_edge_sponge", got, want, st2)

@@ -185,3 +185,23 @@ def test_time_averager_matches_reference_across_calls(oracle_lib):
         st["uvel"] = st["uvel"] + 0.2 * rng.standard_normal(st["uvel"].shape)
         st["wvel"] = st["wvel"] + 0.1 * rng.standard_normal(st["wvel"].shape)
     assert np.abs(ao[4]).max() > 0 and np.abs(ao[10] - st["uvel"]).max() > 0
+
+
+@pytest.mark.parametrize("props", [(0.1, 0.1, 0.1, 0.1), (0.01, 0.01, 0.01, 0.01), (0.3, 0.0, 0.0, 0.25),
+                                   (0.0, 0.5, 0.2, 0.0)])
+def test_edge_sponge_matches_reference(oracle_lib, props):
+    """custom_modules::EdgeSponge: the column profile recorded from one state
+    and the edge relaxation of a later one, bit for bit (corner cells take
+    both zones in the reference's order)."""
+    case, halos, _ = _case("plain")
+    orc = pyphysics.Physics(case, "orc", halos)
+    ref = pyphysics.Physics(case, "ref", halos)
+    st0 = pyphysics.state_of(case, seed=21)
+    co, cr = orc.edge_sponge_set_column(st0), ref.edge_sponge_set_column(st0)
+    assert np.array_equal(co, cr)
+    st = pyphysics.state_of(case, seed=22)
+    a = orc.edge_sponge_apply(st, co, *props)
+    b = ref.edge_sponge_apply(st, cr, *props)
+    for key in a:
+        assert np.array_equal(a[key], b[key]), key
+    assert not np.array_equal(a["uvel"], st["uvel"])

@@ -510,5 +510,7 @@ def assign_coupler_state(c: Coupler, case, perturbed=True):
     rd, u, v, w, T, trc = case.coupler_arrays(perturbed=perturbed)
     for nm, a in zip(("density_dry", "uvel", "vvel", "wvel", "temp"), (rd, u, v, w, T)):
         _copy(c.get(nm), a)
-    for t, nm in enumerate(c.get_tracer_names()):
-        _copy(c.get(nm), trc[t])
+    # By name: tracers that modules registered beside the case's own (the LES
+    # closure's TKE) keep what those modules set.
+    for t, tr in enumerate(case.tracers):
+        _copy(c.get(tr.name), trc[t])

@@ -7,7 +7,8 @@
 Plain mode advances the FP32 (or --precision f64) dycore; --learned first
 harvests stencils from the initial state, trains the network on the GPU and
 then advances with learned weights; --modules times the physics modules
-(LES closure, sponge, geostrophic forcing, surface fluxes) instead.  Prints
+(LES closure, sponge, geostrophic forcing, surface fluxes) instead; --driver
+runs the reference driver's whole chain of modules per dt_phys.  Prints
 one JSON line with the per-kernel CUDA-event times and, in learned mode, the
 fallback fraction.
 """
@@ -62,6 +63,58 @@ def run_modules(case, a):
     return out
 
 
+def run_driver(case, a):
+    """The reference driver's loop with this package's modules on device
+    coupler arrays: per call of dt_phys = 10 dycore steps, the boundary-layer
+    chain (abl_neutral.cpp:93-108: geostrophic forcing, dycore, sponge,
+    surface fluxes, LES closure, time averager) or the urban one
+    (city.cpp:137-142: edge sponge, dycore, sponge, surface fluxes, LES
+    closure, time averager).  CUDA-event time of `steps` calls after one."""
+    import torch
+    from . import (Dynamics_Euler_Stratified_WenoFV, EdgeSponge, LES_Closure, Time_Averager, apply_surface_fluxes,
+                   assign_coupler_state, case_coupler, geostrophic_wind_forcing, sponge_layer)
+    from .physics import register_immersed_halos
+    c = case_coupler(case, device="cuda:%d" % torch.cuda.current_device())
+    register_immersed_halos(c, case)
+    les, dyn, tavg, edge = LES_Closure(), Dynamics_Euler_Stratified_WenoFV(precision=a.precision), Time_Averager(), \
+        EdgeSponge()
+    les.init(c)
+    dyn.init(c)
+    tavg.init(c)
+    urban = a.case == "urban_canopy"
+    if urban:
+        edge.set_column(c)
+    assign_coupler_state(c, case, perturbed=True)
+    dt = 10 * dyn.compute_time_step(c)
+    sub = []
+
+    def call():
+        if urban:
+            edge.apply(c, 0.01, 0.01, 0.01, 0.01)
+        else:
+            geostrophic_wind_forcing(c, dt, 43.289340204, 10.0, 0.0)
+        sub.append(dyn.time_step(c, dt))
+        sponge_layer(c, dt, dt if urban else dt * 100, 0.02 if urban else 0.1)
+        apply_surface_fluxes(c, dt)
+        les.apply(c, dt)
+        tavg.accumulate(c, dt)
+        c.set_option("elapsed_time", c.get_option("elapsed_time") + dt)
+
+    call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        call()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    return {"case": a.case, "grid": [a.nx, a.ny, a.nz], "driver": "urban (city.cpp)" if urban else
+            "boundary layer (abl_neutral.cpp)", "calls": a.steps, "dycore_steps_per_call": sub[-1], "ms_per_call": ms,
+            "cell_steps_per_s": case.ncells * sub[-1] / (ms / 1e3),
+            "note": "cell-steps/s of the whole driver step: the dycore's 10 steps and the modules beside it"}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=sorted(CASES))
@@ -77,6 +130,9 @@ def main(argv=None):
     ap.add_argument("--harvest", type=int, default=1 << 18)
     ap.add_argument("--train-steps", type=int, default=300)
     ap.add_argument("--threshold", type=float, default=0.5)
+    ap.add_argument("--driver", action="store_true",
+                    help="run the reference driver's module chain per dt_phys (boundary layer or urban) on device "
+                         "coupler arrays")
     ap.add_argument("--modules", action="store_true",
                     help="time the physics modules (LES closure, sponge, geostrophic forcing, surface fluxes) "
                          "on the case's coupler arrays instead of dycore steps")
@@ -85,6 +141,9 @@ def main(argv=None):
     case = CASES[a.case](a)
     if a.modules:
         print(json.dumps(run_modules(case, a)), flush=True)
+        return
+    if a.driver:
+        print(json.dumps(run_driver(case, a)), flush=True)
         return
     g = Dycore.from_case(case, precision=a.precision)
     rd, u, v, w, T, trc = [np.ascontiguousarray(x) for x in case.coupler_arrays(perturbed=True)]

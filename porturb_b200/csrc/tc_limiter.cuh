@@ -210,7 +210,8 @@ __device__ __forceinline__ float edge_from_lin(const float (&lin)[5], float s4, 
   float w[5];
 #pragma unroll
   for (int k = 0; k < 5; k++) w[k] = float(LEFT ? IDEAL_L[k] : IDEAL_R[k]) * rk[k];
-  convexify5(w);
+  normalize5(w);
+  float r = 1.f;
   if (do_map) {
 #pragma unroll
     for (int k = 0; k < 5; k++) {
@@ -219,12 +220,12 @@ __device__ __forceinline__ float edge_from_lin(const float (&lin)[5], float s4, 
       const float u = fmaf(-w[k], w[k], w[k]), u3 = u * u * u;
       w[k] = fmaf(t6 * t, fast_rcp(fmaf(2000.f, u3, t6)), dk);
     }
-    convexify5(w);
+    r = fast_rcp(w[0] + w[1] + w[2] + w[3] + w[4]);
   }
   float acc = 0.f;
 #pragma unroll
   for (int k = 0; k < 5; k++) acc = fmaf(w[k], lin[k], acc);
-  return s4 + acc;
+  return fmaf(acc, r, s4);
 }
 
 // The nonlinear rest of the limiter from one TMEM row (z's and lin's).

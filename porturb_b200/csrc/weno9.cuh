@@ -10,11 +10,13 @@
 //      apply map_rs (k=6, m=3, s=2000; WenoLimiter.h:75-82) and normalise
 //      again, then the weighted sub-stencil edge values (WenoLimiter.h:382-426).
 // The arithmetic is rearranged (see gen_weno9.py): stencil differences, an
-// LDL^T form of TV, edge values as s_4 plus linear forms, and one reciprocal
-// shared by both edges for each 1/(TV_k^2+1e-20).  In FP32 the reciprocals
-// use rcp.approx.ftz; every operand is a normal number there: TV_k^2+1e-20 >=
-// 1e-20, the normalisation sums exceed 1e-20 on the branch that divides, and
-// the map_rs denominator is at least ideal_k^6 > 2e-13.
+// LDL^T form of TV, edge values as s_4 plus linear forms, one reciprocal
+// shared by both edges for each 1/(TV_k^2+1e-20), and the normalisation
+// after map_rs applied once to the weighted sum instead of to each weight.
+// In FP32 the reciprocals use rcp.approx.ftz; every operand is a normal
+// number there: TV_k^2+1e-20 >= 1e-20, the normalisation sums exceed 1e-20
+// on the branch that divides (the weight sums always), and the map_rs
+// denominator is at least ideal_k^6 > 2e-13.
 #pragma once
 
 #include "weno9_tables.cuh"
@@ -41,14 +43,32 @@ __device__ __forceinline__ void convexify5(R (&w)[5]) {
   }
 }
 
+// convexify of the ideal-weighted reciprocals, whose sum always passes the
+// reference's test (> 1e-20): rk_k = 1/(TV_k^2 + 1e-20) is at least
+// 1/(1 + 1e-20) when the TV were normalised (each is then at most 1 up to a
+// rounding) and far above 1 when they were not (sum of TV <= 1e-20), so the
+// sum is at least the sum of the ideal weights, 1.
+template <class R>
+__device__ __forceinline__ void normalize5(R (&w)[5]) {
+  const R r = fast_rcp(w[0] + w[1] + w[2] + w[3] + w[4]);
+#pragma unroll
+  for (int k = 0; k < 5; k++) w[k] *= r;
+}
+
 // One edge: weights from the shared reciprocals rk = 1/(TV_k^2 + 1e-20).
+// After map_rs the second convexify is folded into the edge value: the
+// weighted sum of the sub-stencil edges is taken with the mapped weights
+// m_k and scaled once by 1/sum(m) (the reference scales each weight).  The
+// test of that convexify always passes: each m_k >= min(w_k, ideal_k) >= 0,
+// and the k with w_k >= 1/5 gives m_k >= min_k ideal_k = 1/126.
 template <class R, bool LEFT>
 __device__ __forceinline__ R weno9_edge(const R (&d)[8], R s4, const R (&rk)[5], bool do_map) {
   using namespace pu_weno9;
   R w[5];
 #pragma unroll
   for (int k = 0; k < 5; k++) w[k] = R(LEFT ? IDEAL_L[k] : IDEAL_R[k]) * rk[k];
-  convexify5(w);
+  normalize5(w);
+  R r = R(1);
   if (do_map) {
 #pragma unroll
     for (int k = 0; k < 5; k++) {
@@ -61,7 +81,7 @@ __device__ __forceinline__ R weno9_edge(const R (&d)[8], R s4, const R (&rk)[5],
       R den = fma(R(2000.), u3, t6);
       w[k] = fma(t6 * t, fast_rcp(den), dk);
     }
-    convexify5(w);
+    r = fast_rcp(w[0] + w[1] + w[2] + w[3] + w[4]);
   }
   R acc = R(0);
 #pragma unroll
@@ -71,7 +91,7 @@ __device__ __forceinline__ R weno9_edge(const R (&d)[8], R s4, const R (&rk)[5],
     for (int m = 1; m < 4; m++) lin = fma(R(LEFT ? LIN_L[k][m] : LIN_R[k][m]), d[k + m], lin);
     acc = fma(w[k], lin, acc);
   }
-  return s4 + acc;
+  return fma(acc, r, s4);
 }
 
 template <class R>
@@ -131,13 +151,21 @@ __device__ __forceinline__ void convexify5x2(float2 (&w)[5]) {
   for (int k = 0; k < 5; k++) w[k] = mul2(w[k], r);
 }
 
+__device__ __forceinline__ void normalize5x2(float2 (&w)[5]) {
+  const float2 tot = add2(add2(add2(add2(w[0], w[1]), w[2]), w[3]), w[4]);
+  const float2 r = rcp2(tot);
+#pragma unroll
+  for (int k = 0; k < 5; k++) w[k] = mul2(w[k], r);
+}
+
 template <bool LEFT>
 __device__ __forceinline__ float2 weno9_edge2(const float2 (&d)[8], float2 s4, const float2 (&rk)[5], bool2 do_map) {
   using namespace pu_weno9;
   float2 w[5];
 #pragma unroll
   for (int k = 0; k < 5; k++) w[k] = mul2(f2(float(LEFT ? IDEAL_L[k] : IDEAL_R[k])), rk[k]);
-  convexify5x2(w);
+  normalize5x2(w);
+  float2 r = f2(1.f);
   if (do_map.x || do_map.y) {
     float2 m[5];
 #pragma unroll
@@ -151,7 +179,8 @@ __device__ __forceinline__ float2 weno9_edge2(const float2 (&d)[8], float2 s4, c
       const float2 den = fma2(f2(2000.f), u3, t6);
       m[k] = fma2(mul2(t6, t), rcp2(den), dk);
     }
-    convexify5x2(m);
+    const float2 tot = add2(add2(add2(add2(m[0], m[1]), m[2]), m[3]), m[4]);
+    r = make_float2(do_map.x ? fast_rcp(tot.x) : 1.f, do_map.y ? fast_rcp(tot.y) : 1.f);
 #pragma unroll
     for (int k = 0; k < 5; k++) w[k] = make_float2(do_map.x ? m[k].x : w[k].x, do_map.y ? m[k].y : w[k].y);
   }
@@ -163,7 +192,7 @@ __device__ __forceinline__ float2 weno9_edge2(const float2 (&d)[8], float2 s4, c
     for (int m = 1; m < 4; m++) lin = fma2(f2(float(LEFT ? LIN_L[k][m] : LIN_R[k][m])), d[k + m], lin);
     acc = fma2(w[k], lin, acc);
   }
-  return add2(s4, acc);
+  return fma2(acc, r, s4);
 }
 
 __device__ __forceinline__ void weno9_edges2(const float2 (&s)[9], float2 &qL, float2 &qR, bool2 do_map, bool2 imm_L,

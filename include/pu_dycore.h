@@ -291,7 +291,11 @@ int pu_dycore_time_step_noalloc(const pu_config *cfg, const double *hy_dens_cell
  * two-stencil form of the x/y kernel (both give the same bits); 2, 3: the
  * linear forms on the tensor cores (tcgen05.mma kind::tf32, three-term split,
  * A in shared memory / in tensor memory; the two give the same bits and
- * agree with the FP32 forms to rounding; not used by the dycore kernels).
+ * agree with the FP32 forms to rounding; not used by the dycore kernels);
+ * 4: the packed one-edge form the x/y kernel uses for the halo cells that
+ * close a tile's rows, on pairs (2i, 2i+1): the right edge of stencil 2i and
+ * the left edge of stencil 2i+1, each the same bits as variants 0 and 1 (the
+ * pair's other two outputs are NaN).
  * Host or device arrays (mem); synchronous, on the current device. */
 int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long long n, int variant, float *qL,
                        float *qR, int mem);

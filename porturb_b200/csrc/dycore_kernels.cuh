@@ -306,33 +306,66 @@ __device__ __forceinline__ int recon_learned(const Grid<float> &G, uint32_t *sW,
   return nq;
 }
 
-// Plain reconstruction of `total` stencils, two per thread and iteration
-// (stencils it and it+NT) with the packed FP32 limiter; per stencil the
-// result is bit-identical to weno9_edges.  Used when every stencil takes the
-// nonlinear limiter (weno_all).
-template <int NT, class Load, class Store>
-__device__ __forceinline__ void recon_packed(int total, Load load, Store store) {
-  for (int it = threadIdx.x; it < total; it += 2 * NT) {
+// Reconstruction of a tile's lines of faces with the packed FP32 limiter
+// (weno_all).  There are F x LINES lines of W+2 cells (positions 0..W+1,
+// cells -1..W); the faces of a line read both edges of the W inner cells, the
+// right edge of position 0 and the left edge of position W+1.  Inner cells go
+// two per thread and iteration (weno9_edges2); the two halo cells of a line
+// go together through the one-edge form (weno9_outer_edges2), which skips the
+// two edges nobody reads.  Per stencil and edge the bits are those of
+// weno9_edges.  POS_MAJOR: consecutive threads take consecutive lines at one
+// position (y), else consecutive positions of one line (x).
+// load(f, line, pos, s, imm, any10), store(f, line, pos, qL, qR),
+// store_outer(f, line, qR of position 0, qL of position W+1).
+template <int NT, int F, int LINES, int W, bool POS_MAJOR, class Load, class Store, class StoreOuter>
+__device__ __forceinline__ void recon_packed_lines(Load load, Store store, StoreOuter store_outer) {
+  constexpr int N_IN = F * LINES * W;
+  auto coords = [](int it, int &f, int &line, int &pos) {
+    f = it / (LINES * W);
+    const int q = it % (LINES * W);
+    line = POS_MAJOR ? q % LINES : q / W;
+    pos = (POS_MAJOR ? q / LINES : q % W) + 1;
+  };
+  for (int it = threadIdx.x; it < N_IN; it += 2 * NT) {
     const int it2 = it + NT;
-    const bool two = it2 < total;
+    const bool two = it2 < N_IN;
+    int fa, la, pa, fb, lb, pb;
+    coords(it, fa, la, pa);
     float a[9], b[9];
     unsigned ia, ib;
     bool xa, xb;
-    load(it, a, ia, xa);
-    if (two) load(it2, b, ib, xb);
-    else {
+    load(fa, la, pa, a, ia, xa);
+    if (two) {
+      coords(it2, fb, lb, pb);
+      load(fb, lb, pb, b, ib, xb);
+    } else {
 #pragma unroll
       for (int m = 0; m < 9; m++) b[m] = a[m];
       ib = ia;
       xb = xa;
+      fb = fa, lb = la, pb = pa;
     }
     float2 s2[9], qL, qR;
 #pragma unroll
     for (int m = 0; m < 9; m++) s2[m] = make_float2(a[m], b[m]);
     weno9_edges2(s2, qL, qR, bool2{!xa, !xb}, bool2{((ia >> 3) & 1u) != 0, ((ib >> 3) & 1u) != 0},
                  bool2{((ia >> 5) & 1u) != 0, ((ib >> 5) & 1u) != 0});
-    store(it, qL.x, qR.x);
-    if (two) store(it2, qL.y, qR.y);
+    store(fa, la, pa, qL.x, qR.x);
+    if (two) store(fb, lb, pb, qL.y, qR.y);
+  }
+  for (int p = threadIdx.x; p < F * LINES; p += NT) {
+    const int f = p / LINES, line = p % LINES;
+    float a[9], b[9];
+    unsigned ia, ib;
+    bool xa, xb;
+    load(f, line, 0, a, ia, xa);
+    load(f, line, W + 1, b, ib, xb);
+    float2 s2[9];
+#pragma unroll
+    for (int m = 0; m < 9; m++) s2[m] = make_float2(a[m], b[m]);
+    const float2 q = weno9_outer_edges2(s2, bool2{!xa, !xb}, bool2{((ia >> 3) & 1u) != 0, ((ib >> 3) & 1u) != 0},
+                                        bool2{((ia >> 5) & 1u) != 0, ((ib >> 5) & 1u) != 0});
+    store_outer(f, line, q.x, q.y);
   }
 }
 
@@ -393,9 +426,8 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
   }
   __syncthreads();
 
-  // 2. x edges of cells -1..TX of every tile row.
-  auto load_x = [&](int it, R (&s)[9], unsigned &imm, bool &any10) {
-    const int f = it / Sh::EXN, rem = it % Sh::EXN, r = rem / (TX + 2), c = rem % (TX + 2);
+  // 2. x edges of cells -1..TX of every tile row (position c = cell + 1).
+  auto load_xc = [&](int f, int r, int c, R (&s)[9], unsigned &imm, bool &any10) {
     const R *row = H + (f * HY + 5 + r) * HX + c;
 #pragma unroll
     for (int m = 0; m < 9; m++) s[m] = row[m];
@@ -409,6 +441,14 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
       if (f == iV || f == iW || f == iP) der0_modify(s, imm);
     }
   };
+  auto store_xc = [&](int f, int r, int c, R qL, R qR) {
+    EL[f * EN + r * (TX + 2) + c] = qL;
+    ER[f * EN + r * (TX + 2) + c] = qR;
+  };
+  auto load_x = [&](int it, R (&s)[9], unsigned &imm, bool &any10) {
+    const int f = it / Sh::EXN, rem = it % Sh::EXN;
+    load_xc(f, rem / (TX + 2), rem % (TX + 2), s, imm, any10);
+  };
   auto store_x = [&](int it, R qL, R qR) {
     const int f = it / Sh::EXN, rem = it % Sh::EXN;
     EL[f * EN + rem] = qL;
@@ -418,7 +458,11 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
   bool packed = false;
   if constexpr (std::is_same<R, float>::value && PU_PACKED_LIMITER && !LEARNED) {
     packed = G.weno_all != 0;
-    if (packed) recon_packed<NT>(F * Sh::EXN, load_x, store_x);
+    if (packed)
+      recon_packed_lines<NT, F, TY, TX, false>(load_xc, store_xc, [&](int f, int r, R qR0, R qL1) {
+        ER[f * EN + r * (TX + 2)] = qR0;
+        EL[f * EN + r * (TX + 2) + TX + 1] = qL1;
+      });
   }
   if constexpr (LEARNED) {
     n_fb += recon_learned<NT>(G, sW, queue, qn, F * Sh::EXN, load_x, store_x);
@@ -470,8 +514,7 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
 
   if (!sim2d) {
     // 5. y edges of cells -1..TY of every tile column.
-    auto load_y = [&](int it, R (&s)[9], unsigned &imm, bool &any10) {
-      const int f = it / Sh::EYN, rem = it % Sh::EYN, rr = rem / TX, cc = rem % TX;
+    auto load_yc = [&](int f, int cc, int rr, R (&s)[9], unsigned &imm, bool &any10) {
       const R *col = H + (f * HY + rr) * HX + 5 + cc;
 #pragma unroll
       for (int m = 0; m < 9; m++) s[m] = col[m * HX];
@@ -485,6 +528,10 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
         if (f == iU || f == iW || f == iP) der0_modify(s, imm);
       }
     };
+    auto load_y = [&](int it, R (&s)[9], unsigned &imm, bool &any10) {
+      const int f = it / Sh::EYN, rem = it % Sh::EYN;
+      load_yc(f, rem % TX, rem / TX, s, imm, any10);
+    };
     auto store_y = [&](int it, R qL, R qR) {
       const int f = it / Sh::EYN, rem = it % Sh::EYN;
       EL[f * EN + rem] = qL;
@@ -494,7 +541,17 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
       __syncthreads();   // step 4 has read the flux buffer that holds the queue
       n_fb += recon_learned<NT>(G, sW, queue, qn + 1, F * Sh::EYN, load_y, store_y);
     } else if (packed) {
-      if constexpr (std::is_same<R, float>::value) recon_packed<NT>(F * Sh::EYN, load_y, store_y);
+      if constexpr (std::is_same<R, float>::value)
+        recon_packed_lines<NT, F, TX, TY, true>(
+            load_yc,
+            [&](int f, int cc, int rr, R qL, R qR) {
+              EL[f * EN + rr * TX + cc] = qL;
+              ER[f * EN + rr * TX + cc] = qR;
+            },
+            [&](int f, int cc, R qR0, R qL1) {
+              ER[f * EN + cc] = qR0;
+              EL[f * EN + (TY + 1) * TX + cc] = qL1;
+            });
     } else {
       for (int it = tid; it < F * Sh::EYN; it += NT) {
         R s[9];

@@ -335,7 +335,9 @@ int local_exchange(std::vector<pu::ImplBase *> &t, int which, bool x, bool y) {
 namespace {
 
 // The FP32 limiter on a batch of stencils: VARIANT 0 the scalar form, 1 the
-// packed form (stencils 2i and 2i+1 in one thread).
+// packed form (stencils 2i and 2i+1 in one thread), 4 the packed one-edge
+// form (the right edge of stencil 2i and the left edge of stencil 2i+1; the
+// other two outputs of the pair are NaN).
 template <int VARIANT>
 __global__ void k_weno9_eval(const float *__restrict__ s, const unsigned char *__restrict__ flags, long long n,
                              float *__restrict__ qL, float *__restrict__ qR) {
@@ -359,13 +361,25 @@ __global__ void k_weno9_eval(const float *__restrict__ s, const unsigned char *_
     for (int m = 0; m < 9; m++) st[m] = make_float2(s[a * 9 + m], s[bb * 9 + m]);
     const unsigned fa = flags ? flags[a] : 1u, fb = flags ? flags[bb] : 1u;
     float2 L, R;
-    pu::weno9_edges2(st, L, R, pu::bool2{(fa & 1u) != 0, (fb & 1u) != 0}, pu::bool2{(fa & 2u) != 0, (fb & 2u) != 0},
-                     pu::bool2{(fa & 4u) != 0, (fb & 4u) != 0});
-    qL[a] = L.x;
-    qR[a] = R.x;
-    if (b < n) {
-      qL[b] = L.y;
-      qR[b] = R.y;
+    const pu::bool2 mp{(fa & 1u) != 0, (fb & 1u) != 0}, il{(fa & 2u) != 0, (fb & 2u) != 0},
+        ir{(fa & 4u) != 0, (fb & 4u) != 0};
+    if constexpr (VARIANT == 1) {
+      float2 L, R;
+      pu::weno9_edges2(st, L, R, mp, il, ir);
+      qL[a] = L.x;
+      qR[a] = R.x;
+      if (b < n) {
+        qL[b] = L.y;
+        qR[b] = R.y;
+      }
+    } else {
+      const float2 q = pu::weno9_outer_edges2(st, mp, il, ir);
+      qL[a] = __int_as_float(0x7fc00000);
+      qR[a] = q.x;
+      if (b < n) {
+        qL[b] = q.y;
+        qR[b] = __int_as_float(0x7fc00000);
+      }
     }
   }
 }
@@ -888,7 +902,7 @@ int pu_dycore_group_time_step(pu_dycore *const *hs, int n, pu_state_view *views,
 
 int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long long n, int variant, float *qL,
                        float *qR, int mem) {
-  if (!stencils || !qL || !qR || n < 0 || variant < 0 || variant > 3) return fail(PU_ERR_INVALID, "bad argument");
+  if (!stencils || !qL || !qR || n < 0 || variant < 0 || variant > 4) return fail(PU_ERR_INVALID, "bad argument");
   if (n == 0) return PU_OK;
   const bool dev = pu::resolve_mem(mem, stencils) == PU_MEM_DEVICE;
   float *ds = const_cast<float *>(stencils), *dl = qL, *dr = qR;
@@ -906,6 +920,7 @@ int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long l
   int *derr = nullptr;
   if (variant == 0) k_weno9_eval<0><<<blocks, 256>>>(ds, df, n, dl, dr);
   else if (variant == 1) k_weno9_eval<1><<<blocks, 256>>>(ds, df, n, dl, dr);
+  else if (variant == 4) k_weno9_eval<4><<<blocks, 256>>>(ds, df, n, dl, dr);
   else {
     if (cudaMalloc(&derr, sizeof(int)) == cudaSuccess) {
       cudaMemset(derr, 0, sizeof(int));

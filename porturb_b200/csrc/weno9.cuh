@@ -158,19 +158,33 @@ __device__ __forceinline__ void normalize5x2(float2 (&w)[5]) {
   for (int k = 0; k < 5; k++) w[k] = mul2(w[k], r);
 }
 
-template <bool LEFT>
-__device__ __forceinline__ float2 weno9_edge2(const float2 (&d)[8], float2 s4, const float2 (&rk)[5], bool2 do_map) {
+// Per-lane constants of one edge: SIDE 0 the left edge in both lanes, 1 the
+// right edge in both, 2 the right edge in lane x and the left edge in lane y.
+template <int SIDE>
+__device__ __forceinline__ float2 ideal2(int k) {
   using namespace pu_weno9;
+  return SIDE == 0 ? f2(float(IDEAL_L[k])) : SIDE == 1 ? f2(float(IDEAL_R[k]))
+                                                       : make_float2(float(IDEAL_R[k]), float(IDEAL_L[k]));
+}
+template <int SIDE>
+__device__ __forceinline__ float2 lin2(int k, int m) {
+  using namespace pu_weno9;
+  return SIDE == 0 ? f2(float(LIN_L[k][m])) : SIDE == 1 ? f2(float(LIN_R[k][m]))
+                                                        : make_float2(float(LIN_R[k][m]), float(LIN_L[k][m]));
+}
+
+template <int SIDE>
+__device__ __forceinline__ float2 weno9_edge2(const float2 (&d)[8], float2 s4, const float2 (&rk)[5], bool2 do_map) {
   float2 w[5];
 #pragma unroll
-  for (int k = 0; k < 5; k++) w[k] = mul2(f2(float(LEFT ? IDEAL_L[k] : IDEAL_R[k])), rk[k]);
+  for (int k = 0; k < 5; k++) w[k] = mul2(ideal2<SIDE>(k), rk[k]);
   normalize5x2(w);
   float2 r = f2(1.f);
   if (do_map.x || do_map.y) {
     float2 m[5];
 #pragma unroll
     for (int k = 0; k < 5; k++) {
-      const float2 dk = f2(float(LEFT ? IDEAL_L[k] : IDEAL_R[k]));
+      const float2 dk = ideal2<SIDE>(k);
       const float2 t = sub2(w[k], dk);
       const float2 t2 = mul2(t, t);
       const float2 t6 = mul2(mul2(t2, t2), t2);
@@ -187,18 +201,19 @@ __device__ __forceinline__ float2 weno9_edge2(const float2 (&d)[8], float2 s4, c
   float2 acc = f2(0.f);
 #pragma unroll
   for (int k = 0; k < 5; k++) {
-    float2 lin = mul2(f2(float(LEFT ? LIN_L[k][0] : LIN_R[k][0])), d[k]);
+    float2 lin = mul2(lin2<SIDE>(k, 0), d[k]);
 #pragma unroll
-    for (int m = 1; m < 4; m++) lin = fma2(f2(float(LEFT ? LIN_L[k][m] : LIN_R[k][m])), d[k + m], lin);
+    for (int m = 1; m < 4; m++) lin = fma2(lin2<SIDE>(k, m), d[k + m], lin);
     acc = fma2(w[k], lin, acc);
   }
   return fma2(acc, r, s4);
 }
 
-__device__ __forceinline__ void weno9_edges2(const float2 (&s)[9], float2 &qL, float2 &qR, bool2 do_map, bool2 imm_L,
-                                             bool2 imm_R) {
+// Stencil differences and the shared reciprocals rk = 1/(TV_k^2 + 1e-20) of
+// two stencils.
+__device__ __forceinline__ void weno9_rk2(const float2 (&s)[9], float2 (&d)[8], float2 (&rk)[5], bool2 imm_L,
+                                          bool2 imm_R) {
   using namespace pu_weno9;
-  float2 d[8];
 #pragma unroll
   for (int m = 0; m < 8; m++) d[m] = sub2(s[m + 1], s[m]);
   float2 tv[5];
@@ -223,11 +238,25 @@ __device__ __forceinline__ void weno9_edges2(const float2 (&s)[9], float2 &qL, f
     if (imm_R.x) tv[0].x = mx;
     if (imm_R.y) tv[0].y = my;
   }
-  float2 rk[5];
 #pragma unroll
   for (int k = 0; k < 5; k++) rk[k] = rcp2(fma2(tv[k], tv[k], f2(1.e-20f)));
-  qL = weno9_edge2<true>(d, s[4], rk, do_map);
-  qR = weno9_edge2<false>(d, s[4], rk, do_map);
+}
+
+__device__ __forceinline__ void weno9_edges2(const float2 (&s)[9], float2 &qL, float2 &qR, bool2 do_map, bool2 imm_L,
+                                             bool2 imm_R) {
+  float2 d[8], rk[5];
+  weno9_rk2(s, d, rk, imm_L, imm_R);
+  qL = weno9_edge2<0>(d, s[4], rk, do_map);
+  qR = weno9_edge2<1>(d, s[4], rk, do_map);
+}
+
+// The right edge of stencil x and the left edge of stencil y, each
+// bit-identical to that edge from weno9_edges2: the one edge a tile needs
+// from each of the two halo cells that close a row of faces.
+__device__ __forceinline__ float2 weno9_outer_edges2(const float2 (&s)[9], bool2 do_map, bool2 imm_L, bool2 imm_R) {
+  float2 d[8], rk[5];
+  weno9_rk2(s, d, rk, imm_L, imm_R);
+  return weno9_edge2<2>(d, s[4], rk, do_map);
 }
 
 // Normalised nonlinear weights of the left edge (after map_rs when do_map),

@@ -1,6 +1,7 @@
-"""The FP32 order-9 limiter's two forms agree bit for bit
-(pu_weno9_edges_f32): the scalar form (z march, fallbacks) and the packed
-two-stencil form of the x/y kernel (FFMA2/FADD2/FMUL2).  Stencils: random
+"""The FP32 order-9 limiter's forms agree bit for bit
+(pu_weno9_edges_f32): the scalar form (z march, fallbacks), the packed
+two-stencil form of the x/y kernel (FFMA2/FADD2/FMUL2) and its one-edge
+form for the halo cells.  Stencils: random
 normal, polynomials of degree <= 4, constants, smooth data plus noise of
 amplitude 1e-9 .. 1e-1 (weights from ideal to far from it), steps, with
 random map and immersed flags.  The scalar form is also held to the
@@ -53,6 +54,18 @@ def test_limiter_forms_agree_bit_for_bit(gpu_lib):
     assert np.array_equal(out[1][0].view(np.uint32), out[0][0].view(np.uint32))
     assert np.array_equal(out[1][1].view(np.uint32), out[0][1].view(np.uint32))
     assert np.all(np.isfinite(out[0][0])) and np.all(np.isfinite(out[0][1]))
+
+
+def test_one_edge_form_gives_the_same_bits(gpu_lib):
+    """Variant 4, the halo cells of the x/y kernel: the right edge of each
+    even stencil and the left edge of each odd one, bit for bit those of the
+    two-edge forms (random map and immersed flags per lane)."""
+    s, flags = _stencils(40000, seed=3)
+    qL0, qR0 = _run(gpu_lib, s, flags, 0)
+    qL4, qR4 = _run(gpu_lib, s, flags, 4)
+    assert np.array_equal(qR4[0::2].view(np.uint32), qR0[0::2].view(np.uint32))
+    assert np.array_equal(qL4[1::2].view(np.uint32), qL0[1::2].view(np.uint32))
+    assert np.all(np.isnan(qL4[0::2])) and np.all(np.isnan(qR4[1::2]))
 
 
 def test_scalar_form_against_the_reference_limiter(oracle_lib, gpu_lib):

@@ -243,11 +243,13 @@ struct XYShape {
   static constexpr int EN = EXN > EYN ? EXN : EYN;
   static constexpr int FXN = TY * (TX + 1), FYN = (TY + 1) * TX;
   static constexpr int FN = FXN > FYN ? FXN : FYN;
+  // Edges of the y lines' halo cells, taken during the x phase (packed path).
+  static constexpr int YON = 2 * F * TX;
   // Learned mode: per-warp network scratch and two fallback counters; the
   // fallback queue (16-bit stencil indices) lives in the flux buffer, which
   // is idle while edges are reconstructed.
   static constexpr size_t learned_bytes = LEARNED ? size_t(NT / 32) * mlp::WARP_SMEM_BYTES + 16 : 0;
-  static constexpr size_t bytes = sizeof(R) * (size_t(F) * HY * HX + 2 * size_t(F) * EN + size_t(S) * FN) +
+  static constexpr size_t bytes = sizeof(R) * (size_t(F) * HY * HX + 2 * size_t(F) * EN + size_t(S) * FN + YON) +
                                   (IMM ? (size_t(HY) * HX + 15) / 16 * 16 : 0) + learned_bytes;
   static_assert(!LEARNED || size_t(F) * EN * 2 <= sizeof(R) * S * FN, "fallback queue exceeds the flux buffer");
   static_assert(NT % 32 == 0, "whole warps");
@@ -310,15 +312,16 @@ __device__ __forceinline__ int recon_learned(const Grid<float> &G, uint32_t *sW,
 // (weno_all).  There are F x LINES lines of W+2 cells (positions 0..W+1,
 // cells -1..W); the faces of a line read both edges of the W inner cells, the
 // right edge of position 0 and the left edge of position W+1.  Inner cells go
-// two per thread and iteration (weno9_edges2); the two halo cells of a line
-// go together through the one-edge form (weno9_outer_edges2), which skips the
-// two edges nobody reads.  Per stencil and edge the bits are those of
-// weno9_edges.  POS_MAJOR: consecutive threads take consecutive lines at one
-// position (y), else consecutive positions of one line (x).
+// two per thread and iteration (weno9_edges2, recon_packed_inner); the two
+// halo cells of a line go together through the one-edge form
+// (weno9_outer_edges2, recon_outer_pair), which skips the two edges nobody
+// reads.  Per stencil and edge the bits are those of weno9_edges.
+// POS_MAJOR: consecutive threads take consecutive lines at one position (y),
+// else consecutive positions of one line (x).
 // load(f, line, pos, s, imm, any10), store(f, line, pos, qL, qR),
 // store_outer(f, line, qR of position 0, qL of position W+1).
-template <int NT, int F, int LINES, int W, bool POS_MAJOR, class Load, class Store, class StoreOuter>
-__device__ __forceinline__ void recon_packed_lines(Load load, Store store, StoreOuter store_outer) {
+template <int NT, int F, int LINES, int W, bool POS_MAJOR, class Load, class Store>
+__device__ __forceinline__ void recon_packed_inner(Load load, Store store) {
   constexpr int N_IN = F * LINES * W;
   auto coords = [](int it, int &f, int &line, int &pos) {
     f = it / (LINES * W);
@@ -353,20 +356,21 @@ __device__ __forceinline__ void recon_packed_lines(Load load, Store store, Store
     store(fa, la, pa, qL.x, qR.x);
     if (two) store(fb, lb, pb, qL.y, qR.y);
   }
-  for (int p = threadIdx.x; p < F * LINES; p += NT) {
-    const int f = p / LINES, line = p % LINES;
-    float a[9], b[9];
-    unsigned ia, ib;
-    bool xa, xb;
-    load(f, line, 0, a, ia, xa);
-    load(f, line, W + 1, b, ib, xb);
-    float2 s2[9];
+}
+
+template <int W, class Load, class StoreOuter>
+__device__ __forceinline__ void recon_outer_pair(int f, int line, Load load, StoreOuter store_outer) {
+  float a[9], b[9];
+  unsigned ia, ib;
+  bool xa, xb;
+  load(f, line, 0, a, ia, xa);
+  load(f, line, W + 1, b, ib, xb);
+  float2 s2[9];
 #pragma unroll
-    for (int m = 0; m < 9; m++) s2[m] = make_float2(a[m], b[m]);
-    const float2 q = weno9_outer_edges2(s2, bool2{!xa, !xb}, bool2{((ia >> 3) & 1u) != 0, ((ib >> 3) & 1u) != 0},
-                                        bool2{((ia >> 5) & 1u) != 0, ((ib >> 5) & 1u) != 0});
-    store_outer(f, line, q.x, q.y);
-  }
+  for (int m = 0; m < 9; m++) s2[m] = make_float2(a[m], b[m]);
+  const float2 q = weno9_outer_edges2(s2, bool2{!xa, !xb}, bool2{((ia >> 3) & 1u) != 0, ((ib >> 3) & 1u) != 0},
+                                      bool2{((ia >> 5) & 1u) != 0, ((ib >> 5) & 1u) != 0});
+  store_outer(f, line, q.x, q.y);
 }
 
 // x/y fluxes and their divergence for one (x,y) tile of one level.
@@ -381,8 +385,9 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
   R *EL = H + F * HY * HX;
   R *ER = EL + F * EN;
   R *FL = ER + F * EN;
-  uint8_t *M = reinterpret_cast<uint8_t *>(FL + S * FN);
-  unsigned char *lrn = reinterpret_cast<unsigned char *>(FL + S * FN) + (IMM ? (size_t(HY) * HX + 15) / 16 * 16 : 0);
+  R *YO = FL + S * FN;                                       // [2][F][TX] y halo-cell edges
+  uint8_t *M = reinterpret_cast<uint8_t *>(YO + Sh::YON);
+  unsigned char *lrn = reinterpret_cast<unsigned char *>(YO + Sh::YON) + (IMM ? (size_t(HY) * HX + 15) / 16 * 16 : 0);
   int *qn = reinterpret_cast<int *>(lrn);                    // [2] fallback counts (x, y)
   uint32_t *sW = reinterpret_cast<uint32_t *>(lrn + 16) + (threadIdx.x >> 5) * (mlp::WARP_SMEM_BYTES / 4);
   uint16_t *queue = reinterpret_cast<uint16_t *>(FL);
@@ -449,6 +454,21 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
     const int f = it / Sh::EXN, rem = it % Sh::EXN;
     load_xc(f, rem / (TX + 2), rem % (TX + 2), s, imm, any10);
   };
+  // y stencil of cell rr-1 of tile column cc (position rr = 0..TY+1).
+  auto load_yc = [&](int f, int cc, int rr, R (&s)[9], unsigned &imm, bool &any10) {
+    const R *col = H + (f * HY + rr) * HX + 5 + cc;
+#pragma unroll
+    for (int m = 0; m < 9; m++) s[m] = col[m * HX];
+    imm = 0;
+    any10 = false;
+    if (IMM) {
+      const uint8_t *mc = M + rr * HX + 5 + cc;
+#pragma unroll
+      for (int m = 0; m < 9; m++) imm |= (unsigned(mc[m * HX]) & FLAG_IMM) << m;
+      any10 = (mc[4 * HX] & FLAG_ANY10) != 0;
+      if (f == iU || f == iW || f == iP) der0_modify(s, imm);
+    }
+  };
   auto store_x = [&](int it, R qL, R qR) {
     const int f = it / Sh::EXN, rem = it % Sh::EXN;
     EL[f * EN + rem] = qL;
@@ -458,11 +478,27 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
   bool packed = false;
   if constexpr (std::is_same<R, float>::value && PU_PACKED_LIMITER && !LEARNED) {
     packed = G.weno_all != 0;
-    if (packed)
-      recon_packed_lines<NT, F, TY, TX, false>(load_xc, store_xc, [&](int f, int r, R qR0, R qL1) {
-        ER[f * EN + r * (TX + 2)] = qR0;
-        EL[f * EN + r * (TX + 2) + TX + 1] = qL1;
-      });
+    if (packed) {
+      recon_packed_inner<NT, F, TY, TX, false>(load_xc, store_xc);
+      // Halo pairs of the x lines, and already those of the y lines (kept in
+      // YO until the y phase), so that every thread takes one pair here and
+      // the y phase is the inner rounds alone.
+      const int nxo = F * TY, nyo = sim2d ? 0 : F * TX;
+      for (int p = tid; p < nxo + nyo; p += NT) {
+        if (p < nxo) {
+          recon_outer_pair<TX>(p / TY, p % TY, load_xc, [&](int f, int r, R qR0, R qL1) {
+            ER[f * EN + r * (TX + 2)] = qR0;
+            EL[f * EN + r * (TX + 2) + TX + 1] = qL1;
+          });
+        } else {
+          const int q = p - nxo;
+          recon_outer_pair<TY>(q / TX, q % TX, load_yc, [&](int f, int cc, R qR0, R qL1) {
+            YO[f * TX + cc] = qR0;
+            YO[(F + f) * TX + cc] = qL1;
+          });
+        }
+      }
+    }
   }
   if constexpr (LEARNED) {
     n_fb += recon_learned<NT>(G, sW, queue, qn, F * Sh::EXN, load_x, store_x);
@@ -514,20 +550,6 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
 
   if (!sim2d) {
     // 5. y edges of cells -1..TY of every tile column.
-    auto load_yc = [&](int f, int cc, int rr, R (&s)[9], unsigned &imm, bool &any10) {
-      const R *col = H + (f * HY + rr) * HX + 5 + cc;
-#pragma unroll
-      for (int m = 0; m < 9; m++) s[m] = col[m * HX];
-      imm = 0;
-      any10 = false;
-      if (IMM) {
-        const uint8_t *mc = M + rr * HX + 5 + cc;
-#pragma unroll
-        for (int m = 0; m < 9; m++) imm |= (unsigned(mc[m * HX]) & FLAG_IMM) << m;
-        any10 = (mc[4 * HX] & FLAG_ANY10) != 0;
-        if (f == iU || f == iW || f == iP) der0_modify(s, imm);
-      }
-    };
     auto load_y = [&](int it, R (&s)[9], unsigned &imm, bool &any10) {
       const int f = it / Sh::EYN, rem = it % Sh::EYN;
       load_yc(f, rem % TX, rem / TX, s, imm, any10);
@@ -541,17 +563,17 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
       __syncthreads();   // step 4 has read the flux buffer that holds the queue
       n_fb += recon_learned<NT>(G, sW, queue, qn + 1, F * Sh::EYN, load_y, store_y);
     } else if (packed) {
-      if constexpr (std::is_same<R, float>::value)
-        recon_packed_lines<NT, F, TX, TY, true>(
-            load_yc,
-            [&](int f, int cc, int rr, R qL, R qR) {
-              EL[f * EN + rr * TX + cc] = qL;
-              ER[f * EN + rr * TX + cc] = qR;
-            },
-            [&](int f, int cc, R qR0, R qL1) {
-              ER[f * EN + cc] = qR0;
-              EL[f * EN + (TY + 1) * TX + cc] = qL1;
-            });
+      if constexpr (std::is_same<R, float>::value) {
+        recon_packed_inner<NT, F, TX, TY, true>(load_yc, [&](int f, int cc, int rr, R qL, R qR) {
+          EL[f * EN + rr * TX + cc] = qL;
+          ER[f * EN + rr * TX + cc] = qR;
+        });
+        for (int p = tid; p < F * TX; p += NT) {   // the halo-cell edges taken in the x phase
+          const int f = p / TX, cc = p % TX;
+          ER[f * EN + cc] = YO[p];
+          EL[f * EN + (TY + 1) * TX + cc] = YO[F * TX + p];
+        }
+      }
     } else {
       for (int it = tid; it < F * Sh::EYN; it += NT) {
         R s[9];

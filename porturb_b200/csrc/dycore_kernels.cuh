@@ -34,12 +34,16 @@
 namespace pu {
 
 // Packed FP32 limiter (two stencils per FFMA2/FADD2/FMUL2) in the plain x/y
-// kernel; 0 keeps the scalar limiter (results are identical).  The z march
-// keeps the scalar limiter: packing pairs of fields there raises its
-// registers from ~125 to ~165 and the lost occupancy costs more (1.11 against
-// 1.10 ms per launch).
+// kernel; 0 keeps the scalar limiter (results are identical).
 #ifndef PU_PACKED_LIMITER
 #define PU_PACKED_LIMITER 1
+#endif
+// The same in the z march, on pairs of fields of the cell (weno_all): under
+// the 128-register cap of PU_Z_MIN_BLOCKS it fits without spills (126
+// registers; uncapped it took ~165 and lost the time to occupancy) and takes
+// k_z from 1.055 to 0.919 ms on the 256x256x128 boundary layer.
+#ifndef PU_PACKED_Z
+#define PU_PACKED_Z 1
 #endif
 // Minimum resident blocks per SM requested for the plain FP32 x/y kernel: 4
 // (64 registers) keeps 32 warps per SM with the packed limiter (measured on
@@ -842,8 +846,37 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : (s
           eL[f * NT + tid] = qL;
           eRc[f * NT] = qR;
         };
+        bool done = false;
+        if constexpr (std::is_same<R, float>::value && PU_PACKED_Z) {
+          if (G.weno_all) {   // pairs of fields through the packed limiter
 #pragma unroll 1
-        for (int f = 0; f < F; f++) one_field(f);
+            for (int f = 0; f + 1 < F; f += 2) {
+              float a[9], b[9];
+#pragma unroll
+              for (int m = 0; m < 9; m++) {
+                a[m] = ring[sl[m] + f * NT];
+                b[m] = ring[sl[m] + (f + 1) * NT];
+              }
+              if (f == iU || f == iV || f == iP) der0_modify(a, imm);
+              if (f + 1 == iU || f + 1 == iV || f + 1 == iP) der0_modify(b, imm);
+              float2 s2[9], qL, qR;
+#pragma unroll
+              for (int m = 0; m < 9; m++) s2[m] = make_float2(a[m], b[m]);
+              const bool il = (imm >> 3) & 1u, ir = (imm >> 5) & 1u;
+              weno9_edges2(s2, qL, qR, bool2{!any10, !any10}, bool2{il, il}, bool2{ir, ir});
+              eL[f * NT + tid] = qL.x;
+              eL[(f + 1) * NT + tid] = qL.y;
+              eRc[f * NT] = qR.x;
+              eRc[(f + 1) * NT] = qR.y;
+            }
+            if (F & 1) one_field(F - 1);
+            done = true;
+          }
+        }
+        if (!done) {
+#pragma unroll 1
+          for (int f = 0; f < F; f++) one_field(f);
+        }
       }
     }
     if (c > cstart || (wall && c == 0)) {

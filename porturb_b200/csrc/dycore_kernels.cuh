@@ -79,6 +79,8 @@ struct Grid {
   int bc_x, bc_y, bc_z;
   int sim2d, weno_all, enable_gravity;
   R grav, fcor, gamma;
+  R pc[5];                      // C(gamma, n), n = 1..5: the series of pow1pm1
+  int pser;                     // gamma in [1, 5/3]: pow1pm1 may use the series
   unsigned tracer_positive;     // bit t: tracer t is positive definite
   // Level tables.  Cell tables have nz+2*HS entries (index k+HS); edge tables nz+1.
   const R *rho_h, *theta_h;     // hy_dens_cells, hy_theta_cells
@@ -117,10 +119,25 @@ __device__ __forceinline__ double pu_log1p(double x) { return log1p(x); }
 __device__ __forceinline__ float pu_expm1(float x) { return expm1f(x); }
 __device__ __forceinline__ double pu_expm1(double x) { return expm1(x); }
 
+// (1+x)^gamma - 1, the pressure perturbation relative to the column's
+// C0 (rho theta)_h^gamma.  In FP32 and for |x| <= 1/16 (every cell of the
+// boundary-layer, bubble and urban cases) the binomial series to x^5,
+// sum C(gamma,n) x^n by Horner (coefficients G.pc): the first omitted term is
+// below 5e-9 of the result for gamma in [1, 5/3], under the FP32 rounding.
+// Otherwise, and in FP64, expm1(gamma log1p(x)).
+template <class R>
+__device__ __forceinline__ R pow1pm1(const Grid<R> &G, R x) {
+  if constexpr (std::is_same<R, float>::value) {
+    if (G.pser && fabsf(x) <= 0.0625f)
+      return fmaf(fmaf(fmaf(fmaf(G.pc[4], x, G.pc[3]), x, G.pc[2]), x, G.pc[1]), x, G.pc[0]) * x;
+  }
+  return pu_expm1(G.gamma * pu_log1p(x));
+}
+
 // Primitive perturbation fields of one cell (dynamics_rk.h:550-558):
 // rho', u, v, w, theta', p', tracer mixing ratios.  theta' and p' are formed
 // from the perturbation storage without cancellation:
-//   theta' = (q4 - theta_h q0)/rho,   p' = P0_h*expm1(gamma*log1p(q4/(rho theta)_h)) + (P0_h - p_h).
+//   theta' = (q4 - theta_h q0)/rho,   p' = P0_h*((1 + q4/(rho theta)_h)^gamma - 1) + (P0_h - p_h).
 // s holds the S raw fields N elements apart (the resident arrays, N = nz*ny*nx,
 // or a halo slab).
 template <class R, int NTR>
@@ -136,7 +153,7 @@ __device__ __forceinline__ void prims_s(const Grid<R> &G, const R *__restrict__ 
   w[2] = q2 * rr;
   w[3] = q3 * rr;
   w[4] = (q4 - __ldg(G.theta_h + kh) * q0) * rr;
-  w[5] = fma(__ldg(G.p0_h + kh), pu_expm1(G.gamma * pu_log1p(q4 * __ldg(G.rt_inv + kh))), __ldg(G.dp_h + kh));
+  w[5] = fma(__ldg(G.p0_h + kh), pow1pm1(G, q4 * __ldg(G.rt_inv + kh)), __ldg(G.dp_h + kh));
 #pragma unroll
   for (int t = 0; t < NTR; t++) w[6 + t] = __ldg(s + (5 + t) * N + idx) * rr;
 }
@@ -680,7 +697,7 @@ __device__ __forceinline__ void prims_of(const Grid<R> &G, const R (&q)[5 + NTR]
   w[2] = q[2] * rr;
   w[3] = q[3] * rr;
   w[4] = (q[4] - __ldg(G.theta_h + kh) * q[0]) * rr;
-  w[5] = fma(__ldg(G.p0_h + kh), pu_expm1(G.gamma * pu_log1p(q[4] * __ldg(G.rt_inv + kh))), __ldg(G.dp_h + kh));
+  w[5] = fma(__ldg(G.p0_h + kh), pow1pm1(G, q[4] * __ldg(G.rt_inv + kh)), __ldg(G.dp_h + kh));
 #pragma unroll
   for (int t = 0; t < NTR; t++) w[6 + t] = q[5 + t] * rr;
 }

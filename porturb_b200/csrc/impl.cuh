@@ -622,6 +622,14 @@ struct Impl : ImplBase {
     G.grav = R(cfg.grav);
     G.fcor = R(2 * 7.2921e-5 * std::sin(cfg.latitude / 180 * M_PI));
     G.gamma = R(cfg.gamma_d);
+    {
+      double c = 1;
+      for (int n = 1; n <= 5; n++) {
+        c *= (cfg.gamma_d - (n - 1)) / n;
+        G.pc[n - 1] = R(c);
+      }
+      G.pser = cfg.gamma_d >= 1. && cfg.gamma_d <= 5. / 3.;
+    }
     G.tracer_positive = 0;
     for (int t = 0; t < NTR; t++)
       if (cfg.tracer_positive[t]) G.tracer_positive |= 1u << t;

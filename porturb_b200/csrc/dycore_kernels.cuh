@@ -62,6 +62,11 @@ namespace pu {
 #ifndef PU_LEARNED_XY_MIN_BLOCKS
 #define PU_LEARNED_XY_MIN_BLOCKS 2
 #endif
+// Minimum resident blocks per SM requested for the tiled z kernel k_zt
+// (256 threads: 4 blocks cap it at 64 registers, as the x/y kernel).
+#ifndef PU_ZT_MIN_BLOCKS
+#define PU_ZT_MIN_BLOCKS 4
+#endif
 #ifndef PU_LEARNED_Z_MIN_BLOCKS
 #define PU_LEARNED_Z_MIN_BLOCKS 3
 #endif
@@ -953,6 +958,168 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : (s
     atomicAdd(G.ml_counts, n_learned);
     atomicAdd(G.ml_counts + 1, n_fallback);
   }
+}
+
+// Shared memory of k_zt: primitive fields of the tile's columns at levels
+// k0-5 .. k0+TZ+4, left/right z edges of the cells at levels k0-1 .. k0+TZ,
+// the fluxes on faces k0 .. k0+TZ, and whether each level lies beyond the
+// domain (the immersed bit of the z stencils).
+template <int NTR, int TX, int TZ>
+struct ZTShape {
+  static constexpr int F = 6 + NTR, S = 5 + NTR, NT = TX * TZ, HZ = TZ + 10;
+  static constexpr int EN = (TZ + 2) * TX, FN = (TZ + 1) * TX;
+  static constexpr size_t bytes = sizeof(float) * (size_t(F) * HZ * TX + 2 * size_t(F) * EN + size_t(S) * FN) +
+                                  (size_t(HZ) * TX + 15) / 16 * 16;
+};
+
+// The z operator and the stage combination of k_z on a tile of TX columns of
+// one row by TZ levels, with the work spread over the block instead of
+// marched: the same results bit for bit (the same primitive fields, face
+// states, limiter bits per stencil, Riemann fluxes and combination).  The
+// primitive fields of levels k0-5 .. k0+TZ+4 go to shared memory; the z edges
+// of the TZ inner cells of each column come from the packed limiter two
+// stencils per thread, the two cells that close a column (k0-1: right edge,
+// k0+TZ: left edge) from its one-edge form; then the Riemann fluxes on faces
+// k0 .. k0+TZ, and each thread finalises one cell.  FP32 with weno_all and
+// no immersed cells; every other form keeps the march (with immersed cells
+// the per-stencil flags and enforcement cost this schedule more than it
+// gains: 0.968 against 0.914 ms on a 256x256x128 urban canopy).
+template <int NTR, int TX, int TZ>
+__global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<float> G, const float *__restrict__ sin,
+                                                               const float *sn, float *sout,
+                                                               const float *__restrict__ txy, float a_n, float a_dt,
+                                                               int n_enforce) {
+  using R = float;
+  using Sh = ZTShape<NTR, TX, TZ>;
+  constexpr int F = Sh::F, S = Sh::S, NT = Sh::NT, HZ = Sh::HZ, FN = Sh::FN;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *H = reinterpret_cast<R *>(smem_raw);   // [F][HZ][TX]
+  R *EL = H + F * HZ * TX;                   // [F][TZ+2][TX]
+  R *ER = EL + F * Sh::EN;
+  R *FL = ER + F * Sh::EN;                   // [S][TZ+1][TX]
+  uint8_t *M = reinterpret_cast<uint8_t *>(FL + S * FN);   // [HZ][TX]
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * TX, j = blockIdx.y, k0 = blockIdx.z * TZ;
+  const int nx = G.nx, nz = G.nz;
+  const bool wall = G.bc_z == BC_WALL;
+  const size_t NP = G.NP, row = size_t(j) * nx;
+  // Level whose state feeds level p (wall halos replicate the boundary cell,
+  // periodic halos wrap; dynamics_rk.h:780-797).
+  auto src_level = [&](int p) { return (p >= 0 && p < nz) ? p : (wall ? clampi(p, nz) : wrapi(p, nz)); };
+
+  // 1. Primitive fields of levels k0-5 .. k0+TZ+4, and which of them lie
+  // beyond the domain.  Columns beyond the domain read its last column; their
+  // results are discarded.
+  for (int it = tid; it < HZ * TX; it += NT) {
+    const int r = it / TX, c = it % TX;
+    const int p = k0 - 5 + r, lv = src_level(p);
+    const size_t col = row + min(i0 + c, nx - 1);
+    R q[S], w[F];
+    load_cell<R, NTR>(G, sin, size_t(lv) * NP + col, q);
+    prims_of<R, NTR>(G, q, lv, w);
+    if (wall && (p < 0 || p >= nz)) {
+      w[iW] = R(0);
+      w[iT] = R(0);
+    }
+#pragma unroll
+    for (int f = 0; f < F; f++) H[(f * HZ + r) * TX + c] = w[f];
+    M[r * TX + c] = (p < 0 || p >= nz) ? uint8_t(1) : uint8_t(0);
+  }
+  __syncthreads();
+
+  // 2. z edges of the cells at positions q = 0 .. TZ+1 (level k0-1+q).  The
+  // immersed bits of a stencil are those of the levels around its canonical
+  // cell (wrapped in periodic z): levels beyond the domain count as immersed
+  // (the z halos of the proportion are 1, dynamics_rk.h:1031-1034).
+  auto load = [&](int f, int c, int q, R (&s)[9], unsigned &imm, bool &any10) {
+    const R *colh = H + (f * HZ + q) * TX + c;
+#pragma unroll
+    for (int m = 0; m < 9; m++) s[m] = colh[m * TX];
+    const int L = k0 - 1 + q;
+    imm = 0;
+    any10 = false;
+    if (L >= 0 && L < nz) {
+#pragma unroll
+      for (int m = 0; m < 9; m++) imm |= unsigned(M[(q + m) * TX + c]) << m;
+    } else {
+      // A cell beyond the domain: periodic z only (in a wall domain no face
+      // reads it).
+      const int cc = wrapi(L, nz);
+#pragma unroll
+      for (int m = 0; m < 9; m++) imm |= unsigned(cc - 4 + m < 0 || cc - 4 + m >= nz) << m;
+    }
+    if (f == iU || f == iV || f == iP) der0_modify(s, imm);
+  };
+  recon_packed_inner<NT, F, TX, TZ, true>(load, [&](int f, int c, int q, R qL, R qR) {
+    EL[(f * (TZ + 2) + q) * TX + c] = qL;
+    ER[(f * (TZ + 2) + q) * TX + c] = qR;
+  });
+  for (int pr = tid; pr < F * TX; pr += NT)
+    recon_outer_pair<TZ>(pr / TX, pr % TX, load, [&](int f, int c, R qR0, R qL1) {
+      ER[(f * (TZ + 2)) * TX + c] = qR0;
+      EL[(f * (TZ + 2) + TZ + 1) * TX + c] = qL1;
+    });
+  __syncthreads();
+
+  // 3. Riemann fluxes on faces k0 .. k0+TZ (face fz+k0 between the cells at
+  // positions fz and fz+1; edge_exchange z, dynamics_rk.h:891-908).
+  for (int it = tid; it < FN; it += NT) {
+    const int fz = it / TX, c = it % TX, cf = k0 + fz;
+    if (cf > nz) continue;
+    R Lf[F], Rf[F];
+    if (wall && cf == 0) {
+#pragma unroll
+      for (int f = 0; f < F; f++) Lf[f] = Rf[f] = EL[(f * (TZ + 2) + fz + 1) * TX + c];
+      Lf[iW] = Rf[iW] = Lf[iT] = Rf[iT] = R(0);
+    } else if (wall && cf == nz) {
+#pragma unroll
+      for (int f = 0; f < F; f++) Lf[f] = Rf[f] = ER[(f * (TZ + 2) + fz) * TX + c];
+      Lf[iW] = Rf[iW] = Lf[iT] = Rf[iT] = R(0);
+    } else {
+#pragma unroll
+      for (int f = 0; f < F; f++) {
+        Lf[f] = ER[(f * (TZ + 2) + fz) * TX + c];
+        Rf[f] = EL[(f * (TZ + 2) + fz + 1) * TX + c];
+      }
+    }
+    R fl[S];
+    riemann<R, NTR>(Lf, Rf, __ldg(G.rho_e + cf), __ldg(G.theta_e + cf), iW, fl);
+#pragma unroll
+    for (int s2 = 0; s2 < S; s2++) FL[s2 * FN + it] = fl[s2];
+  }
+  __syncthreads();
+
+  // 4. Divergence, sources, stage combination and enforcement of one cell.
+  const int c = tid % TX, kz = tid / TX, k = k0 + kz, gi = i0 + c;
+  if (gi >= nx || k >= nz) return;
+  const size_t idx = size_t(k) * NP + row + gi;
+  R qin[S], tend[S], out[S];
+#pragma unroll
+  for (int s2 = 0; s2 < S; s2++) {
+    qin[s2] = sin[s2 * G.N + idx];
+    tend[s2] = txy[s2 * G.N + idx] - (FL[s2 * FN + (kz + 1) * TX + c] - FL[s2 * FN + kz * TX + c]) * G.rdz;
+  }
+  if (G.sim2d) tend[iV] = R(0);
+  if (G.enable_gravity) tend[iW] += -G.grav * qin[iR];
+  if (G.fcor != R(0) && !G.sim2d) {
+    tend[iU] += G.fcor * qin[iV];
+    tend[iV] -= G.fcor * qin[iU];
+  }
+  if (sn) {
+#pragma unroll
+    for (int s2 = 0; s2 < S; s2++) out[s2] = qin[s2] + fma(a_n, sn[s2 * G.N + idx] - qin[s2], a_dt * tend[s2]);
+  } else {
+#pragma unroll
+    for (int s2 = 0; s2 < S; s2++) out[s2] = qin[s2] + a_dt * tend[s2];
+  }
+  for (int e = 0; e < n_enforce; e++) enforce_cell<R, NTR, false>(G, out, idx, k);
+  bool bad = false;
+#pragma unroll
+  for (int s2 = 0; s2 < S; s2++) {
+    bad |= !isfinite(out[s2]);
+    sout[s2 * G.N + idx] = out[s2];
+  }
+  if (bad) atomicOr(G.err, 1);
 }
 
 // a += b elementwise.

@@ -480,6 +480,7 @@ struct Impl : ImplBase {
   static constexpr int XTX_BIG = PU_XY_TILE_X, XTY_BIG = PU_XY_TILE_Y;   // x/y tile for ny >= 16
   static constexpr int LTX = 16, LTY = 16;           // x/y tile of the learned form (ny >= 16)
   static constexpr int XTX_SM = 32, XTY_SM = 4;      // x/y tile for thin domains
+  static constexpr int ZT_X = 8, ZT_Z = 32;          // tiled z kernel: columns x levels per block
   static constexpr int ZTX = 32, ZTY = 4;            // z-march columns per block
   LevelTables<R> lt{};
   bool small_tile = false;
@@ -574,6 +575,8 @@ struct Impl : ImplBase {
     PU_CK(cudaFuncSetAttribute(k_z<R, NTR, ZTX, ZTY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(ZShape<R, NTR, ZTX, ZTY>::bytes)));
     if constexpr (std::is_same<R, float>::value) {
+      PU_CK(cudaFuncSetAttribute(k_zt<NTR, ZT_X, ZT_Z>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(ZTShape<NTR, ZT_X, ZT_Z>::bytes)));
       PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, LTX, LTY, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(XYShape<R, NTR, LTX, LTY, false, true>::bytes)));
       PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, LTX, LTY, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -830,6 +833,13 @@ struct Impl : ImplBase {
     return check_err();
   }
 
+  // The tiled z kernel (k_zt) takes the plain FP32 limiter with weno_all on
+  // domains without immersed cells, unless a z chunk was asked for (the
+  // march, which gives the same bits).
+  bool z_tiled(bool learned) const {
+    return std::is_same<R, float>::value && cfg.weno_all && !learned && cfg.z_chunk <= 0;
+  }
+
   // Learned weights replace the nonlinear limiter where it runs on every
   // stencil (weno_all) in FP32.
   bool learned_active() const {
@@ -861,6 +871,16 @@ struct Impl : ImplBase {
     const int kc = cfg.z_chunk > 0 ? cfg.z_chunk : (cfg.nz < 16 ? cfg.nz : 16);
     dim3 gz(blocks(cfg.nx, ZTX), blocks(cfg.ny, ZTY), blocks(cfg.nz, kc));
     cudaEvent_t e1 = prof_begin();
+    if constexpr (std::is_same<R, float>::value) {
+      if (!IMM && z_tiled(L)) {
+        dim3 gt(blocks(cfg.nx, ZT_X), cfg.ny, blocks(cfg.nz, ZT_Z));
+        k_zt<NTR, ZT_X, ZT_Z><<<gt, ZT_X * ZT_Z, ZTShape<NTR, ZT_X, ZT_Z>::bytes, st>>>(G, sin, sn, sout, t, a_n,
+                                                                                           a_dt, n_enforce);
+        PU_LAUNCHED();
+        prof_end(1, e1);
+        return PU_OK;
+      }
+    }
     // The learned z march needs full warps: every block's columns inside the domain.
     if (L && cfg.nx % ZTX == 0 && cfg.ny % ZTY == 0)
       k_z<R, NTR, ZTX, ZTY, IMM, L><<<gz, ZTX * ZTY, ZShape<R, NTR, ZTX, ZTY, L>::bytes, st>>>(

@@ -835,9 +835,10 @@ struct Impl : ImplBase {
 
   // The tiled z kernel (k_zt) takes the plain FP32 limiter with weno_all on
   // domains without immersed cells, unless a z chunk was asked for (the
-  // march, which gives the same bits).
+  // march, which gives the same bits).  Its grid has one y row per block
+  // row, so ny is held to the grid's y limit.
   bool z_tiled(bool learned) const {
-    return std::is_same<R, float>::value && cfg.weno_all && !learned && cfg.z_chunk <= 0;
+    return std::is_same<R, float>::value && cfg.weno_all && !learned && cfg.z_chunk <= 0 && cfg.ny <= 65535;
   }
 
   // Learned weights replace the nonlinear limiter where it runs on every

@@ -271,12 +271,16 @@ struct XYShape {
   static constexpr int FN = FXN > FYN ? FXN : FYN;
   // Edges of the y lines' halo cells, taken during the x phase (packed path).
   static constexpr int YON = 2 * F * TX;
+  // Immersed domains: the flag byte of every tile and halo cell, then the
+  // stencil masks of the x lines ([TY][TX+2]) and the y lines ([TY+2][TX]).
+  static constexpr size_t MB = (size_t(HY) * HX + 15) / 16 * 16;
+  static constexpr size_t MASKB = (size_t(2) * (TY * (TX + 2) + (TY + 2) * TX) + 15) / 16 * 16;
   // Learned mode: per-warp network scratch and two fallback counters; the
   // fallback queue (16-bit stencil indices) lives in the flux buffer, which
   // is idle while edges are reconstructed.
   static constexpr size_t learned_bytes = LEARNED ? size_t(NT / 32) * mlp::WARP_SMEM_BYTES + 16 : 0;
   static constexpr size_t bytes = sizeof(R) * (size_t(F) * HY * HX + 2 * size_t(F) * EN + size_t(S) * FN + YON) +
-                                  (IMM ? (size_t(HY) * HX + 15) / 16 * 16 : 0) + learned_bytes;
+                                  (IMM ? MB + MASKB : 0) + learned_bytes;
   static_assert(!LEARNED || size_t(F) * EN * 2 <= sizeof(R) * S * FN, "fallback queue exceeds the flux buffer");
   static_assert(NT % 32 == 0, "whole warps");
 };
@@ -413,7 +417,9 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
   R *FL = ER + F * EN;
   R *YO = FL + S * FN;                                       // [2][F][TX] y halo-cell edges
   uint8_t *M = reinterpret_cast<uint8_t *>(YO + Sh::YON);
-  unsigned char *lrn = reinterpret_cast<unsigned char *>(YO + Sh::YON) + (IMM ? (size_t(HY) * HX + 15) / 16 * 16 : 0);
+  uint16_t *MX = reinterpret_cast<uint16_t *>(M + Sh::MB);  // [TY][TX+2] x-stencil masks (immersed only)
+  uint16_t *MY = MX + TY * (TX + 2);                          // [TY+2][TX] y-stencil masks
+  unsigned char *lrn = reinterpret_cast<unsigned char *>(YO + Sh::YON) + (IMM ? Sh::MB + Sh::MASKB : 0);
   int *qn = reinterpret_cast<int *>(lrn);                    // [2] fallback counts (x, y)
   uint32_t *sW = reinterpret_cast<uint32_t *>(lrn + 16) + (threadIdx.x >> 5) * (mlp::WARP_SMEM_BYTES / 4);
   uint16_t *queue = reinterpret_cast<uint16_t *>(FL);
@@ -456,6 +462,30 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
     for (int f = 0; f < F; f++) H[(f * HY + r) * HX + c] = w[f];
   }
   __syncthreads();
+  if (IMM) {
+    // 1b. The stencil mask of every x and y stencil position, once for all
+    // fields: bits 0-8 the immersed flags of the stencil's cells, bit 9 an
+    // immersed cell within 10 of its centre.
+    constexpr int NXM = TY * (TX + 2), NYM = (TY + 2) * TX;
+    for (int it = tid; it < NXM + (sim2d ? 0 : NYM); it += NT) {
+      const uint8_t *m0;
+      int step;
+      if (it < NXM) {
+        m0 = M + (5 + it / (TX + 2)) * HX + it % (TX + 2);
+        step = 1;
+      } else {
+        const int q = it - NXM;
+        m0 = M + (q / TX) * HX + 5 + q % TX;
+        step = HX;
+      }
+      unsigned e = (m0[4 * step] & FLAG_ANY10) ? 0x200u : 0u;
+#pragma unroll
+      for (int m = 0; m < 9; m++) e |= (unsigned(m0[m * step]) & FLAG_IMM) << m;
+      if (it < NXM) MX[it] = uint16_t(e);
+      else MY[it - NXM] = uint16_t(e);
+    }
+    __syncthreads();
+  }
 
   // 2. x edges of cells -1..TX of every tile row (position c = cell + 1).
   auto load_xc = [&](int f, int r, int c, R (&s)[9], unsigned &imm, bool &any10) {
@@ -465,10 +495,9 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
     imm = 0;
     any10 = false;
     if (IMM) {
-      const uint8_t *mr = M + (5 + r) * HX + c;
-#pragma unroll
-      for (int m = 0; m < 9; m++) imm |= (unsigned(mr[m]) & FLAG_IMM) << m;
-      any10 = (mr[4] & FLAG_ANY10) != 0;
+      const unsigned e = MX[r * (TX + 2) + c];
+      imm = e & 0x1ffu;
+      any10 = (e & 0x200u) != 0;
       if (f == iV || f == iW || f == iP) der0_modify(s, imm);
     }
   };
@@ -488,10 +517,9 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
     imm = 0;
     any10 = false;
     if (IMM) {
-      const uint8_t *mc = M + rr * HX + 5 + cc;
-#pragma unroll
-      for (int m = 0; m < 9; m++) imm |= (unsigned(mc[m * HX]) & FLAG_IMM) << m;
-      any10 = (mc[4 * HX] & FLAG_ANY10) != 0;
+      const unsigned e = MY[rr * TX + cc];
+      imm = e & 0x1ffu;
+      any10 = (e & 0x200u) != 0;
       if (f == iU || f == iW || f == iP) der0_modify(s, imm);
     }
   };

@@ -335,7 +335,7 @@ __device__ __forceinline__ void linear9_edges(const R (&s)[9], R &qL, R &qR) {
 // imm: bit m set when stencil entry m is immersed.
 template <class R>
 __device__ __forceinline__ void der0_modify(R (&s)[9], unsigned imm) {
-  if (imm & 0x10u) return;
+  if (imm == 0u || (imm & 0x10u)) return;
   bool hit = false;
   R v = s[4];
 #pragma unroll

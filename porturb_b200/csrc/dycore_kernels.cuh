@@ -817,6 +817,8 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : (s
 #pragma unroll
   for (int s = 0; s < S; s++) Fp[s] = R(0);
   int par = 0;   // eR double-buffer index of the current cell
+  unsigned imm_prev = 0;
+  int cc_prev = -1000;   // canonical cell whose stencil flags imm_prev holds
 
   for (int c = cstart; c <= k1; c++) {
     store_plane(c + 4, qnext);
@@ -837,7 +839,18 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : (s
     R *eRc = eR + par * F * NT + tid, *eRp = eR + (par ^ 1) * F * NT + tid;
     if (have_cell) {
       const int cc = wall ? c : wrapi(c, nz);
-      const unsigned imm = stencil_flags(cc);
+      // Stencil flags of cc: one level beyond the previous cell's, one new
+      // flag; else (the first cell, a periodic wrap) all nine.
+      if (cc == cc_prev + 1) {
+        const int p = cc + 4;
+        const unsigned b =
+            (p < 0 || p >= nz) ? 1u : (IMM ? (unsigned(__ldg(G.flags + size_t(p) * NP + col)) & FLAG_IMM) : 0u);
+        imm_prev = (imm_prev >> 1) | (b << 8);
+      } else {
+        imm_prev = stencil_flags(cc);
+      }
+      cc_prev = cc;
+      const unsigned imm = imm_prev;
       const bool any10 = IMM && (__ldg(G.flags + size_t(cc) * NP + col) & FLAG_ANY10);
       int sl[9];
 #pragma unroll

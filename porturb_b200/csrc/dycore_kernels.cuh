@@ -735,6 +735,43 @@ __device__ __forceinline__ void prims_of(const Grid<R> &G, const R (&q)[5 + NTR]
   for (int t = 0; t < NTR; t++) w[6 + t] = q[5 + t] * rr;
 }
 
+// The end of one cell's stage in both z kernels: tend = txy - dF/dz plus
+// gravity and Coriolis, the combination a_n*sn + (1-a_n)*sin + a_dt*tend
+// (sn null: sin + a_dt*tend), n_enforce applications of the immersed and
+// positivity enforcement, the store and the finite check.  dF is the flux
+// difference F(k+1/2) - F(k-1/2); qn(s) gives field s of sn and is called
+// only when sn is set.
+template <class R, int NTR, bool IMM, class Qn>
+__device__ __forceinline__ void finish_cell(const Grid<R> &G, const R (&qin)[5 + NTR], const R (&tx)[5 + NTR],
+                                            Qn qn, const R (&dF)[5 + NTR], bool have_sn, R a_n, R a_dt,
+                                            int n_enforce, size_t idx, int k, R *sout) {
+  constexpr int S = 5 + NTR;
+  R tend[S], out[S];
+#pragma unroll
+  for (int s = 0; s < S; s++) tend[s] = tx[s] - dF[s] * G.rdz;
+  if (G.sim2d) tend[iV] = R(0);
+  if (G.enable_gravity) tend[iW] += -G.grav * qin[iR];
+  if (G.fcor != R(0) && !G.sim2d) {
+    tend[iU] += G.fcor * qin[iV];
+    tend[iV] -= G.fcor * qin[iU];
+  }
+  if (have_sn) {
+#pragma unroll
+    for (int s = 0; s < S; s++) out[s] = qin[s] + fma(a_n, qn(s) - qin[s], a_dt * tend[s]);
+  } else {
+#pragma unroll
+    for (int s = 0; s < S; s++) out[s] = qin[s] + a_dt * tend[s];
+  }
+  for (int e = 0; e < n_enforce; e++) enforce_cell<R, NTR, IMM>(G, out, idx, k);
+  bool bad = false;
+#pragma unroll
+  for (int s = 0; s < S; s++) {
+    bad |= !isfinite(out[s]);
+    sout[s * G.N + idx] = out[s];
+  }
+  if (bad) atomicOr(G.err, 1);
+}
+
 // z fluxes, their divergence, sources and the SSPRK3 stage combination
 // a_n*sn + (1-a_n)*sin + a_dt*tend, evaluated as
 //   out = sin + (a_n*(sn - sin) + a_dt*tend),   tend = txy - dFz/dz + sources
@@ -963,32 +1000,11 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : (s
       R Fc[S];
       riemann<R, NTR>(Lf, Rf, __ldg(G.rho_e + c), __ldg(G.theta_e + c), iW, Fc);
       if (fin) {
-        const int k = c - 1;
-        const size_t idx = size_t(k) * NP + col;
-        R tend[S], out[S];
+        R dF[S];
 #pragma unroll
-        for (int s = 0; s < S; s++) tend[s] = tx[s] - (Fc[s] - Fp[s]) * G.rdz;
-        if (G.sim2d) tend[iV] = R(0);
-        if (G.enable_gravity) tend[iW] += -G.grav * qin[iR];
-        if (G.fcor != R(0) && !G.sim2d) {
-          tend[iU] += G.fcor * qin[iV];
-          tend[iV] -= G.fcor * qin[iU];
-        }
-        if (sn) {
-#pragma unroll
-          for (int s = 0; s < S; s++) out[s] = qin[s] + fma(a_n, qn[s] - qin[s], a_dt * tend[s]);
-        } else {
-#pragma unroll
-          for (int s = 0; s < S; s++) out[s] = qin[s] + a_dt * tend[s];
-        }
-        for (int e = 0; e < n_enforce; e++) enforce_cell<R, NTR, IMM>(G, out, idx, k);
-        bool bad = false;
-#pragma unroll
-        for (int s = 0; s < S; s++) {
-          bad |= !isfinite(out[s]);
-          sout[s * G.N + idx] = out[s];
-        }
-        if (bad) atomicOr(G.err, 1);
+        for (int s = 0; s < S; s++) dF[s] = Fc[s] - Fp[s];
+        finish_cell<R, NTR, IMM>(G, qin, tx, [&](int s) { return qn[s]; }, dF, sn != nullptr, a_n, a_dt,
+                                 n_enforce, size_t(c - 1) * NP + col, c - 1, sout);
       }
 #pragma unroll
       for (int s = 0; s < S; s++) Fp[s] = Fc[s];
@@ -1134,33 +1150,15 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
   const int c = tid % TX, kz = tid / TX, k = k0 + kz, gi = i0 + c;
   if (gi >= nx || k >= nz) return;
   const size_t idx = size_t(k) * NP + row + gi;
-  R qin[S], tend[S], out[S];
+  R qin[S], tx[S], dF[S];
 #pragma unroll
   for (int s2 = 0; s2 < S; s2++) {
     qin[s2] = sin[s2 * G.N + idx];
-    tend[s2] = txy[s2 * G.N + idx] - (FL[s2 * FN + (kz + 1) * TX + c] - FL[s2 * FN + kz * TX + c]) * G.rdz;
+    tx[s2] = txy[s2 * G.N + idx];
+    dF[s2] = FL[s2 * FN + (kz + 1) * TX + c] - FL[s2 * FN + kz * TX + c];
   }
-  if (G.sim2d) tend[iV] = R(0);
-  if (G.enable_gravity) tend[iW] += -G.grav * qin[iR];
-  if (G.fcor != R(0) && !G.sim2d) {
-    tend[iU] += G.fcor * qin[iV];
-    tend[iV] -= G.fcor * qin[iU];
-  }
-  if (sn) {
-#pragma unroll
-    for (int s2 = 0; s2 < S; s2++) out[s2] = qin[s2] + fma(a_n, sn[s2 * G.N + idx] - qin[s2], a_dt * tend[s2]);
-  } else {
-#pragma unroll
-    for (int s2 = 0; s2 < S; s2++) out[s2] = qin[s2] + a_dt * tend[s2];
-  }
-  for (int e = 0; e < n_enforce; e++) enforce_cell<R, NTR, false>(G, out, idx, k);
-  bool bad = false;
-#pragma unroll
-  for (int s2 = 0; s2 < S; s2++) {
-    bad |= !isfinite(out[s2]);
-    sout[s2 * G.N + idx] = out[s2];
-  }
-  if (bad) atomicOr(G.err, 1);
+  finish_cell<R, NTR, false>(G, qin, tx, [&](int s2) { return sn[s2 * G.N + idx]; }, dF, sn != nullptr, a_n, a_dt,
+                             n_enforce, idx, k, sout);
 }
 
 // a += b elementwise.

@@ -1019,14 +1019,12 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : (s
 
 // Shared memory of k_zt: primitive fields of the tile's columns at levels
 // k0-5 .. k0+TZ+4, left/right z edges of the cells at levels k0-1 .. k0+TZ,
-// the fluxes on faces k0 .. k0+TZ, and whether each level lies beyond the
-// domain (the immersed bit of the z stencils).
+// and the fluxes on faces k0 .. k0+TZ.
 template <int NTR, int TX, int TZ>
 struct ZTShape {
   static constexpr int F = 6 + NTR, S = 5 + NTR, NT = TX * TZ, HZ = TZ + 10;
   static constexpr int EN = (TZ + 2) * TX, FN = (TZ + 1) * TX;
-  static constexpr size_t bytes = sizeof(float) * (size_t(F) * HZ * TX + 2 * size_t(F) * EN + size_t(S) * FN) +
-                                  (size_t(HZ) * TX + 15) / 16 * 16;
+  static constexpr size_t bytes = sizeof(float) * (size_t(F) * HZ * TX + 2 * size_t(F) * EN + size_t(S) * FN);
 };
 
 // The z operator and the stage combination of k_z on a tile of TX columns of
@@ -1054,7 +1052,6 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
   R *EL = H + F * HZ * TX;                   // [F][TZ+2][TX]
   R *ER = EL + F * Sh::EN;
   R *FL = ER + F * Sh::EN;                   // [S][TZ+1][TX]
-  uint8_t *M = reinterpret_cast<uint8_t *>(FL + S * FN);   // [HZ][TX]
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * TX, j = blockIdx.y, k0 = blockIdx.z * TZ;
   const int nx = G.nx, nz = G.nz;
@@ -1064,9 +1061,8 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
   // periodic halos wrap; dynamics_rk.h:780-797).
   auto src_level = [&](int p) { return (p >= 0 && p < nz) ? p : (wall ? clampi(p, nz) : wrapi(p, nz)); };
 
-  // 1. Primitive fields of levels k0-5 .. k0+TZ+4, and which of them lie
-  // beyond the domain.  Columns beyond the domain read its last column; their
-  // results are discarded.
+  // 1. Primitive fields of levels k0-5 .. k0+TZ+4.  Columns beyond the domain
+  // read its last column; their results are discarded.
   for (int it = tid; it < HZ * TX; it += NT) {
     const int r = it / TX, c = it % TX;
     const int p = k0 - 5 + r, lv = src_level(p);
@@ -1080,31 +1076,26 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
     }
 #pragma unroll
     for (int f = 0; f < F; f++) H[(f * HZ + r) * TX + c] = w[f];
-    M[r * TX + c] = (p < 0 || p >= nz) ? uint8_t(1) : uint8_t(0);
   }
   __syncthreads();
 
   // 2. z edges of the cells at positions q = 0 .. TZ+1 (level k0-1+q).  The
-  // immersed bits of a stencil are those of the levels around its canonical
-  // cell (wrapped in periodic z): levels beyond the domain count as immersed
-  // (the z halos of the proportion are 1, dynamics_rk.h:1031-1034).
+  // immersed bits of a stencil are the levels around its canonical cell cc
+  // (wrapped in periodic z) that lie beyond the domain (the z halos of the
+  // proportion are 1, dynamics_rk.h:1031-1034): bits 0..3-cc below, bits
+  // nz+4-cc..8 above.
   auto load = [&](int f, int c, int q, R (&s)[9], unsigned &imm, bool &any10) {
     const R *colh = H + (f * HZ + q) * TX + c;
 #pragma unroll
     for (int m = 0; m < 9; m++) s[m] = colh[m * TX];
     const int L = k0 - 1 + q;
+    // A cell beyond the domain is read in periodic z only (in a wall domain
+    // no face reads it).
+    const int cc = (L >= 0 && L < nz) ? L : wrapi(L, nz);
     imm = 0;
     any10 = false;
-    if (L >= 0 && L < nz) {
-#pragma unroll
-      for (int m = 0; m < 9; m++) imm |= unsigned(M[(q + m) * TX + c]) << m;
-    } else {
-      // A cell beyond the domain: periodic z only (in a wall domain no face
-      // reads it).
-      const int cc = wrapi(L, nz);
-#pragma unroll
-      for (int m = 0; m < 9; m++) imm |= unsigned(cc - 4 + m < 0 || cc - 4 + m >= nz) << m;
-    }
+    if (cc < 4) imm |= (1u << (4 - cc)) - 1u;
+    if (cc > nz - 5) imm |= 0x1ffu & ~((1u << (nz + 4 - cc)) - 1u);
     if (f == iU || f == iV || f == iP) der0_modify(s, imm);
   };
   recon_packed_inner<NT, F, TX, TZ, true>(load, [&](int f, int c, int q, R qL, R qR) {

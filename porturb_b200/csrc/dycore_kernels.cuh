@@ -359,6 +359,36 @@ __device__ __forceinline__ void recon_packed_inner(Load load, Store store) {
     line = POS_MAJOR ? q % LINES : q / W;
     pos = (POS_MAJOR ? q / LINES : q % W) + 1;
   };
+  if constexpr (NT == LINES * W) {
+    // One position per thread: walk its fields in pairs (the same pairs as
+    // below, where stencil it+NT is the next field of stencil it).
+    int f0, line, pos;
+    coords(threadIdx.x, f0, line, pos);
+#pragma unroll 1
+    for (int f = 0; f < F; f += 2) {
+      const bool two = f + 1 < F;
+      float a[9], b[9];
+      unsigned ia, ib;
+      bool xa, xb;
+      load(f, line, pos, a, ia, xa);
+      if (two) {
+        load(f + 1, line, pos, b, ib, xb);
+      } else {
+#pragma unroll
+        for (int m = 0; m < 9; m++) b[m] = a[m];
+        ib = ia;
+        xb = xa;
+      }
+      float2 s2[9], qL, qR;
+#pragma unroll
+      for (int m = 0; m < 9; m++) s2[m] = make_float2(a[m], b[m]);
+      weno9_edges2(s2, qL, qR, bool2{!xa, !xb}, bool2{((ia >> 3) & 1u) != 0, ((ib >> 3) & 1u) != 0},
+                   bool2{((ia >> 5) & 1u) != 0, ((ib >> 5) & 1u) != 0});
+      store(f, line, pos, qL.x, qR.x);
+      if (two) store(f + 1, line, pos, qL.y, qR.y);
+    }
+    return;
+  }
   for (int it = threadIdx.x; it < N_IN; it += 2 * NT) {
     const int it2 = it + NT;
     const bool two = it2 < N_IN;

@@ -114,6 +114,7 @@ struct Grid {
 };
 
 __device__ __forceinline__ int wrapi(int i, int n) {
+  if (unsigned(i) < unsigned(n)) return i;   // inside: no division
   i %= n;
   return i < 0 ? i + n : i;
 }

@@ -349,10 +349,13 @@ __device__ __forceinline__ int recon_learned(const Grid<float> &G, uint32_t *sW,
 // reads.  Per stencil and edge the bits are those of weno9_edges.
 // POS_MAJOR: consecutive threads take consecutive lines at one position (y),
 // else consecutive positions of one line (x).
-// load(f, line, pos, s, imm, any10), store(f, line, pos, qL, qR),
-// store_outer(f, line, qR of position 0, qL of position W+1).
-template <int NT, int F, int LINES, int W, bool POS_MAJOR, class Load, class Store>
-__device__ __forceinline__ void recon_packed_inner(Load load, Store store) {
+// mask(line, pos, imm, any10) gives a position's immersed bits (the same for
+// all fields), vals(f, line, pos, s, imm) a field's stencil with the immersed
+// modification applied; load(f, line, pos, s, imm, any10) is the two
+// together; store(f, line, pos, qL, qR), store_outer(f, line, qR of position
+// 0, qL of position W+1).
+template <int NT, int F, int LINES, int W, bool POS_MAJOR, class Mask, class Vals, class Store>
+__device__ __forceinline__ void recon_packed_inner(Mask mask, Vals vals, Store store) {
   constexpr int N_IN = F * LINES * W;
   auto coords = [](int it, int &f, int &line, int &pos) {
     f = it / (LINES * W);
@@ -365,26 +368,25 @@ __device__ __forceinline__ void recon_packed_inner(Load load, Store store) {
     // below, where stencil it+NT is the next field of stencil it).
     int f0, line, pos;
     coords(threadIdx.x, f0, line, pos);
+    unsigned im;
+    bool ax;
+    mask(line, pos, im, ax);
+    const bool il = ((im >> 3) & 1u) != 0, ir = ((im >> 5) & 1u) != 0;
 #pragma unroll 1
     for (int f = 0; f < F; f += 2) {
       const bool two = f + 1 < F;
       float a[9], b[9];
-      unsigned ia, ib;
-      bool xa, xb;
-      load(f, line, pos, a, ia, xa);
+      vals(f, line, pos, a, im);
       if (two) {
-        load(f + 1, line, pos, b, ib, xb);
+        vals(f + 1, line, pos, b, im);
       } else {
 #pragma unroll
         for (int m = 0; m < 9; m++) b[m] = a[m];
-        ib = ia;
-        xb = xa;
       }
       float2 s2[9], qL, qR;
 #pragma unroll
       for (int m = 0; m < 9; m++) s2[m] = make_float2(a[m], b[m]);
-      weno9_edges2(s2, qL, qR, bool2{!xa, !xb}, bool2{((ia >> 3) & 1u) != 0, ((ib >> 3) & 1u) != 0},
-                   bool2{((ia >> 5) & 1u) != 0, ((ib >> 5) & 1u) != 0});
+      weno9_edges2(s2, qL, qR, bool2{!ax, !ax}, bool2{il, il}, bool2{ir, ir});
       store(f, line, pos, qL.x, qR.x);
       if (two) store(f + 1, line, pos, qL.y, qR.y);
     }
@@ -398,10 +400,12 @@ __device__ __forceinline__ void recon_packed_inner(Load load, Store store) {
     float a[9], b[9];
     unsigned ia, ib;
     bool xa, xb;
-    load(fa, la, pa, a, ia, xa);
+    mask(la, pa, ia, xa);
+    vals(fa, la, pa, a, ia);
     if (two) {
       coords(it2, fb, lb, pb);
-      load(fb, lb, pb, b, ib, xb);
+      mask(lb, pb, ib, xb);
+      vals(fb, lb, pb, b, ib);
     } else {
 #pragma unroll
       for (int m = 0; m < 9; m++) b[m] = a[m];
@@ -519,18 +523,24 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
   }
 
   // 2. x edges of cells -1..TX of every tile row (position c = cell + 1).
-  auto load_xc = [&](int f, int r, int c, R (&s)[9], unsigned &imm, bool &any10) {
-    const R *row = H + (f * HY + 5 + r) * HX + c;
-#pragma unroll
-    for (int m = 0; m < 9; m++) s[m] = row[m];
+  auto mask_xc = [&](int r, int c, unsigned &imm, bool &any10) {
     imm = 0;
     any10 = false;
     if (IMM) {
       const unsigned e = MX[r * (TX + 2) + c];
       imm = e & 0x1ffu;
       any10 = (e & 0x200u) != 0;
-      if (f == iV || f == iW || f == iP) der0_modify(s, imm);
     }
+  };
+  auto vals_xc = [&](int f, int r, int c, R (&s)[9], unsigned imm) {
+    const R *row = H + (f * HY + 5 + r) * HX + c;
+#pragma unroll
+    for (int m = 0; m < 9; m++) s[m] = row[m];
+    if (IMM && (f == iV || f == iW || f == iP)) der0_modify(s, imm);
+  };
+  auto load_xc = [&](int f, int r, int c, R (&s)[9], unsigned &imm, bool &any10) {
+    mask_xc(r, c, imm, any10);
+    vals_xc(f, r, c, s, imm);
   };
   auto store_xc = [&](int f, int r, int c, R qL, R qR) {
     EL[f * EN + r * (TX + 2) + c] = qL;
@@ -541,18 +551,24 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
     load_xc(f, rem / (TX + 2), rem % (TX + 2), s, imm, any10);
   };
   // y stencil of cell rr-1 of tile column cc (position rr = 0..TY+1).
-  auto load_yc = [&](int f, int cc, int rr, R (&s)[9], unsigned &imm, bool &any10) {
-    const R *col = H + (f * HY + rr) * HX + 5 + cc;
-#pragma unroll
-    for (int m = 0; m < 9; m++) s[m] = col[m * HX];
+  auto mask_yc = [&](int cc, int rr, unsigned &imm, bool &any10) {
     imm = 0;
     any10 = false;
     if (IMM) {
       const unsigned e = MY[rr * TX + cc];
       imm = e & 0x1ffu;
       any10 = (e & 0x200u) != 0;
-      if (f == iU || f == iW || f == iP) der0_modify(s, imm);
     }
+  };
+  auto vals_yc = [&](int f, int cc, int rr, R (&s)[9], unsigned imm) {
+    const R *col = H + (f * HY + rr) * HX + 5 + cc;
+#pragma unroll
+    for (int m = 0; m < 9; m++) s[m] = col[m * HX];
+    if (IMM && (f == iU || f == iW || f == iP)) der0_modify(s, imm);
+  };
+  auto load_yc = [&](int f, int cc, int rr, R (&s)[9], unsigned &imm, bool &any10) {
+    mask_yc(cc, rr, imm, any10);
+    vals_yc(f, cc, rr, s, imm);
   };
   auto store_x = [&](int it, R qL, R qR) {
     const int f = it / Sh::EXN, rem = it % Sh::EXN;
@@ -564,7 +580,7 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
   if constexpr (std::is_same<R, float>::value && PU_PACKED_LIMITER && !LEARNED) {
     packed = G.weno_all != 0;
     if (packed) {
-      recon_packed_inner<NT, F, TY, TX, false>(load_xc, store_xc);
+      recon_packed_inner<NT, F, TY, TX, false>(mask_xc, vals_xc, store_xc);
       // Halo pairs of the x lines, and already those of the y lines (kept in
       // YO until the y phase), so that every thread takes one pair here and
       // the y phase is the inner rounds alone.
@@ -649,7 +665,7 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
       n_fb += recon_learned<NT>(G, sW, queue, qn + 1, F * Sh::EYN, load_y, store_y);
     } else if (packed) {
       if constexpr (std::is_same<R, float>::value) {
-        recon_packed_inner<NT, F, TX, TY, true>(load_yc, [&](int f, int cc, int rr, R qL, R qR) {
+        recon_packed_inner<NT, F, TX, TY, true>(mask_yc, vals_yc, [&](int f, int cc, int rr, R qL, R qR) {
           EL[f * EN + rr * TX + cc] = qL;
           ER[f * EN + rr * TX + cc] = qR;
         });
@@ -1115,10 +1131,7 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
   // (wrapped in periodic z) that lie beyond the domain (the z halos of the
   // proportion are 1, dynamics_rk.h:1031-1034): bits 0..3-cc below, bits
   // nz+4-cc..8 above.
-  auto load = [&](int f, int c, int q, R (&s)[9], unsigned &imm, bool &any10) {
-    const R *colh = H + (f * HZ + q) * TX + c;
-#pragma unroll
-    for (int m = 0; m < 9; m++) s[m] = colh[m * TX];
+  auto mask = [&](int, int q, unsigned &imm, bool &any10) {
     const int L = k0 - 1 + q;
     // A cell beyond the domain is read in periodic z only (in a wall domain
     // no face reads it).
@@ -1127,9 +1140,18 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
     any10 = false;
     if (cc < 4) imm |= (1u << (4 - cc)) - 1u;
     if (cc > nz - 5) imm |= 0x1ffu & ~((1u << (nz + 4 - cc)) - 1u);
+  };
+  auto vals = [&](int f, int c, int q, R (&s)[9], unsigned imm) {
+    const R *colh = H + (f * HZ + q) * TX + c;
+#pragma unroll
+    for (int m = 0; m < 9; m++) s[m] = colh[m * TX];
     if (f == iU || f == iV || f == iP) der0_modify(s, imm);
   };
-  recon_packed_inner<NT, F, TX, TZ, true>(load, [&](int f, int c, int q, R qL, R qR) {
+  auto load = [&](int f, int c, int q, R (&s)[9], unsigned &imm, bool &any10) {
+    mask(c, q, imm, any10);
+    vals(f, c, q, s, imm);
+  };
+  recon_packed_inner<NT, F, TX, TZ, true>(mask, vals, [&](int f, int c, int q, R qL, R qR) {
     EL[(f * (TZ + 2) + q) * TX + c] = qL;
     ER[(f * (TZ + 2) + q) * TX + c] = qR;
   });

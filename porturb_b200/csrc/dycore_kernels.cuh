@@ -373,22 +373,24 @@ __device__ __forceinline__ void recon_packed_inner(Mask mask, Vals vals, Store s
     mask(line, pos, im, ax);
     const bool il = ((im >> 3) & 1u) != 0, ir = ((im >> 5) & 1u) != 0;
 #pragma unroll 1
-    for (int f = 0; f < F; f += 2) {
-      const bool two = f + 1 < F;
+    for (int f = 0; f + 1 < F; f += 2) {
       float a[9], b[9];
       vals(f, line, pos, a, im);
-      if (two) {
-        vals(f + 1, line, pos, b, im);
-      } else {
-#pragma unroll
-        for (int m = 0; m < 9; m++) b[m] = a[m];
-      }
+      vals(f + 1, line, pos, b, im);
       float2 s2[9], qL, qR;
 #pragma unroll
       for (int m = 0; m < 9; m++) s2[m] = make_float2(a[m], b[m]);
       weno9_edges2(s2, qL, qR, bool2{!ax, !ax}, bool2{il, il}, bool2{ir, ir});
       store(f, line, pos, qL.x, qR.x);
-      if (two) store(f + 1, line, pos, qL.y, qR.y);
+      store(f + 1, line, pos, qL.y, qR.y);
+    }
+    if constexpr (F % 2 == 1) {
+      // The odd field alone through the scalar limiter (the same bits): a
+      // packed pair with an idle lane would cost the FMA pipe as much as two.
+      float a[9], qL, qR;
+      vals(F - 1, line, pos, a, im);
+      weno9_edges(a, qL, qR, !ax, il, ir);
+      store(F - 1, line, pos, qL, qR);
     }
     return;
   }

@@ -392,36 +392,36 @@ __device__ __forceinline__ void recon_packed_inner(Mask mask, Vals vals, Store s
       weno9_edges(a, qL, qR, !ax, il, ir);
       store(F - 1, line, pos, qL, qR);
     }
-    return;
-  }
-  for (int it = threadIdx.x; it < N_IN; it += 2 * NT) {
-    const int it2 = it + NT;
-    const bool two = it2 < N_IN;
-    int fa, la, pa, fb, lb, pb;
-    coords(it, fa, la, pa);
-    float a[9], b[9];
-    unsigned ia, ib;
-    bool xa, xb;
-    mask(la, pa, ia, xa);
-    vals(fa, la, pa, a, ia);
-    if (two) {
-      coords(it2, fb, lb, pb);
-      mask(lb, pb, ib, xb);
-      vals(fb, lb, pb, b, ib);
-    } else {
+  } else {
+    for (int it = threadIdx.x; it < N_IN; it += 2 * NT) {
+      const int it2 = it + NT;
+      const bool two = it2 < N_IN;
+      int fa, la, pa, fb, lb, pb;
+      coords(it, fa, la, pa);
+      float a[9], b[9];
+      unsigned ia, ib;
+      bool xa, xb;
+      mask(la, pa, ia, xa);
+      vals(fa, la, pa, a, ia);
+      if (two) {
+        coords(it2, fb, lb, pb);
+        mask(lb, pb, ib, xb);
+        vals(fb, lb, pb, b, ib);
+      } else {
 #pragma unroll
-      for (int m = 0; m < 9; m++) b[m] = a[m];
-      ib = ia;
-      xb = xa;
-      fb = fa, lb = la, pb = pa;
+        for (int m = 0; m < 9; m++) b[m] = a[m];
+        ib = ia;
+        xb = xa;
+        fb = fa, lb = la, pb = pa;
+      }
+      float2 s2[9], qL, qR;
+#pragma unroll
+      for (int m = 0; m < 9; m++) s2[m] = make_float2(a[m], b[m]);
+      weno9_edges2(s2, qL, qR, bool2{!xa, !xb}, bool2{((ia >> 3) & 1u) != 0, ((ib >> 3) & 1u) != 0},
+                   bool2{((ia >> 5) & 1u) != 0, ((ib >> 5) & 1u) != 0});
+      store(fa, la, pa, qL.x, qR.x);
+      if (two) store(fb, lb, pb, qL.y, qR.y);
     }
-    float2 s2[9], qL, qR;
-#pragma unroll
-    for (int m = 0; m < 9; m++) s2[m] = make_float2(a[m], b[m]);
-    weno9_edges2(s2, qL, qR, bool2{!xa, !xb}, bool2{((ia >> 3) & 1u) != 0, ((ib >> 3) & 1u) != 0},
-                 bool2{((ia >> 5) & 1u) != 0, ((ib >> 5) & 1u) != 0});
-    store(fa, la, pa, qL.x, qR.x);
-    if (two) store(fb, lb, pb, qL.y, qR.y);
   }
 }
 
@@ -1067,13 +1067,13 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : (s
 }
 
 // Shared memory of k_zt: primitive fields of the tile's columns at levels
-// k0-5 .. k0+TZ+4, left/right z edges of the cells at levels k0-1 .. k0+TZ,
-// and the fluxes on faces k0 .. k0+TZ.
+// k0-5 .. k0+TZ+4 and the left/right z edges of the cells at levels
+// k0-1 .. k0+TZ.
 template <int NTR, int TX, int TZ>
 struct ZTShape {
   static constexpr int F = 6 + NTR, S = 5 + NTR, NT = TX * TZ, HZ = TZ + 10;
-  static constexpr int EN = (TZ + 2) * TX, FN = (TZ + 1) * TX;
-  static constexpr size_t bytes = sizeof(float) * (size_t(F) * HZ * TX + 2 * size_t(F) * EN + size_t(S) * FN);
+  static constexpr int EN = (TZ + 2) * TX;
+  static constexpr size_t bytes = sizeof(float) * (size_t(F) * HZ * TX + 2 * size_t(F) * EN);
 };
 
 // The z operator and the stage combination of k_z on a tile of TX columns of
@@ -1095,12 +1095,11 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
                                                                int n_enforce) {
   using R = float;
   using Sh = ZTShape<NTR, TX, TZ>;
-  constexpr int F = Sh::F, S = Sh::S, NT = Sh::NT, HZ = Sh::HZ, FN = Sh::FN;
+  constexpr int F = Sh::F, S = Sh::S, NT = Sh::NT, HZ = Sh::HZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R *H = reinterpret_cast<R *>(smem_raw);   // [F][HZ][TX]
   R *EL = H + F * HZ * TX;                   // [F][TZ+2][TX]
   R *ER = EL + F * Sh::EN;
-  R *FL = ER + F * Sh::EN;                   // [S][TZ+1][TX]
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * TX, j = blockIdx.y, k0 = blockIdx.z * TZ;
   const int nx = G.nx, nz = G.nz;
@@ -1164,11 +1163,16 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
     });
   __syncthreads();
 
-  // 3. Riemann fluxes on faces k0 .. k0+TZ (face fz+k0 between the cells at
-  // positions fz and fz+1; edge_exchange z, dynamics_rk.h:891-908).
-  for (int it = tid; it < FN; it += NT) {
-    const int fz = it / TX, c = it % TX, cf = k0 + fz;
-    if (cf > nz) continue;
+  // 3. Each thread takes the Riemann fluxes through the two faces of its
+  // cell (face k0+fz lies between the cells at positions fz and fz+1;
+  // edge_exchange z, dynamics_rk.h:891-908) -- each inner face is computed
+  // by the two cells beside it, with the same bits, which spares a block
+  // barrier -- then the divergence, sources, stage combination and
+  // enforcement of the cell.
+  const int c = tid % TX, kz = tid / TX, k = k0 + kz, gi = i0 + c;
+  if (gi >= nx || k >= nz) return;
+  auto face_flux = [&](int fz, R (&fl)[S]) {
+    const int cf = k0 + fz;
     R Lf[F], Rf[F];
     if (wall && cf == 0) {
 #pragma unroll
@@ -1185,23 +1189,18 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
         Rf[f] = EL[(f * (TZ + 2) + fz + 1) * TX + c];
       }
     }
-    R fl[S];
     riemann<R, NTR>(Lf, Rf, __ldg(G.rho_e + cf), __ldg(G.theta_e + cf), iW, fl);
-#pragma unroll
-    for (int s2 = 0; s2 < S; s2++) FL[s2 * FN + it] = fl[s2];
-  }
-  __syncthreads();
-
-  // 4. Divergence, sources, stage combination and enforcement of one cell.
-  const int c = tid % TX, kz = tid / TX, k = k0 + kz, gi = i0 + c;
-  if (gi >= nx || k >= nz) return;
+  };
+  R Fb[S], Ft[S], dF[S];
+  face_flux(kz, Fb);
+  face_flux(kz + 1, Ft);
   const size_t idx = size_t(k) * NP + row + gi;
-  R qin[S], tx[S], dF[S];
+  R qin[S], tx[S];
 #pragma unroll
   for (int s2 = 0; s2 < S; s2++) {
     qin[s2] = sin[s2 * G.N + idx];
     tx[s2] = txy[s2 * G.N + idx];
-    dF[s2] = FL[s2 * FN + (kz + 1) * TX + c] - FL[s2 * FN + kz * TX + c];
+    dF[s2] = __fsub_rn(Ft[s2], Fb[s2]);   // not fused with the flux products: the march's bits
   }
   finish_cell<R, NTR, false>(G, qin, tx, [&](int s2) { return sn[s2 * G.N + idx]; }, dF, sn != nullptr, a_n, a_dt,
                              n_enforce, idx, k, sout);

@@ -360,7 +360,6 @@ __global__ void k_weno9_eval(const float *__restrict__ s, const unsigned char *_
 #pragma unroll
     for (int m = 0; m < 9; m++) st[m] = make_float2(s[a * 9 + m], s[bb * 9 + m]);
     const unsigned fa = flags ? flags[a] : 1u, fb = flags ? flags[bb] : 1u;
-    float2 L, R;
     const pu::bool2 mp{(fa & 1u) != 0, (fb & 1u) != 0}, il{(fa & 2u) != 0, (fb & 2u) != 0},
         ir{(fa & 4u) != 0, (fb & 4u) != 0};
     if constexpr (VARIANT == 1) {

@@ -1069,11 +1069,14 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : (s
 // Shared memory of k_zt: primitive fields of the tile's columns at levels
 // k0-5 .. k0+TZ+4 and the left/right z edges of the cells at levels
 // k0-1 .. k0+TZ.
-template <int NTR, int TX, int TZ>
+template <int NTR, int TX, int TZ, bool IMM = false>
 struct ZTShape {
   static constexpr int F = 6 + NTR, S = 5 + NTR, NT = TX * TZ, HZ = TZ + 10;
   static constexpr int EN = (TZ + 2) * TX;
-  static constexpr size_t bytes = sizeof(float) * (size_t(F) * HZ * TX + 2 * size_t(F) * EN);
+  // Immersed domains add one flag byte per level and column (bit 0 immersed,
+  // bit 1 an immersed cell within 10).
+  static constexpr size_t bytes = sizeof(float) * (size_t(F) * HZ * TX + 2 * size_t(F) * EN) +
+                                  (IMM ? (size_t(HZ) * TX + 15) / 16 * 16 : 0);
 };
 
 // The z operator and the stage combination of k_z on a tile of TX columns of
@@ -1083,23 +1086,23 @@ struct ZTShape {
 // primitive fields of levels k0-5 .. k0+TZ+4 go to shared memory; the z edges
 // of the TZ inner cells of each column come from the packed limiter two
 // stencils per thread, the two cells that close a column (k0-1: right edge,
-// k0+TZ: left edge) from its one-edge form; then the Riemann fluxes on faces
-// k0 .. k0+TZ, and each thread finalises one cell.  FP32 with weno_all and
-// no immersed cells; every other form keeps the march (with immersed cells
-// the per-stencil flags and enforcement cost this schedule more than it
-// gains: 0.968 against 0.914 ms on a 256x256x128 urban canopy).
-template <int NTR, int TX, int TZ>
+// k0+TZ: left edge) from its one-edge form; then each thread takes the
+// Riemann fluxes through the two faces of its cell and finalises it.  FP32
+// with weno_all (IMM: domains with immersed cells, whose level flags go to
+// shared memory with the fields); every other form keeps the march.
+template <int NTR, int TX, int TZ, bool IMM>
 __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<float> G, const float *__restrict__ sin,
                                                                const float *sn, float *sout,
                                                                const float *__restrict__ txy, float a_n, float a_dt,
                                                                int n_enforce) {
   using R = float;
-  using Sh = ZTShape<NTR, TX, TZ>;
+  using Sh = ZTShape<NTR, TX, TZ, IMM>;
   constexpr int F = Sh::F, S = Sh::S, NT = Sh::NT, HZ = Sh::HZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R *H = reinterpret_cast<R *>(smem_raw);   // [F][HZ][TX]
   R *EL = H + F * HZ * TX;                   // [F][TZ+2][TX]
   R *ER = EL + F * Sh::EN;
+  uint8_t *M = reinterpret_cast<uint8_t *>(ER + F * Sh::EN);   // [HZ][TX], immersed domains
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * TX, j = blockIdx.y, k0 = blockIdx.z * TZ;
   const int nx = G.nx, nz = G.nz;
@@ -1124,6 +1127,14 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
     }
 #pragma unroll
     for (int f = 0; f < F; f++) H[(f * HZ + r) * TX + c] = w[f];
+    if (IMM) {
+      uint8_t fl = 0;
+      if (p >= 0 && p < nz) {
+        const uint8_t g = __ldg(G.flags + size_t(p) * NP + col);
+        fl = uint8_t(((g & FLAG_IMM) ? 1 : 0) | ((g & FLAG_ANY10) ? 2 : 0));
+      }
+      M[r * TX + c] = fl;
+    }
   }
   __syncthreads();
 
@@ -1132,15 +1143,31 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
   // (wrapped in periodic z) that lie beyond the domain (the z halos of the
   // proportion are 1, dynamics_rk.h:1031-1034): bits 0..3-cc below, bits
   // nz+4-cc..8 above.
-  auto mask = [&](int, int q, unsigned &imm, bool &any10) {
+  auto mask = [&](int c, int q, unsigned &imm, bool &any10) {
     const int L = k0 - 1 + q;
     // A cell beyond the domain is read in periodic z only (in a wall domain
     // no face reads it).
-    const int cc = (L >= 0 && L < nz) ? L : wrapi(L, nz);
+    const bool inside = L >= 0 && L < nz;
+    const int cc = inside ? L : wrapi(L, nz);
     imm = 0;
     any10 = false;
     if (cc < 4) imm |= (1u << (4 - cc)) - 1u;
     if (cc > nz - 5) imm |= 0x1ffu & ~((1u << (nz + 4 - cc)) - 1u);
+    if (IMM) {
+      if (inside) {
+#pragma unroll
+        for (int m = 0; m < 9; m++) imm |= (unsigned(M[(q + m) * TX + c]) & 1u) << m;
+        any10 = (M[(q + 4) * TX + c] & 2u) != 0;
+      } else {
+        const size_t col = row + min(i0 + c, nx - 1);
+#pragma unroll
+        for (int m = 0; m < 9; m++) {
+          const int p = cc - 4 + m;
+          if (p >= 0 && p < nz) imm |= ((__ldg(G.flags + size_t(p) * NP + col) & FLAG_IMM) ? 1u : 0u) << m;
+        }
+        any10 = (__ldg(G.flags + size_t(cc) * NP + col) & FLAG_ANY10) != 0;
+      }
+    }
   };
   auto vals = [&](int f, int c, int q, R (&s)[9], unsigned imm) {
     const R *colh = H + (f * HZ + q) * TX + c;
@@ -1202,8 +1229,8 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
     tx[s2] = txy[s2 * G.N + idx];
     dF[s2] = __fsub_rn(Ft[s2], Fb[s2]);   // not fused with the flux products: the march's bits
   }
-  finish_cell<R, NTR, false>(G, qin, tx, [&](int s2) { return sn[s2 * G.N + idx]; }, dF, sn != nullptr, a_n, a_dt,
-                             n_enforce, idx, k, sout);
+  finish_cell<R, NTR, IMM>(G, qin, tx, [&](int s2) { return sn[s2 * G.N + idx]; }, dF, sn != nullptr, a_n, a_dt,
+                           n_enforce, idx, k, sout);
 }
 
 // a += b elementwise.

@@ -575,8 +575,10 @@ struct Impl : ImplBase {
     PU_CK(cudaFuncSetAttribute(k_z<R, NTR, ZTX, ZTY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                int(ZShape<R, NTR, ZTX, ZTY>::bytes)));
     if constexpr (std::is_same<R, float>::value) {
-      PU_CK(cudaFuncSetAttribute(k_zt<NTR, ZT_X, ZT_Z>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(ZTShape<NTR, ZT_X, ZT_Z>::bytes)));
+      PU_CK(cudaFuncSetAttribute(k_zt<NTR, ZT_X, ZT_Z, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(ZTShape<NTR, ZT_X, ZT_Z, false>::bytes)));
+      PU_CK(cudaFuncSetAttribute(k_zt<NTR, ZT_X, ZT_Z, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(ZTShape<NTR, ZT_X, ZT_Z, true>::bytes)));
       PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, LTX, LTY, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(XYShape<R, NTR, LTX, LTY, false, true>::bytes)));
       PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, LTX, LTY, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -833,9 +835,8 @@ struct Impl : ImplBase {
     return check_err();
   }
 
-  // The tiled z kernel (k_zt) takes the plain FP32 limiter with weno_all on
-  // domains without immersed cells, unless a z chunk was asked for (the
-  // march, which gives the same bits).  Its grid has one y row per block
+  // The tiled z kernel (k_zt) takes the plain FP32 limiter with weno_all,
+  // unless a z chunk was asked for (the march, which gives the same bits).  Its grid has one y row per block
   // row, so ny is held to the grid's y limit.
   bool z_tiled(bool learned) const {
     return std::is_same<R, float>::value && cfg.weno_all && !learned && cfg.z_chunk <= 0 && cfg.ny <= 65535;
@@ -873,9 +874,9 @@ struct Impl : ImplBase {
     dim3 gz(blocks(cfg.nx, ZTX), blocks(cfg.ny, ZTY), blocks(cfg.nz, kc));
     cudaEvent_t e1 = prof_begin();
     if constexpr (std::is_same<R, float>::value) {
-      if (!IMM && z_tiled(L)) {
+      if (z_tiled(L)) {
         dim3 gt(blocks(cfg.nx, ZT_X), cfg.ny, blocks(cfg.nz, ZT_Z));
-        k_zt<NTR, ZT_X, ZT_Z><<<gt, ZT_X * ZT_Z, ZTShape<NTR, ZT_X, ZT_Z>::bytes, st>>>(G, sin, sn, sout, t, a_n,
+        k_zt<NTR, ZT_X, ZT_Z, IMM><<<gt, ZT_X * ZT_Z, ZTShape<NTR, ZT_X, ZT_Z, IMM>::bytes, st>>>(G, sin, sn, sout, t, a_n,
                                                                                            a_dt, n_enforce);
         PU_LAUNCHED();
         prof_end(1, e1);

@@ -1,12 +1,12 @@
 """The tiled z kernel (k_zt: 8 columns x 32 levels per block, the default
-for FP32 with weno_all on domains without immersed cells) gives the bits of
-the z march (k_z, selected by an explicit z chunk): the same primitive
-fields, wall and periodic halos, wall-adjacent stencil modifications, face
-states, limiter bits per stencil, Riemann fluxes, stage combination and
-positivity clip.  Cases: walls, periodic z, three tracers (an odd number of
-fields), precursor x/y, Coriolis, a 2-D domain, the warm bubble, and grids
-whose x and z extents are not multiples of the tile (partial tiles, several
-z tiles)."""
+for FP32 with weno_all) gives the bits of the z march (k_z, selected by an
+explicit z chunk): the same primitive fields, wall and periodic halos,
+immersed and wall-adjacent stencil modifications, face states, limiter bits
+per stencil, Riemann fluxes, stage combination, immersed relaxation and
+positivity clip.  Cases: walls with and without an immersed cuboid,
+periodic z, three tracers (an odd number of fields), precursor x/y,
+Coriolis, a 2-D domain, the warm bubble, and grids whose x and z extents
+are not multiples of the tile (partial tiles, several z tiles)."""
 import numpy as np
 import pytest
 
@@ -17,6 +17,9 @@ pytestmark = pytest.mark.gpu
 
 CASES = {
     "walls": lambda: cases.small_mixed(immersed=False),
+    "walls_immersed": lambda: cases.small_mixed(),
+    "periodic_z_immersed": lambda: cases.small_mixed(bc_z="periodic", nz=40),
+    "partial_tiles_immersed": lambda: cases.small_mixed(nx=37, ny=6, nz=75),
     "periodic_z": lambda: cases.small_mixed(bc_z="periodic", immersed=False),
     "periodic_z_tall": lambda: cases.small_mixed(bc_z="periodic", nz=70, immersed=False),
     "three_tracers": lambda: cases.small_mixed(ntr=3, immersed=False),

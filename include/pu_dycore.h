@@ -76,7 +76,9 @@ typedef struct pu_config {
   int weno_mode;                           /* pu_weno_mode */
   int device;                              /* CUDA device ordinal */
   void *stream;                            /* cudaStream_t, or NULL */
-  int z_chunk;                             /* levels per z-march work item; 0 = auto */
+  int z_chunk;                             /* 0: the tiled z kernel (FP32 with weno_all) or the z
+                                              march with its own chunk; > 0: the z march with
+                                              this many levels per work item (the same results) */
 } pu_config;
 
 /* The coupler-side state: density_dry, uvel, vvel, wvel, temp and the tracer

@@ -1141,8 +1141,8 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
   // 2. z edges of the cells at positions q = 0 .. TZ+1 (level k0-1+q).  The
   // immersed bits of a stencil are the levels around its canonical cell cc
   // (wrapped in periodic z) that lie beyond the domain (the z halos of the
-  // proportion are 1, dynamics_rk.h:1031-1034): bits 0..3-cc below, bits
-  // nz+4-cc..8 above.
+  // proportion are 1, dynamics_rk.h:1031-1034: bits 0..3-cc below, bits
+  // nz+4-cc..8 above) or, with IMM, hold an immersed cell.
   auto mask = [&](int c, int q, unsigned &imm, bool &any10) {
     const int L = k0 - 1 + q;
     // A cell beyond the domain is read in periodic z only (in a wall domain

@@ -273,9 +273,15 @@ int pu_dycore_profile_read(pu_dycore *h, pu_profile *out);
  *     holds until the process exits; grids that need more return
  *     PU_ERR_UNSUPPORTED (about 110 bytes per cell with two tracers, i.e. up
  *     to roughly 600k cells);
+ *   - the configuration does not say whether the domain has immersed cells,
+ *     and this call cannot detect them: on an urban or turbine domain it
+ *     returns the step of the same grid without immersed cells (no error);
+ *     such domains need pu_dycore_time_step;
  *   - the first call on a device looks up that array's device address
- *     (cudaGetSymbolAddress, with the device current); make that first call
- *     before any stream capture;
+ *     (cudaGetSymbolAddress, with the device current) and keeps it; make that
+ *     first call before any stream capture.  Resetting the device
+ *     (cudaDeviceReset) while the library is loaded is not supported: the
+ *     kept address would belong to the context that the reset destroyed;
  *   - every call shares the one array and it keeps the previous call's
  *     contents (only the error word is cleared per call), so calls whose GPU
  *     work overlaps -- on different streams or host threads -- race;
@@ -301,6 +307,16 @@ int pu_dycore_time_step_noalloc(const pu_config *cfg, const double *hy_dens_cell
  * Host or device arrays (mem); synchronous, on the current device. */
 int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long long n, int variant, float *qL,
                        float *qR, int mem);
+
+/* The learned weights' input convention on n stencils of 9 floats (host
+ * arrays; synchronous, on the current device): x = (s - min)/(max - min), all
+ * zeros when max - min <= 1e-20, and jump = the largest |x[m+1] - x[m]|, the
+ * acceptance check of the learned path.  It follows the limiter's normalize
+ * (WenoLimiter.h:85-96, threshold 1e-20), the form of the dycore's unused
+ * normalize (dynamics_rk.h:42-53, which floors the range at 1e-10 instead);
+ * the scale is applied as a multiply by the correctly rounded reciprocal of
+ * the range. */
+int pu_learned_normalize_f32(const float *stencils, long long n, float *x, float *jump);
 
 /* ---------------------------------------------------------------------------
  * Domain decomposition across GPUs (coupler.h:132-229): a handle can be one

@@ -17,7 +17,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libporturb_ref.so")
-REFERENCE_DIR = "/root/reference"
+# The reference tree: $PORTURB_REFERENCE, by default where this image mounts it.
+REFERENCE_DIR = os.environ.get("PORTURB_REFERENCE", "/root/reference")
 
 MAX_TRACERS = 16
 BC = {"periodic": 0, "precursor": 1, "solid_wall": 2}

@@ -3,8 +3,8 @@
 //
 // The reference's dycore headers (model/modules/dynamics_rk.h,
 // helpers/WenoLimiter.h, helpers/TransformMatrices.h and core/MultipleFields.h)
-// are compiled unchanged against this file, from where they lie, by
-// oracle/build_ref.sh.  Their external dependencies (YAKL, Kokkos, MPI,
+// are compiled unchanged against this file, from where they lie, by the
+// `ref` target of oracle/Makefile.  Their external dependencies (YAKL, Kokkos, MPI,
 // PNetCDF, yaml-cpp) are empty submodules in the reference tree, so this shim
 // supplies, for one host process:
 //   * yakl::SArray     -- fixed-size array, C order, (i,j,...) indexing

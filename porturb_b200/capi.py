@@ -144,6 +144,7 @@ SIGNATURES = {
     "pu_dycore_time_step_noalloc": (_I, [C.POINTER(pu_config), _P, _P, _P, C.POINTER(pu_state_view), _D,
                                          C.POINTER(_I)]),
     "pu_weno9_edges_f32": (_I, [_P, _P, C.c_longlong, _I, _P, _P, _I]),
+    "pu_learned_normalize_f32": (_I, [_P, C.c_longlong, _P, _P]),
     "pu_decomp_process_grid": (_I, [_I, C.c_longlong, C.c_longlong, C.POINTER(_I), C.POINTER(_I)]),
     "pu_decomp_tile": (_I, [C.c_longlong, _I, _I, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "pu_decomp_neighbors": (_I, [C.POINTER(pu_decomp), C.POINTER(_I)]),

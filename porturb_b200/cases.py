@@ -87,6 +87,19 @@ class Case:
             rd, T = self.perturbed["rho_d"], self.perturbed["temp"]
         return rd, self.uvel, self.vvel, self.wvel, T, self.tracer_data
 
+    def block(self, i0: int, j0: int, nx: int, ny: int) -> "Case":
+        """The columns [i0, i0+nx) x [j0, j0+ny) of this case as a case of its
+        own (copies; same spacing, levels and options; its lateral boundaries
+        are whatever the options say, periodic for the generators here)."""
+        xs, ys = slice(i0, i0 + nx), slice(j0, j0 + ny)
+        cut = lambda a: np.ascontiguousarray(a[..., ys, xs])
+        pert = None if self.perturbed is None else {k: cut(v) for k, v in self.perturbed.items()}
+        return Case(name="%s_block" % self.name, nx=nx, ny=ny, nz=self.nz, xlen=self.xlen * nx / self.nx,
+                    ylen=self.ylen * ny / self.ny, zlen=self.zlen, options=dict(self.options),
+                    tracers=list(self.tracers), rho_d=cut(self.rho_d), uvel=cut(self.uvel), vvel=cut(self.vvel),
+                    wvel=cut(self.wvel), temp=cut(self.temp), tracer_data=cut(self.tracer_data),
+                    immersed_proportion=cut(self.immersed_proportion), perturbed=pert, steps=self.steps)
+
 
 def splitmix64_uniform(seed: int, index: np.ndarray) -> np.ndarray:
     """Uniform [0,1) doubles from splitmix64(seed * 2^32 + index)."""
@@ -199,22 +212,29 @@ def abl_neutral(nx=256, ny=256, nz=128, dx=10.0, theta0=300.0, z_inv=500.0, laps
 
 
 def urban_canopy(nx=512, ny=512, nz=128, dx=2.0, theta0=300.0, lot=40.0, foot=(20.0, 32.0), height=(10.0, 60.0),
-                 occupancy=0.7, noise_amp=0.1, seed=0, cfl=0.6, steps=1000, u0=10.0) -> Case:
+                 occupancy=0.7, noise_amp=0.1, seed=0, cfl=0.6, steps=1000, u0=10.0, window=None) -> Case:
     """Immersed-boundary urban canopy: seeded cuboid buildings, one per
     occupied 40 m lot, footprints U[20,32] m, heights U[10,60] m, 70 % lot
     occupancy, a binary immersed mask, theta = 300 K with seeded +-0.1 K noise
-    applied after init, and a uniform 10 m/s initial flow outside buildings."""
+    applied after init, and a uniform 10 m/s initial flow outside buildings.
+
+    window = (i0, j0, bx, by) gives only the columns [i0, i0+bx) x [j0, j0+by)
+    of the nx x ny domain, as a case of its own (the same buildings and noise,
+    which are keyed by lot and by global cell index), without forming the rest."""
+    i0, j0, bx, by = window if window is not None else (0, 0, nx, ny)
+    if not (0 <= i0 and i0 + bx <= nx and 0 <= j0 and j0 + by <= ny and bx > 0 and by > 0):
+        raise ValueError("window outside the domain")
     opts = default_options(cfl=cfl)
     tr = [Tracer("water_vapor", "water_vapor", True, True, True)]
-    b = _base("urban_canopy", nx, ny, nz, nx * dx, ny * dx, nz * dx, tr, opts)
+    b = _base("urban_canopy", bx, by, nz, bx * dx, by * dx, nz * dx, tr, opts)
     xlen, ylen = nx * dx, ny * dx
     nlx, nly = int(xlen // lot), int(ylen // lot)
     rng_idx = np.arange(nlx * nly * 5, dtype=np.uint64)
     r = splitmix64_uniform(seed + 1, rng_idx).reshape(nly, nlx, 5)
-    xc = (np.arange(nx) + 0.5) * dx
-    yc = (np.arange(ny) + 0.5) * dx
+    xc = (np.arange(i0, i0 + bx) + 0.5) * dx
+    yc = (np.arange(j0, j0 + by) + 0.5) * dx
     zc = (np.arange(nz) + 0.5) * dx
-    mask = np.zeros((nz, ny, nx))
+    mask = np.zeros((nz, by, bx))
     for jl in range(nly):
         for il in range(nlx):
             occ, fx, fy, h, _ = r[jl, il]
@@ -226,17 +246,22 @@ def urban_canopy(nx=512, ny=512, nz=128, dx=2.0, theta0=300.0, lot=40.0, foot=(2
             cx, cy = (il + 0.5) * lot, (jl + 0.5) * lot
             inx = np.abs(xc - cx) <= wx / 2
             iny = np.abs(yc - cy) <= wy / 2
+            if not (inx.any() and iny.any()):
+                continue
             inz = zc <= hh
             mask[np.ix_(inz, iny, inx)] = 1.0
     b["immersed_proportion"][...] = mask
-    shape = (nz, ny, nx)
+    shape = (nz, by, bx)
     pi = _exner_column(zc, lambda z: np.full_like(z, theta0), opts)
     press = opts["p0"] * pi ** (opts["cp_d"] / opts["R_d"])
     p3 = np.broadcast_to(press[:, None, None], shape).copy()
     th = np.full(shape, theta0)
     rho, T = _state_from_theta_p(th, p3, opts)
     b["uvel"][...] = np.where(mask > 0, 0.0, u0)
-    idx = np.arange(nz * ny * nx, dtype=np.uint64).reshape(shape)
+    k = np.arange(nz, dtype=np.uint64)[:, None, None]
+    j = np.arange(j0, j0 + by, dtype=np.uint64)[None, :, None]
+    i = np.arange(i0, i0 + bx, dtype=np.uint64)[None, None, :]
+    idx = (k * np.uint64(ny) + j) * np.uint64(nx) + i
     noise = (splitmix64_uniform(seed, idx) * 2.0 - 1.0) * noise_amp
     rho_p, T_p = _state_from_theta_p(th + noise, p3, opts)
     return Case(rho_d=rho, temp=T, perturbed=dict(rho_d=rho_p, temp=T_p), steps=steps, **b)

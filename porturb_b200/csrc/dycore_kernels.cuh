@@ -1457,42 +1457,48 @@ struct LevelTables {
 // round32, every stored profile is rounded to float as the reference's
 // float DataManager arrays are, and the derived tables use those values.
 // If sums is null the cell profiles already in out.cells are used (restart).
+// One block (HYDRO_THREADS threads): every phase is a loop over levels whose
+// iterations are independent, with a barrier between phases that read what
+// the previous one wrote; each value is computed as a serial loop would.
+constexpr int HYDRO_THREADS = 256;
+
 template <class R>
-__global__ void k_hydro_finish(const double *__restrict__ sums, int nz, double r_nx_ny, double gamma, double C0,
-                               double grav, double dz, int round32, HydroOut out, LevelTables<R> tab) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__global__ void __launch_bounds__(HYDRO_THREADS) k_hydro_finish(const double *__restrict__ sums, int nz, double r_nx_ny,
+                                                                double gamma, double C0, double grav, double dz,
+                                                                int round32, HydroOut out, LevelTables<R> tab) {
+  if (blockIdx.x != 0) return;
+  const int tid = threadIdx.x, nt = blockDim.x;
   const int nzh = nz + 2 * HS;
   double *r = out.cells, *t = out.cells + nzh, *p = out.cells + 2 * nzh;
   auto rnd = [&](double x) { return round32 ? double(float(x)) : x; };
   if (!sums && round32)
-    for (int k = 0; k < 3 * nzh; k++) out.cells[k] = rnd(out.cells[k]);
+    for (int k = tid; k < 3 * nzh; k += nt) out.cells[k] = rnd(out.cells[k]);
   if (sums) {
-    for (int k = 0; k < nz; k++) {
+    // Level means (dynamics_rk.h:967-978).
+    for (int k = tid; k < nz; k += nt) {
       r[HS + k] = rnd(sums[k] * r_nx_ny);
       t[HS + k] = rnd(sums[nz + k] * r_nx_ny);
       p[HS + k] = rnd(sums[2 * nz + k] * r_nx_ny);
     }
-    for (int kk = 0; kk < HS; kk++) {
-      {
-        const int k0 = HS, k = k0 - 1 - kk;
-        const double rho0 = r[k0], theta0 = t[k0];
-        const double rho0_gm1 = pow(rho0, gamma - 1), theta0_g = pow(theta0, gamma);
-        r[k] = rnd(pow(rho0_gm1 + grav * (gamma - 1) * dz * (kk + 1) / (gamma * C0 * theta0_g), 1. / (gamma - 1)));
-        t[k] = rnd(theta0);
-        p[k] = rnd(C0 * pow(r[k] * theta0, gamma));
-      }
-      {
-        const int k0 = HS + nz - 1, k = k0 + 1 + kk;
-        const double rho0 = r[k0], theta0 = t[k0];
-        const double rho0_gm1 = pow(rho0, gamma - 1), theta0_g = pow(theta0, gamma);
-        r[k] = rnd(pow(rho0_gm1 - grav * (gamma - 1) * dz * (kk + 1) / (gamma * C0 * theta0_g), 1. / (gamma - 1)));
-        t[k] = rnd(theta0);
-        p[k] = rnd(C0 * pow(r[k] * theta0, gamma));
-      }
+    __syncthreads();
+    // Isentropic extension into the HS halo levels below and above
+    // (dynamics_rk.h:980-1008): item q < HS below, q >= HS above.
+    for (int q = tid; q < 2 * HS; q += nt) {
+      const int kk = q % HS;
+      const bool below = q < HS;
+      const int k0 = below ? HS : HS + nz - 1, k = below ? k0 - 1 - kk : k0 + 1 + kk;
+      const double rho0 = r[k0], theta0 = t[k0];
+      const double rho0_gm1 = pow(rho0, gamma - 1), theta0_g = pow(theta0, gamma);
+      const double dg = grav * (gamma - 1) * dz * (kk + 1) / (gamma * C0 * theta0_g);
+      r[k] = rnd(pow(below ? rho0_gm1 + dg : rho0_gm1 - dg, 1. / (gamma - 1)));
+      t[k] = rnd(theta0);
+      p[k] = rnd(C0 * pow(r[k] * theta0, gamma));
     }
   }
+  __syncthreads();
+  // Edge profiles (dynamics_rk.h:1145-1186).
   double *re = out.edges, *te = out.edges + (nz + 1), *pe = out.edges + 2 * (nz + 1);
-  for (int k = 0; k < nz + 1; k++) {
+  for (int k = tid; k < nz + 1; k += nt) {
     re[k] = rnd(exp(-1. / 12. * log(r[HS + k - 2]) + 7. / 12. * log(r[HS + k - 1]) + 7. / 12. * log(r[HS + k]) +
                     -1. / 12. * log(r[HS + k + 1])));
     te[k] = rnd(-1. / 12. * t[HS + k - 2] + 7. / 12. * t[HS + k - 1] + 7. / 12. * t[HS + k] + -1. / 12. * t[HS + k + 1]);
@@ -1501,7 +1507,7 @@ __global__ void k_hydro_finish(const double *__restrict__ sums, int nz, double r
     tab.rho_e[k] = R(re[k]);
     tab.theta_e[k] = R(te[k]);
   }
-  for (int k = 0; k < nzh; k++) {
+  for (int k = tid; k < nzh; k += nt) {
     const double rt = r[k] * t[k];
     const double P0 = C0 * pow(rt, gamma);
     tab.rho_h[k] = R(r[k]);
@@ -1510,7 +1516,7 @@ __global__ void k_hydro_finish(const double *__restrict__ sums, int nz, double r
     tab.p0_h[k] = R(P0);
     tab.dp_h[k] = R(P0 - p[k]);
   }
-  for (int k = 0; k < nz; k++) {
+  for (int k = tid; k < nz; k += nt) {
     const double rt = r[HS + k] * t[HS + k];
     out.rho_off[k] = r[HS + k];
     out.rt_off[k] = rt;

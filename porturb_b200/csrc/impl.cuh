@@ -714,7 +714,7 @@ struct Impl : ImplBase {
     PU_LAUNCHED();
     HydroOut ho{cells, edges, rho_off, rt_off};
     const double r_nx_ny = 1. / (double(cfg.nx) * double(cfg.ny));
-    k_hydro_finish<R><<<1, 1, 0, st>>>(sums, cfg.nz, r_nx_ny, cfg.gamma_d, cfg.C0, cfg.grav, cfg.dz,
+    k_hydro_finish<R><<<1, HYDRO_THREADS, 0, st>>>(sums, cfg.nz, r_nx_ny, cfg.gamma_d, cfg.C0, cfg.grav, cfg.dz,
                                        sizeof(R) == 4, ho, lt);
     PU_LAUNCHED();
     // Immersed preprocessing.
@@ -1060,7 +1060,7 @@ struct Impl : ImplBase {
     }
     HydroOut ho{cells, edges, rho_off, rt_off};
     const double r = 1. / (double(dc.d.nx_glob) * double(dc.d.ny_glob));
-    k_hydro_finish<R><<<1, 1, 0, st>>>(sums, cfg.nz, r, cfg.gamma_d, cfg.C0, cfg.grav, cfg.dz, sizeof(R) == 4, ho,
+    k_hydro_finish<R><<<1, HYDRO_THREADS, 0, st>>>(sums, cfg.nz, r, cfg.gamma_d, cfg.C0, cfg.grav, cfg.dz, sizeof(R) == 4, ho,
                                        lt);
     PU_LAUNCHED();
     return PU_OK;
@@ -1223,7 +1223,7 @@ struct Impl : ImplBase {
       }
       cudaMemcpyAsync(cells, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, st);
       HydroOut ho{cells, edges, rho_off, rt_off};
-      k_hydro_finish<R><<<1, 1, 0, st>>>(nullptr, cfg.nz, 0., cfg.gamma_d, cfg.C0, cfg.grav, cfg.dz, sizeof(R) == 4, ho,
+      k_hydro_finish<R><<<1, HYDRO_THREADS, 0, st>>>(nullptr, cfg.nz, 0., cfg.gamma_d, cfg.C0, cfg.grav, cfg.dz, sizeof(R) == 4, ho,
                                          lt);
       launches++;
       k_rebase<R><<<blocks(N, 256), 256, 0, st>>>(static_cast<R *>(s[0]), old_r, old_rt, rho_off, rt_off, N, NP);
@@ -1347,7 +1347,7 @@ struct Impl : ImplBase {
     PU_CK(cudaMemcpyAsync(im.cells + nzh, theta_cells, nzh * sizeof(double), cudaMemcpyHostToDevice, im.st));
     PU_CK(cudaMemcpyAsync(im.cells + 2 * nzh, pressure_cells, nzh * sizeof(double), cudaMemcpyHostToDevice, im.st));
     HydroOut ho{im.cells, im.edges, im.rho_off, im.rt_off};
-    k_hydro_finish<R><<<1, 1, 0, im.st>>>(nullptr, c.nz, 0., c.gamma_d, c.C0, c.grav, c.dz, sizeof(R) == 4, ho, im.lt);
+    k_hydro_finish<R><<<1, HYDRO_THREADS, 0, im.st>>>(nullptr, c.nz, 0., c.gamma_d, c.C0, c.grav, c.dz, sizeof(R) == 4, ho, im.lt);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
       set_error(std::string("kernel launch: ") + cudaGetErrorString(e));

@@ -334,6 +334,22 @@ int local_exchange(std::vector<pu::ImplBase *> &t, int which, bool x, bool y) {
 
 namespace {
 
+// The learned path's input normalisation (normalize9) on n stencils: x = the
+// stencil scaled to [0,1] by its range, jump = the largest normalised
+// neighbour difference (the acceptance check).
+__global__ void k_normalize9_eval(const float *__restrict__ s, long long n, float *__restrict__ x,
+                                  float *__restrict__ jump) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float st[9], xs[9];
+#pragma unroll
+  for (int m = 0; m < 9; m++) st[m] = s[i * 9 + m];
+  const float j = pu::normalize9(st, xs);
+#pragma unroll
+  for (int m = 0; m < 9; m++) x[i * 9 + m] = xs[m];
+  jump[i] = j;
+}
+
 // The FP32 limiter on a batch of stencils: VARIANT 0 the scalar form, 1 the
 // packed form (stencils 2i and 2i+1 in one thread), 4 the packed one-edge
 // form (the right edge of stencil 2i and the left edge of stencil 2i+1; the
@@ -951,6 +967,31 @@ int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long l
   }
   if (e != cudaSuccess) return fail(PU_ERR_CUDA, cudaGetErrorString(e));
   if (herr) return fail(PU_ERR_CUDA, "tensor-core limiter: an MMA did not complete in time");
+  return PU_OK;
+}
+
+int pu_learned_normalize_f32(const float *stencils, long long n, float *x, float *jump) {
+  if (!stencils || !x || !jump || n < 0) return fail(PU_ERR_INVALID, "bad argument");
+  if (n == 0) return PU_OK;
+  float *ds = nullptr, *dx = nullptr, *dj = nullptr;
+  if (cudaMalloc(&ds, size_t(n) * 9 * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&dx, size_t(n) * 9 * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&dj, size_t(n) * sizeof(float)) != cudaSuccess) {
+    cudaFree(ds);
+    cudaFree(dx);
+    return fail(PU_ERR_NOMEM, "cudaMalloc");
+  }
+  cudaError_t e = cudaMemcpy(ds, stencils, size_t(n) * 9 * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_normalize9_eval<<<unsigned((n + 255) / 256), 256>>>(ds, n, dx, dj);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(x, dx, size_t(n) * 9 * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(jump, dj, size_t(n) * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(ds);
+  cudaFree(dx);
+  cudaFree(dj);
+  if (e != cudaSuccess) return fail(PU_ERR_CUDA, cudaGetErrorString(e));
   return PU_OK;
 }
 

@@ -9,9 +9,13 @@
 // host-side stand-in for the symbol, not a device address: its device address
 // is looked up with cudaGetSymbolAddress once per device, with that device
 // current, on the first call that runs on it, and that address is what the
-// kernels receive.
+// kernels receive.  The address is cached per device; a device reset
+// (cudaDeviceReset, or a reset of the primary context) while the library is
+// loaded is not supported: the cached address would outlive the context it
+// belongs to.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <string>
 
@@ -35,19 +39,26 @@ namespace {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[PU_NOALLOC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 64;
-unsigned char *g_scratch_addr[kMaxDevices] = {};
+// Device address of g_noalloc_scratch per device ordinal.  Two host threads
+// making their first call on one device may both look it up; they store the
+// same value, and the atomic makes that race well defined.
+std::atomic<unsigned char *> g_scratch_addr[kMaxDevices] = {};
 
 int fail(int code, const std::string &msg) {
   pu::set_error(msg);
   return code;
 }
 
+// Makes `dev` current for the call and restores the previous device after it;
+// `ok` is false when the switch failed (nothing may then run on `dev`).
 struct DeviceGuard {
   int prev = -1;
+  cudaError_t status = cudaSuccess;
   explicit DeviceGuard(int dev) {
     if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != dev) cudaSetDevice(dev);
+    if (prev != dev) status = cudaSetDevice(dev);
   }
+  bool ok() const { return status == cudaSuccess; }
   ~DeviceGuard() {
     int cur = -1;
     if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
@@ -80,6 +91,7 @@ extern "C" int pu_dycore_time_step_noalloc(const pu_config *cfg, const double *d
   if (cfg->device < 0 || cfg->device >= ndev || cfg->device >= kMaxDevices)
     return fail(PU_ERR_INVALID, "bad device ordinal");
   DeviceGuard g(cfg->device);
+  if (!g.ok()) return fail(PU_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(g.status));
   // Coupler arrays must already be on the device: there is no staging buffer.
   const double *arrs[5] = {coupler->rho_d, coupler->uvel, coupler->vvel, coupler->wvel, coupler->temp};
   for (int a = 0; a < 5 + cfg->ntracers; a++) {
@@ -91,12 +103,13 @@ extern "C" int pu_dycore_time_step_noalloc(const pu_config *cfg, const double *d
   pu_state_view v = *coupler;
   v.mem = PU_MEM_DEVICE;
   // Set-up, once per device: the device address of the scratch array.
-  unsigned char *&scratch = g_scratch_addr[cfg->device];
+  unsigned char *scratch = g_scratch_addr[cfg->device].load(std::memory_order_acquire);
   if (!scratch) {
     void *addr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
     if (e != cudaSuccess) return fail(PU_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     scratch = static_cast<unsigned char *>(addr);
+    g_scratch_addr[cfg->device].store(scratch, std::memory_order_release);
   }
   switch (cfg->ntracers) {
     case 1: return pu::noalloc_time_step_f32_1(*cfg, scratch, dens_cells, theta_cells, pressure_cells, &v, dt_phys, ncycles);

@@ -10,7 +10,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 EXE = os.path.join(HERE, "_build", "dropin_driver")
 PHYS_EXE = os.path.join(HERE, "_build", "physics_driver")
 PG_EXE = os.path.join(HERE, "_build", "pg_driver")
-REF_CORE = "/root/reference/model/core"
+# The reference tree: $PORTURB_REFERENCE, by default where this image mounts it.
+REF_CORE = os.path.join(os.environ.get("PORTURB_REFERENCE", "/root/reference"), "model", "core")
 
 
 def _compile(src, exe, libdir):

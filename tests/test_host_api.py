@@ -79,3 +79,19 @@ def test_case_generators():
     assert m[0].mean() > 0.2 and m[-1].max() == 0.0
     u2 = cases.urban_canopy(nx=128, ny=128, nz=40)
     assert np.array_equal(u2.immersed_proportion, m)               # seeded, deterministic
+
+
+def test_urban_window_is_the_block_of_the_full_domain():
+    """The bounded CPU sample of the urban workloads is a window of the full
+    grid: the same buildings and noise as that block of the whole domain."""
+    full = cases.urban_canopy(nx=160, ny=120, nz=40, dx=2.0)
+    for w in [(0, 0, 64, 48), (37, 53, 80, 60), (0, 0, 160, 120)]:
+        b = cases.urban_canopy(nx=160, ny=120, nz=40, dx=2.0, window=w)
+        c = full.block(*w)
+        for nm in ("rho_d", "uvel", "vvel", "wvel", "temp", "tracer_data", "immersed_proportion"):
+            assert np.array_equal(getattr(b, nm), getattr(c, nm)), nm
+        for k in ("rho_d", "temp"):
+            assert np.array_equal(b.perturbed[k], c.perturbed[k])
+        assert (b.nx, b.ny, b.xlen, b.ylen) == (c.nx, c.ny, c.xlen, c.ylen)
+    with pytest.raises(ValueError):
+        cases.urban_canopy(nx=160, ny=120, nz=40, window=(100, 0, 64, 48))

@@ -5,10 +5,11 @@ host model whose own allocator has already reserved the GPU's memory, or a
 plug-in running inside a time loop where device allocation is not allowed.
 Its working memory is one static device array inside the library.  This test
 drives it through the C-ABI twice in a row and checks each result against the
-handle-based pu_dycore_time_step on identical device-resident coupler arrays,
-with the FP32 tolerance of the parity tests (L2 <= 1e-5 and Linf <= 1e-4 of
-each field's departure from its level mean).  Each call reuses the array the
-previous call left behind.
+handle-based pu_dycore_time_step on identical device-resident coupler arrays.
+Both run the same kernels on the same cell profiles, so they must agree bit
+for bit.  Each call reuses the array the previous call left behind.  The
+device's free memory (cudaMemGetInfo) must not change across the two calls,
+after one warm-up call has loaded the kernels.
 """
 import ctypes as C
 
@@ -24,14 +25,6 @@ CASES = {
     "small_two_tracers": lambda: cases.small_mixed(immersed=False),
     "abl_block_48x40x32": lambda: cases.abl_neutral(nx=48, ny=40, nz=32),
 }
-
-
-def _departure_err(a, b):
-    """(L2, Linf) of a-b relative to b's departure from its level means."""
-    dep = b - b.mean(axis=(1, 2), keepdims=True)
-    d = a - b
-    return (np.sqrt(np.mean(d ** 2)) / (np.sqrt(np.mean(dep ** 2)) + 1e-300),
-            np.abs(d).max() / (np.abs(dep).max() + 1e-300))
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -51,20 +44,34 @@ def test_noalloc_matches_time_step_on_two_calls(name):
         tr = [torch.tensor(np.ascontiguousarray(t), device=dev) for t in pert[5]]
         return st, tr
 
+    lib = capi.load()
+
+    def noalloc(view):
+        n = C.c_int()
+        capi.check(lib.pu_dycore_time_step_noalloc(C.byref(g.cfg), cells[0].ctypes.data, cells[1].ctypes.data,
+                                                   cells[2].ctypes.data, C.byref(view), dt_phys, C.byref(n)))
+        return n.value
+
+    # Warm-up call on a throw-away copy: it loads the kernels (lazy module
+    # loading takes device memory once) and sets up the scratch address.
+    w_st, w_tr = device_copy()
+    noalloc(make_view(*w_st, w_tr))
+    torch.cuda.synchronize()
+
     a_st, a_tr = device_copy()        # existing entry point
     b_st, b_tr = device_copy()        # no-allocation entry point
     view_b = make_view(*b_st, b_tr)
-    lib = capi.load()
     for call in range(2):
         n_ref = g.time_step(*a_st, a_tr, dt_phys)
-        n = C.c_int()
-        capi.check(lib.pu_dycore_time_step_noalloc(C.byref(g.cfg), cells[0].ctypes.data, cells[1].ctypes.data,
-                                                   cells[2].ctypes.data, C.byref(view_b), dt_phys, C.byref(n)))
         torch.cuda.synchronize()
-        assert n.value == n_ref == 3
+        free0 = torch.cuda.mem_get_info(0)[0]
+        n = noalloc(view_b)
+        torch.cuda.synchronize()
+        free1 = torch.cuda.mem_get_info(0)[0]
+        assert free1 == free0, (name, call, free0, free1)
+        assert n == n_ref == 3
         for x, y in zip(b_st + b_tr, a_st + a_tr):
-            e2, ei = _departure_err(x.cpu().numpy(), y.cpu().numpy())
-            assert e2 <= 1e-5 and ei <= 1e-4, (name, call, e2, ei)
+            assert torch.equal(x, y), (name, call, (x - y).abs().max().item())
     g.close()
 
 

@@ -45,7 +45,8 @@ typedef enum {
   PU_ERR_NONFINITE = 3,    /* the state became NaN/Inf during a step */
   PU_ERR_STATE = 4,        /* call out of order (e.g. time_step before init) */
   PU_ERR_NOMEM = 5,        /* device allocation failed */
-  PU_ERR_UNSUPPORTED = 6   /* configuration outside what this build supports */
+  PU_ERR_UNSUPPORTED = 6,  /* configuration outside what this build supports */
+  PU_ERR_TRANSPORT = 7     /* a host transport callback reported a failure */
 } pu_status;
 
 typedef enum { PU_BC_PERIODIC = 0, PU_BC_PRECURSOR = 1, PU_BC_WALL = 2 } pu_bc;
@@ -368,6 +369,36 @@ int pu_nccl_get_unique_id(unsigned char *id);
  * not).  With id NULL the tiles of the grid are handles of one process on
  * one stream, driven by the pu_dycore_group_* calls. */
 int pu_dycore_set_decomposition(pu_dycore *h, const pu_decomp *d, const unsigned char *nccl_id);
+
+/* A host transport for a decomposed tile: the caller's own message layer
+ * (MPI, a Python process group, ...) moves the halo slabs and the init
+ * reductions through host memory, where the reference's coupler calls MPI
+ * (ParallelComm.h send_receive / all_reduce, used by coupler.h:985-1165 for
+ * the halos and dynamics_rk.h:976-978 for the column sums).  The library
+ * calls these from the thread that drives the handle, during set-up, init and
+ * every stage, with pinned host buffers it owns; each returns 0 on success
+ * (anything else makes the dycore call return PU_ERR_TRANSPORT).
+ *   exchange: for every direction d (x-, x+, y-, y+) with bytes[d] > 0, send
+ *     snd[d] to rank nbr[d] and receive from rank nbr[d] into rcv[d]; what a
+ *     rank sends as snd[d] its neighbour receives as rcv[d ^ 1] (a rank can be
+ *     its own neighbour, and the x- and x+ neighbours can be one rank);
+ *   allreduce_sum_f64: buf[0..n) = its sum over all ranks, in place; the same
+ *     order of summation on every rank keeps the tiles' profiles identical;
+ *   allgather: out = the `bytes` bytes of `in` of every rank, in rank order. */
+typedef struct pu_host_transport {
+  int (*exchange)(void *user, void *const *snd, void *const *rcv, const size_t *bytes, const int *nbr);
+  int (*allreduce_sum_f64)(void *user, double *buf, size_t n);
+  int (*allgather)(void *user, const void *in, void *out, size_t bytes);
+  void *user;
+} pu_host_transport;
+
+/* Makes the handle tile (px, py) of a decomposed domain whose ranks talk
+ * through the host transport t (copied; its user pointer must stay valid
+ * while the handle lives); call before pu_dycore_init.  Like the NCCL form,
+ * this call, init and every time step are collective over the
+ * nproc_x*nproc_y ranks, and this call checks with allgather that the tiles
+ * fit together, failing on every rank alike if they do not. */
+int pu_dycore_set_decomposition_host(pu_dycore *h, const pu_decomp *d, const pu_host_transport *t);
 
 /* init, advance and time_step of an in-process group: hs holds the n =
  * nproc_x*nproc_y tiles (any order) made with pu_dycore_set_decomposition(h,

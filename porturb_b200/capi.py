@@ -13,7 +13,8 @@ LIB_PATH = os.path.join(HERE, "_lib", "libpu_dycore.so")
 
 PU_MAX_TRACERS = 4
 PU_HS = 4
-PU_OK, PU_ERR_INVALID, PU_ERR_CUDA, PU_ERR_NONFINITE, PU_ERR_STATE, PU_ERR_NOMEM, PU_ERR_UNSUPPORTED = range(7)
+(PU_OK, PU_ERR_INVALID, PU_ERR_CUDA, PU_ERR_NONFINITE, PU_ERR_STATE, PU_ERR_NOMEM, PU_ERR_UNSUPPORTED,
+ PU_ERR_TRANSPORT) = range(8)
 PU_BC_PERIODIC, PU_BC_PRECURSOR, PU_BC_WALL = 0, 1, 2
 PU_F32, PU_F64 = 0, 1
 PU_WENO_PLAIN, PU_WENO_LEARNED = 0, 1
@@ -21,7 +22,7 @@ PU_MEM_HOST, PU_MEM_DEVICE = 0, 1
 BC_NAMES = {"periodic": PU_BC_PERIODIC, "precursor": PU_BC_PRECURSOR, "solid_wall": PU_BC_WALL}
 
 STATUS_NAMES = {0: "PU_OK", 1: "PU_ERR_INVALID", 2: "PU_ERR_CUDA", 3: "PU_ERR_NONFINITE", 4: "PU_ERR_STATE",
-                5: "PU_ERR_NOMEM", 6: "PU_ERR_UNSUPPORTED"}
+                5: "PU_ERR_NOMEM", 6: "PU_ERR_UNSUPPORTED", 7: "PU_ERR_TRANSPORT"}
 
 
 class PortUrbError(RuntimeError):
@@ -56,6 +57,18 @@ class pu_diag(C.Structure):
     _fields_ = [("mass", C.c_double), ("rho_theta", C.c_double), ("kinetic", C.c_double),
                 ("internal", C.c_double), ("potential", C.c_double), ("total_energy", C.c_double),
                 ("tracer_mass", C.c_double * PU_MAX_TRACERS)]
+
+
+# pu_host_transport callbacks (include/pu_dycore.h)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_size_t),
+                          C.POINTER(C.c_int))
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double), C.c_size_t)
+ALLGATHER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t)
+
+
+class pu_host_transport(C.Structure):
+    _fields_ = [("exchange", EXCHANGE_FN), ("allreduce_sum_f64", ALLREDUCE_FN), ("allgather", ALLGATHER_FN),
+                ("user", C.c_void_p)]
 
 
 PU_MLP_PARAMS = 1541
@@ -150,6 +163,7 @@ SIGNATURES = {
     "pu_decomp_neighbors": (_I, [C.POINTER(pu_decomp), C.POINTER(_I)]),
     "pu_nccl_get_unique_id": (_I, [C.c_char_p]),
     "pu_dycore_set_decomposition": (_I, [_P, C.POINTER(pu_decomp), C.c_char_p]),
+    "pu_dycore_set_decomposition_host": (_I, [_P, C.POINTER(pu_decomp), C.POINTER(pu_host_transport)]),
     "pu_dycore_group_init": (_I, [C.POINTER(_P), _I, C.POINTER(pu_state_view), C.POINTER(_P), C.POINTER(_P), _I]),
     "pu_dycore_group_advance": (_I, [C.POINTER(_P), _I, _D, _I]),
     "pu_dycore_group_time_step": (_I, [C.POINTER(_P), _I, C.POINTER(pu_state_view), _D, C.POINTER(_I)]),

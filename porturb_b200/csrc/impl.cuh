@@ -49,15 +49,21 @@ void set_error(const std::string &msg);
 // Buffers of one halo exchange, per direction d = x-, x+, y-, y+: snd[d] holds
 // this tile's cells next to edge d, rcv[d] receives the neighbour's cells
 // beyond edge d (the neighbour's snd[d ^ 1]).
+// hsnd/hrcv: pinned host copies of the slabs for a host transport (made on
+// first use).
 struct HaloSet {
   void *snd[4] = {nullptr, nullptr, nullptr, nullptr};
   void *rcv[4] = {nullptr, nullptr, nullptr, nullptr};
+  void *hsnd[4] = {nullptr, nullptr, nullptr, nullptr};
+  void *hrcv[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t bytes[4] = {0, 0, 0, 0};
   void release() {
     for (int d = 0; d < 4; d++) {
       if (snd[d]) cudaFree(snd[d]);
       if (rcv[d]) cudaFree(rcv[d]);
-      snd[d] = rcv[d] = nullptr;
+      if (hsnd[d]) cudaFreeHost(hsnd[d]);
+      if (hrcv[d]) cudaFreeHost(hrcv[d]);
+      snd[d] = rcv[d] = hsnd[d] = hrcv[d] = nullptr;
       bytes[d] = 0;
     }
   }
@@ -73,7 +79,9 @@ struct Decomposition {
   pu_decomp d{};
   int rank = 0, nranks = 1;  // rank = py*nproc_x + px (coupler.h:168-171)
   int nbr[4] = {0, 0, 0, 0}; // ranks beyond the x-, x+, y-, y+ edges, periodic (coupler.h:203-214)
-  ncclComm_t comm = nullptr; // null: an in-process group of tiles (pu_dycore_group_*)
+  ncclComm_t comm = nullptr; // null: a host transport (below) or an in-process group of tiles (pu_dycore_group_*)
+  bool host = false;         // the caller's host transport moves the slabs and sums
+  pu_host_transport ht{};
   HaloSet state;             // the stage input's raw state, HALO_W wide
   uint8_t *fslab[4] = {nullptr, nullptr, nullptr, nullptr};  // immersed flags of the cells in state.rcv
   HaloSet ix, iy;            // the immersed proportion at init, INIT_HALO wide (FP64)
@@ -416,6 +424,62 @@ struct ImplBase {
     if (r != ncclSuccess) return nccl_fail(r, "ncclGroupEnd");
     return PU_OK;
   }
+  // The exchange through the caller's host transport: the active slabs to
+  // pinned host memory, the transport's exchange, the received slabs back.
+  int host_exchange(HaloSet &h, bool x, bool y) {
+    void *s[4] = {nullptr, nullptr, nullptr, nullptr}, *r[4] = {nullptr, nullptr, nullptr, nullptr};
+    size_t b[4] = {0, 0, 0, 0};
+    for (int d = 0; d < 4; d++) {
+      if ((d < 2 && !x) || (d >= 2 && !y) || !h.bytes[d]) continue;
+      if (!h.hsnd[d]) PU_CK(cudaHostAlloc(&h.hsnd[d], h.bytes[d], cudaHostAllocDefault));
+      if (!h.hrcv[d]) PU_CK(cudaHostAlloc(&h.hrcv[d], h.bytes[d], cudaHostAllocDefault));
+      PU_CK(cudaMemcpyAsync(h.hsnd[d], h.snd[d], h.bytes[d], cudaMemcpyDeviceToHost, st));
+      s[d] = h.hsnd[d];
+      r[d] = h.hrcv[d];
+      b[d] = h.bytes[d];
+    }
+    PU_CK(cudaStreamSynchronize(st));
+    const int q = dc.ht.exchange(dc.ht.user, s, r, b, dc.nbr);
+    if (q != 0) {
+      set_error("host transport: exchange returned " + std::to_string(q));
+      return PU_ERR_TRANSPORT;
+    }
+    for (int d = 0; d < 4; d++)
+      if (b[d]) PU_CK(cudaMemcpyAsync(h.rcv[d], h.hrcv[d], b[d], cudaMemcpyHostToDevice, st));
+    return PU_OK;
+  }
+  // The halo exchange of one HaloSet through this tile's transport.
+  int exchange(HaloSet &h, bool x, bool y) {
+    if (dc.comm) return nccl_exchange(h, x, y);
+    if (dc.host) return host_exchange(h, x, y);
+    set_error("halo exchange without a transport");
+    return PU_ERR_STATE;
+  }
+  // Sums the 3*nz column sums over all tiles, in place on the device.
+  int sum_columns() {
+    const size_t n = size_t(3) * cfg.nz;
+    if (dc.comm) {
+      const ncclResult_t r = nccl().AllReduce(sums, sums, n, ncclFloat64, ncclSum, dc.comm, st);
+      if (r != ncclSuccess) return nccl_fail(r, "ncclAllReduce");
+      return PU_OK;
+    }
+    if (!dc.host) {
+      set_error("column sums without a transport");
+      return PU_ERR_STATE;
+    }
+    std::vector<double> h(n);
+    PU_CK(cudaMemcpyAsync(h.data(), sums, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PU_CK(cudaStreamSynchronize(st));
+    const int q = dc.ht.allreduce_sum_f64(dc.ht.user, h.data(), n);
+    if (q != 0) {
+      set_error("host transport: allreduce_sum_f64 returned " + std::to_string(q));
+      return PU_ERR_TRANSPORT;
+    }
+    PU_CK(cudaMemcpyAsync(sums, h.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+    PU_CK(cudaStreamSynchronize(st));
+    return PU_OK;
+  }
+  bool has_transport() const { return dc.comm != nullptr || dc.host; }
   // Type-dependent parts of the decomposed path (Impl).
   virtual int dec_alloc() = 0;
   virtual int dinit_begin(const pu_state_view *v, const double *prop, const double *proj, int mem) = 0;
@@ -694,17 +758,16 @@ struct Impl : ImplBase {
 
   int init(const pu_state_view *v, const double *prop, int mem, const double *proj = nullptr) override {
     if (dc.on) {
-      if (!dc.comm) {
+      if (!has_transport()) {
         set_error("the tiles of an in-process group are initialised with pu_dycore_group_init");
         return PU_ERR_STATE;
       }
       PU_TRY(dinit_begin(v, prop, proj, mem));
-      const ncclResult_t r = nccl().AllReduce(sums, sums, size_t(3) * cfg.nz, ncclFloat64, ncclSum, dc.comm, st);
-      if (r != ncclSuccess) return nccl_fail(r, "ncclAllReduce");
+      PU_TRY(sum_columns());
       PU_TRY(dinit_hydro(nullptr));
-      PU_TRY(nccl_exchange(dc.ix, true, false));
+      PU_TRY(exchange(dc.ix, true, false));
       PU_TRY(dinit_mid());
-      if (!sim2d()) PU_TRY(nccl_exchange(dc.iy, false, true));
+      if (!sim2d()) PU_TRY(exchange(dc.iy, false, true));
       return dinit_end(v);
     }
     CouplerPtrs cp;
@@ -916,7 +979,7 @@ struct Impl : ImplBase {
   int advance(double dt, int nsteps) override {
     if (nsteps <= 0) return PU_OK;
     if (dc.on) {
-      if (!dc.comm) {
+      if (!has_transport()) {
         set_error("the tiles of an in-process group advance with pu_dycore_group_advance");
         return PU_ERR_STATE;
       }
@@ -924,7 +987,7 @@ struct Impl : ImplBase {
       for (int n = 0; n < nsteps; n++)
         for (int sg = 0; sg < 3; sg++) {
           PU_TRY(dec_pack(sg));
-          PU_TRY(nccl_exchange(dc.state, true, !sim2d()));
+          PU_TRY(exchange(dc.state, true, !sim2d()));
           PU_TRY(dec_compute(sg, dt, n == nsteps - 1));
         }
       return PU_OK;

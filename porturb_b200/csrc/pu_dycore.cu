@@ -298,7 +298,7 @@ int group_tiles(pu_dycore *const *hs, int n, std::vector<pu::ImplBase *> &byrank
   byrank.assign(n, nullptr);
   for (int i = 0; i < n; i++) {
     pu::ImplBase &I = *hs[i]->impl;
-    if (!I.dc.on || I.dc.comm)
+    if (!I.dc.on || I.dc.comm || I.dc.host)
       return fail(PU_ERR_STATE, "group tiles are made with pu_dycore_set_decomposition(h, d, NULL)");
     if (I.dc.d.nproc_x != h0.dc.d.nproc_x || I.dc.d.nproc_y != h0.dc.d.nproc_y ||
         I.dc.d.nx_glob != h0.dc.d.nx_glob || I.dc.d.ny_glob != h0.dc.d.ny_glob)
@@ -836,6 +836,37 @@ int pu_dycore_set_decomposition(pu_dycore *h, const pu_decomp *d, const unsigned
   rc = set_decomposition(I, *d, nccl_id);
   if (rc) I.dec_release();
   return rc;
+}
+
+int pu_dycore_set_decomposition_host(pu_dycore *h, const pu_decomp *d, const pu_host_transport *t) {
+  if (!h || !d || !t) return fail(PU_ERR_INVALID, "null argument");
+  if (!t->exchange || !t->allreduce_sum_f64 || !t->allgather)
+    return fail(PU_ERR_INVALID, "the host transport needs exchange, allreduce_sum_f64 and allgather");
+  auto &I = *h->impl;
+  if (I.inited) return fail(PU_ERR_STATE, "pu_dycore_set_decomposition_host comes before pu_dycore_init");
+  if (I.dc.on) return fail(PU_ERR_STATE, "the handle is already decomposed");
+  if (I.weno_mode == PU_WENO_LEARNED) return fail(PU_ERR_UNSUPPORTED, "learned weights do not run on decomposed tiles");
+  int rc = check_decomp(d, I.cfg);
+  if (rc) return rc;
+  DeviceGuard g(h->device);
+  rc = set_decomposition(I, *d, nullptr);
+  if (!rc) {
+    // Every rank checks the whole table of tiles before any halo moves.
+    const TileInfo mine{d->px, d->py, I.cfg.nx, I.cfg.ny, I.cfg.nz, I.S, I.cfg.precision};
+    std::vector<TileInfo> all(I.dc.nranks);
+    const int q = t->allgather(t->user, &mine, all.data(), sizeof(TileInfo));
+    std::string why;
+    if (q != 0) rc = fail(PU_ERR_TRANSPORT, "host transport: allgather returned " + std::to_string(q));
+    else if (!tiles_fit(*d, all, why)) rc = fail(PU_ERR_INVALID, why);
+  }
+  if (rc) {
+    I.dec_release();
+    I.dc.on = false;
+    return rc;
+  }
+  I.dc.host = true;
+  I.dc.ht = *t;
+  return PU_OK;
 }
 
 int pu_dycore_group_init(pu_dycore *const *hs, int n, const pu_state_view *views, const double *const *props,

@@ -12,6 +12,10 @@ decomposition entry points of include/pu_dycore.h.
   :func:`distributed_tile` does this over ``torch.distributed``.
 * :class:`TileGroup` -- the tiles of a grid as handles of one process on one
   stream, stepped together with device copies for the exchange.
+* :class:`TorchHostTransport` -- a pu_host_transport over a torch.distributed
+  process group with CPU tensors (gloo): the halo slabs and the init
+  reductions go through host memory, as the reference's coupler sends them
+  through MPI; :func:`host_transport_tile` makes this rank's tile with it.
 """
 from __future__ import annotations
 
@@ -196,3 +200,108 @@ def distributed_tile(case, precision="f32", device=None, stream=None, group=None
     h = Dycore.from_case(tc, precision=precision, device=device, stream=stream, **kw)
     set_decomposition(h, t, case.nx, case.ny, nccl_id=box[0])
     return h, t, tc
+
+
+class TorchHostTransport:
+    """The callbacks of a pu_host_transport on a torch.distributed process
+    group that carries CPU tensors (gloo).
+
+    exchange: for each active direction d, the slab snd[d] goes to rank
+    nbr[d] with tag d ^ 1 (the receiver's slot for it) and rcv[d] is received
+    from nbr[d] with tag d; a rank that is its own neighbour takes its own
+    snd[d ^ 1].  allreduce_sum_f64 and allgather map to the group's
+    all_reduce and all_gather.  A callback that raises returns 1 (the dycore
+    call then returns PU_ERR_TRANSPORT) and keeps the exception in `error`.
+    Keep the object alive while the handle that uses it lives."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+        self.dist = dist
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.world = dist.get_world_size(group)
+        self.error: Optional[BaseException] = None
+        self.calls = {"exchange": 0, "allreduce_sum_f64": 0, "allgather": 0}
+        self._fns = (capi.EXCHANGE_FN(self._exchange), capi.ALLREDUCE_FN(self._allreduce),
+                     capi.ALLGATHER_FN(self._allgather))
+        self.struct = capi.pu_host_transport(self._fns[0], self._fns[1], self._fns[2], None)
+
+    def _global(self, r):
+        return r if self.group is None else self.dist.get_global_rank(self.group, r)
+
+    @staticmethod
+    def _bytes(ptr, n):
+        import torch
+        return torch.from_numpy(np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint8)), shape=(int(n),)))
+
+    def _exchange(self, user, snd, rcv, nbytes, nbr):
+        try:
+            self.calls["exchange"] += 1
+            reqs, local = [], []
+            for d in range(4):
+                b = int(nbytes[d])
+                if not b:
+                    continue
+                if nbr[d] == self.rank:
+                    local.append(d)
+                    continue
+                peer = self._global(int(nbr[d]))
+                reqs.append(self.dist.isend(self._bytes(snd[d], b), dst=peer, tag=d ^ 1, group=self.group))
+                reqs.append(self.dist.irecv(self._bytes(rcv[d], b), src=peer, tag=d, group=self.group))
+            for d in local:
+                if int(nbytes[d ^ 1]) != int(nbytes[d]):
+                    raise ValueError("own-neighbour slabs differ in size")
+                C.memmove(rcv[d], snd[d ^ 1], int(nbytes[d]))
+            for q in reqs:
+                q.wait()
+            return 0
+        except BaseException as e:  # a ctypes callback must not raise
+            self.error = e
+            return 1
+
+    def _allreduce(self, user, buf, n):
+        try:
+            import torch
+            self.calls["allreduce_sum_f64"] += 1
+            t = torch.from_numpy(np.ctypeslib.as_array(buf, shape=(int(n),)))
+            self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM, group=self.group)
+            return 0
+        except BaseException as e:
+            self.error = e
+            return 1
+
+    def _allgather(self, user, src, out, nbytes):
+        try:
+            import torch
+            self.calls["allgather"] += 1
+            b = int(nbytes)
+            mine = self._bytes(src, b).clone()
+            parts = [torch.empty(b, dtype=torch.uint8) for _ in range(self.world)]
+            self.dist.all_gather(parts, mine, group=self.group)
+            dst = self._bytes(out, b * self.world)
+            for r, part in enumerate(parts):
+                dst[r * b:(r + 1) * b] = part
+            return 0
+        except BaseException as e:
+            self.error = e
+            return 1
+
+
+def set_decomposition_host(dyc: Dycore, t: Tile, nx_glob: int, ny_glob: int, transport: TorchHostTransport):
+    d = make_decomp(t.nproc_x, t.nproc_y, t.px, t.py, nx_glob, ny_glob)
+    dyc._transport = transport          # the callbacks must outlive the handle's use of them
+    check(dyc.lib.pu_dycore_set_decomposition_host(dyc.h, C.byref(d), C.byref(transport.struct)))
+
+
+def host_transport_tile(case, precision="f32", device=0, stream=None, group=None, **kw):
+    """This rank's tile of a global case, its halos moved through host memory
+    by a :class:`TorchHostTransport` on ``group`` (gloo): the process grid of
+    coupler.h:148-171 for the group's size, the handle decomposed
+    (collective).  Returns (Dycore, Tile, tile case, transport)."""
+    tr = TorchHostTransport(group)
+    npx, npy = process_grid(tr.world, case.nx, case.ny)
+    t = tiles(case.nx, case.ny, npx, npy)[tr.rank]
+    tc = tile_case(case, t)
+    h = Dycore.from_case(tc, precision=precision, device=device, stream=stream, **kw)
+    set_decomposition_host(h, t, case.nx, case.ny, tr)
+    return h, t, tc, tr

@@ -80,6 +80,9 @@ typedef struct pu_config {
   int z_chunk;                             /* 0: the tiled z kernel (FP32 with weno_all) or the z
                                               march with its own chunk; > 0: the z march with
                                               this many levels per work item (the same results) */
+  int thread_loads;                        /* 0: the stage kernels stage their tiles through TMA
+                                              where the grid allows it (nx % 4 == 0); 1: every
+                                              tile is loaded by the threads (the same results) */
 } pu_config;
 
 /* The coupler-side state: density_dry, uvel, vvel, wvel, temp and the tracer

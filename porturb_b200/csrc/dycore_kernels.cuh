@@ -29,6 +29,7 @@
 #include <type_traits>
 
 #include "mlp_infer.cuh"
+#include "tma.cuh"
 #include "weno9.cuh"
 
 namespace pu {
@@ -74,6 +75,9 @@ namespace pu {
 constexpr int HS = 4;
 constexpr int BC_PERIODIC = 0, BC_PRECURSOR = 1, BC_WALL = 2;
 constexpr unsigned FLAG_IMM = 1u, FLAG_ANY10 = 2u;
+// Bits of the device error word (Grid::err): a non-finite state, a tile copy
+// (TMA) that did not complete within its wait limit.
+constexpr int ERR_NONFINITE = 1, ERR_TMA = 2;
 constexpr int iR = 0, iU = 1, iV = 2, iW = 3, iT = 4, iP = 5;
 
 template <class R>
@@ -818,7 +822,7 @@ __device__ __forceinline__ void finish_cell(const Grid<R> &G, const R (&qin)[5 +
     bad |= !isfinite(out[s]);
     sout[s * G.N + idx] = out[s];
   }
-  if (bad) atomicOr(G.err, 1);
+  if (bad) atomicOr(G.err, ERR_NONFINITE);
 }
 
 // z fluxes, their divergence, sources and the SSPRK3 stage combination
@@ -1069,14 +1073,47 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_Z_MIN_BLOCKS : (s
 // Shared memory of k_zt: primitive fields of the tile's columns at levels
 // k0-5 .. k0+TZ+4 and the left/right z edges of the cells at levels
 // k0-1 .. k0+TZ.
+//
+// With TMA staging, the raw stage input of levels k0-5 .. k0+TZ+4
+// ([S][HZ][TX], x fastest) lands in the edge buffers, which are idle until
+// the primitive fields have been formed from it; when they fit beside four
+// blocks per SM, the cell inputs of the finalisation -- the stage input, the
+// step's initial state and the x/y tendency of levels k0 .. k0+TZ-1
+// ([S][TZ][TX] each) -- land in buffers of their own, copied while the block
+// reconstructs.  Two mbarriers complete the copies.
 template <int NTR, int TX, int TZ, bool IMM = false>
 struct ZTShape {
   static constexpr int F = 6 + NTR, S = 5 + NTR, NT = TX * TZ, HZ = TZ + 10;
   static constexpr int EN = (TZ + 2) * TX;
+  static constexpr size_t al(size_t b) { return (b + 127) / 128 * 128; }
   // Immersed domains add one flag byte per level and column (bit 0 immersed,
   // bit 1 an immersed cell within 10).
-  static constexpr size_t bytes = sizeof(float) * (size_t(F) * HZ * TX + 2 * size_t(F) * EN) +
-                                  (IMM ? (size_t(HZ) * TX + 15) / 16 * 16 : 0);
+  static constexpr size_t base_bytes = sizeof(float) * (size_t(F) * HZ * TX + 2 * size_t(F) * EN) +
+                                       (IMM ? (size_t(HZ) * TX + 15) / 16 * 16 : 0);
+  // The kernel rounds the start of its dynamic shared memory up to 128 bytes
+  // (the alignment of the TMA destinations): PAD bytes more than the layout.
+  static constexpr size_t PAD = 128;
+  static constexpr size_t bytes = base_bytes + PAD;
+  // TMA staging (byte offsets from the start of shared memory).
+  static constexpr size_t el_off = sizeof(float) * size_t(F) * HZ * TX;
+  static constexpr size_t raw_off = al(el_off);
+  static constexpr size_t raw_bytes = sizeof(float) * size_t(S) * HZ * TX;
+  static constexpr size_t cell_bytes = sizeof(float) * size_t(S) * TZ * TX;
+  static_assert(raw_off + raw_bytes <= el_off + sizeof(float) * 2 * size_t(F) * EN, "raw tile exceeds the edge buffers");
+  static constexpr size_t cells_off = al(base_bytes);
+  static constexpr size_t bar_off = cells_off + 3 * cell_bytes;
+  static constexpr size_t tma_bytes_prefetch = bar_off + 16;
+  // Four blocks per SM share 228 KB (1 KB of it reserved per block).
+  static constexpr bool PREFETCH = 4 * (tma_bytes_prefetch + PAD + 1024) <= 228 * 1024;
+  static constexpr size_t tma_bar_off = PREFETCH ? bar_off : al(base_bytes);
+  static constexpr size_t tma_bytes = tma_bar_off + 16 + PAD;
+};
+
+// Tensor maps of one k_zt launch (TMA staging): the stage input with the
+// halo box (TX, 1, TZ+10, S) and with the cell box (TX, 1, TZ, S), the step's
+// initial state and the x/y tendency with the cell box.
+struct ZtMaps {
+  CUtensorMap raw, qin, sn, txy;
 };
 
 // The z operator and the stage combination of k_z on a tile of TX columns of
@@ -1090,27 +1127,66 @@ struct ZTShape {
 // Riemann fluxes through the two faces of its cell and finalises it.  FP32
 // with weno_all (IMM: domains with immersed cells, whose level flags go to
 // shared memory with the fields); every other form keeps the march.
+//
+// use_tma: the raw tile and the finalisation's cell inputs come from TMA
+// copies (maps: tensor maps of sin, sn and txy); rows the halo box does not
+// hold (the wrapped levels of a periodic z) and, when the cell buffers do
+// not fit, the cell inputs are read per thread as without it.  Columns
+// beyond the domain read zero there instead of the last column; their
+// results are discarded either way.
 template <int NTR, int TX, int TZ, bool IMM>
 __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<float> G, const float *__restrict__ sin,
                                                                const float *sn, float *sout,
                                                                const float *__restrict__ txy, float a_n, float a_dt,
-                                                               int n_enforce) {
+                                                               int n_enforce, const __grid_constant__ ZtMaps maps,
+                                                               int use_tma) {
   using R = float;
   using Sh = ZTShape<NTR, TX, TZ, IMM>;
   constexpr int F = Sh::F, S = Sh::S, NT = Sh::NT, HZ = Sh::HZ;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_zt[];
+  unsigned char *smem_raw = smem_zt + ((128u - (tma::saddr(smem_zt) & 127u)) & 127u);
   R *H = reinterpret_cast<R *>(smem_raw);   // [F][HZ][TX]
   R *EL = H + F * HZ * TX;                   // [F][TZ+2][TX]
   R *ER = EL + F * Sh::EN;
   uint8_t *M = reinterpret_cast<uint8_t *>(ER + F * Sh::EN);   // [HZ][TX], immersed domains
+  R *RAW = reinterpret_cast<R *>(smem_raw + Sh::raw_off);     // [S][HZ][TX] (TMA), in the edge buffers
+  R *QIN = reinterpret_cast<R *>(smem_raw + Sh::cells_off);   // [S][TZ][TX] (TMA with PREFETCH)
+  R *SN = QIN + S * TZ * TX;
+  R *TXY = SN + S * TZ * TX;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + Sh::tma_bar_off);
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * TX, j = blockIdx.y, k0 = blockIdx.z * TZ;
   const int nx = G.nx, nz = G.nz;
   const bool wall = G.bc_z == BC_WALL;
   const size_t NP = G.NP, row = size_t(j) * nx;
+  const bool pref = Sh::PREFETCH && use_tma;
   // Level whose state feeds level p (wall halos replicate the boundary cell,
   // periodic halos wrap; dynamics_rk.h:780-797).
   auto src_level = [&](int p) { return (p >= 0 && p < nz) ? p : (wall ? clampi(p, nz) : wrapi(p, nz)); };
+
+  if (use_tma) {
+    if (tid == 0) {
+      tma::mbar_init(bar);
+      tma::mbar_init(bar + 1);
+      tma::mbar_expect(bar, uint32_t(Sh::raw_bytes));
+      tma::load_4d(RAW, &maps.raw, i0, j, k0 - 5, 0, bar);
+      if (pref) {
+        tma::mbar_expect(bar + 1, uint32_t(Sh::cell_bytes) * (sn ? 3u : 2u));
+        tma::load_4d(QIN, &maps.qin, i0, j, k0, 0, bar + 1);
+        tma::load_4d(TXY, &maps.txy, i0, j, k0, 0, bar + 1);
+        if (sn) tma::load_4d(SN, &maps.sn, i0, j, k0, 0, bar + 1);
+      }
+    }
+    __syncthreads();
+    if (!__syncthreads_and(tma::mbar_wait(bar, 0))) {
+      // The copy did not complete: report it, give the copies in flight a
+      // last bounded wait, and give up the tile.
+      if (tid == 0) atomicOr(G.err, ERR_TMA);
+      tma::mbar_wait(bar, 0);
+      if (pref) tma::mbar_wait(bar + 1, 0);
+      return;
+    }
+  }
 
   // 1. Primitive fields of levels k0-5 .. k0+TZ+4.  Columns beyond the domain
   // read its last column; their results are discarded.
@@ -1119,7 +1195,13 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
     const int p = k0 - 5 + r, lv = src_level(p);
     const size_t col = row + min(i0 + c, nx - 1);
     R q[S], w[F];
-    load_cell<R, NTR>(G, sin, size_t(lv) * NP + col, q);
+    const int rr = lv - (k0 - 5);   // the halo box's row of level lv
+    if (use_tma && rr >= 0 && rr < HZ) {
+#pragma unroll
+      for (int s2 = 0; s2 < S; s2++) q[s2] = RAW[(s2 * HZ + rr) * TX + c];
+    } else {
+      load_cell<R, NTR>(G, sin, size_t(lv) * NP + col, q);
+    }
     prims_of<R, NTR>(G, q, lv, w);
     if (wall && (p < 0 || p >= nz)) {
       w[iW] = R(0);
@@ -1190,6 +1272,13 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
     });
   __syncthreads();
 
+  // The cell inputs of the finalisation, copied while the block reconstructed.
+  if (pref && !__syncthreads_and(tma::mbar_wait(bar + 1, 0))) {
+    if (tid == 0) atomicOr(G.err, ERR_TMA);
+    tma::mbar_wait(bar + 1, 0);
+    return;
+  }
+
   // 3. Each thread takes the Riemann fluxes through the two faces of its
   // cell (face k0+fz lies between the cells at positions fz and fz+1;
   // edge_exchange z, dynamics_rk.h:891-908) -- each inner face is computed
@@ -1223,14 +1312,16 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
   face_flux(kz + 1, Ft);
   const size_t idx = size_t(k) * NP + row + gi;
   R qin[S], tx[S];
+  const int cq = kz * TX + c;   // the cell in the [S][TZ][TX] buffers
 #pragma unroll
   for (int s2 = 0; s2 < S; s2++) {
-    qin[s2] = sin[s2 * G.N + idx];
-    tx[s2] = txy[s2 * G.N + idx];
+    qin[s2] = pref ? QIN[s2 * TZ * TX + cq] : sin[s2 * G.N + idx];
+    tx[s2] = pref ? TXY[s2 * TZ * TX + cq] : txy[s2 * G.N + idx];
     dF[s2] = __fsub_rn(Ft[s2], Fb[s2]);   // not fused with the flux products: the march's bits
   }
-  finish_cell<R, NTR, IMM>(G, qin, tx, [&](int s2) { return sn[s2 * G.N + idx]; }, dF, sn != nullptr, a_n, a_dt,
-                           n_enforce, idx, k, sout);
+  finish_cell<R, NTR, IMM>(
+      G, qin, tx, [&](int s2) { return pref ? SN[s2 * TZ * TX + cq] : sn[s2 * G.N + idx]; }, dF, sn != nullptr,
+      a_n, a_dt, n_enforce, idx, k, sout);
 }
 
 // a += b elementwise.

@@ -515,6 +515,10 @@ struct ImplBase {
     PU_CK(cudaStreamSynchronize(st));
     if (h) {
       PU_CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+      if (h & ERR_TMA) {
+        set_error("a tile copy (TMA) did not complete within its wait limit; the step's results are invalid");
+        return PU_ERR_CUDA;
+      }
       set_error("the dycore state became non-finite");
       return PU_ERR_NONFINITE;
     }
@@ -548,6 +552,29 @@ struct Impl : ImplBase {
   static constexpr int ZTX = 32, ZTY = 4;            // z-march columns per block
   LevelTables<R> lt{};
   bool small_tile = false;
+  // TMA staging of the tiled z kernel: maps per stage-input buffer s[b]
+  // (halo and cell boxes of s[b], the cell boxes of s[0] and txy).
+  ZtMaps zt_maps[3];
+  bool zt_tma = false;
+
+  // Tensor maps of the state buffers for the tiled z kernel (host-side
+  // encoding only, no allocation).  Off when the config asks for thread
+  // loads or a buffer breaks a TMA rule.
+  void make_maps() {
+    zt_tma = false;
+    if constexpr (std::is_same<R, float>::value) {
+      if (cfg.thread_loads) return;
+      const int nx = cfg.nx, ny = cfg.ny, nz = cfg.nz;
+      bool ok = true;
+      for (int b = 0; b < 3 && ok; b++) {
+        ok = tma::encode_state(&zt_maps[b].raw, s[b], nx, ny, nz, S, ZT_X, 1, ZT_Z + 10, S) &&
+             tma::encode_state(&zt_maps[b].qin, s[b], nx, ny, nz, S, ZT_X, 1, ZT_Z, S) &&
+             tma::encode_state(&zt_maps[b].sn, s[0], nx, ny, nz, S, ZT_X, 1, ZT_Z, S) &&
+             tma::encode_state(&zt_maps[b].txy, txy, nx, ny, nz, S, ZT_X, 1, ZT_Z, S);
+      }
+      zt_tma = ok;
+    }
+  }
 
   ~Impl() override {
     if (!owns) return;
@@ -608,6 +635,7 @@ struct Impl : ImplBase {
     diag_blocks = 296;
     PU_TRY(dalloc(diag_part, size_t(diag_blocks) * NDIAG * 2));
     PU_TRY(dalloc(diag_out, size_t(NDIAG)));
+    make_maps();
     return configure();
   }
 
@@ -640,9 +668,9 @@ struct Impl : ImplBase {
                                int(ZShape<R, NTR, ZTX, ZTY>::bytes)));
     if constexpr (std::is_same<R, float>::value) {
       PU_CK(cudaFuncSetAttribute(k_zt<NTR, ZT_X, ZT_Z, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(ZTShape<NTR, ZT_X, ZT_Z, false>::bytes)));
+                                 int(ZTShape<NTR, ZT_X, ZT_Z, false>::tma_bytes)));
       PU_CK(cudaFuncSetAttribute(k_zt<NTR, ZT_X, ZT_Z, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(ZTShape<NTR, ZT_X, ZT_Z, true>::bytes)));
+                                 int(ZTShape<NTR, ZT_X, ZT_Z, true>::tma_bytes)));
       PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, LTX, LTY, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(XYShape<R, NTR, LTX, LTY, false, true>::bytes)));
       PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, LTX, LTY, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -938,9 +966,15 @@ struct Impl : ImplBase {
     cudaEvent_t e1 = prof_begin();
     if constexpr (std::is_same<R, float>::value) {
       if (z_tiled(L)) {
+        using Zs = ZTShape<NTR, ZT_X, ZT_Z, IMM>;
         dim3 gt(blocks(cfg.nx, ZT_X), cfg.ny, blocks(cfg.nz, ZT_Z));
-        k_zt<NTR, ZT_X, ZT_Z, IMM><<<gt, ZT_X * ZT_Z, ZTShape<NTR, ZT_X, ZT_Z, IMM>::bytes, st>>>(G, sin, sn, sout, t, a_n,
-                                                                                           a_dt, n_enforce);
+        // The maps of this stage input (s[b]); the cell maps of sn and txy
+        // are the same for every b.
+        int b = 0;
+        while (b < 2 && static_cast<const void *>(sin) != s[b]) b++;
+        const bool use_tma = zt_tma && static_cast<const void *>(sin) == s[b];
+        k_zt<NTR, ZT_X, ZT_Z, IMM><<<gt, ZT_X * ZT_Z, use_tma ? Zs::tma_bytes : Zs::bytes, st>>>(
+            G, sin, sn, sout, t, a_n, a_dt, n_enforce, zt_maps[b], use_tma ? 1 : 0);
         PU_LAUNCHED();
         prof_end(1, e1);
         return PU_OK;
@@ -1401,6 +1435,7 @@ struct Impl : ImplBase {
     im.lt.rt_target = im.lt.theta_e + (c.nz + 1);
     for (int b = 0; b < 3; b++) im.s[b] = take(size_t(im.S) * im.N * sizeof(R));
     im.txy = take(size_t(im.S) * im.N * sizeof(R));
+    im.make_maps();
     int rc = im.configure();
     if (rc) return rc;
     // The array keeps the previous call's contents: the error word must start at zero.

@@ -128,6 +128,7 @@ int check_config(const pu_config *c) {
   if (c->weno_mode != PU_WENO_PLAIN && c->weno_mode != PU_WENO_LEARNED) return fail(PU_ERR_INVALID, "bad WENO mode");
   if (!(c->gamma_d > 1 && c->C0 > 0 && c->R_d > 0 && c->cfl > 0)) return fail(PU_ERR_INVALID, "bad thermodynamic options");
   if (c->z_chunk < 0) return fail(PU_ERR_INVALID, "z_chunk must be >= 0");
+  if (c->thread_loads != 0 && c->thread_loads != 1) return fail(PU_ERR_INVALID, "thread_loads must be 0 or 1");
   return PU_OK;
 }
 }  // namespace pu

@@ -1,0 +1,52 @@
+"""TMA staging of the stage kernels' tiles gives the same bits as the
+threads' own loads (pu_config.thread_loads = 1).
+
+The tiled z kernel copies its raw tile (levels k0-5 .. k0+36) and, where
+the buffers fit beside four blocks per SM (up to three tracers), the cell
+inputs of its finalisation with bulk tensor copies; wall halo levels come
+from the replicated boundary row of the box, the wrapped levels of a
+periodic z from the threads, columns beyond the domain read zero (their
+results are discarded).  Cases: walls and periodic z, immersed cells, one to
+four tracers (with and without the prefetched cell inputs), partial tiles in
+x (nx = 20, 52) and z (nz = 40), and a grid whose nx breaks the TMA stride
+rule (nx % 4 != 0: thread loads everywhere).
+"""
+import numpy as np
+import pytest
+
+from porturb_b200 import cases
+from helpers import gpu_run
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "abl_64x48x40": lambda: cases.abl_neutral(nx=64, ny=48, nz=40),
+    "urban_52x40x48": lambda: cases.urban_canopy(nx=52, ny=40, nz=48, dx=2.0),
+    "mixed_periodic_z": lambda: cases.small_mixed(nx=20, ny=12, nz=40, bc_z="periodic"),
+    "mixed_immersed_3tr": lambda: cases.small_mixed(nx=24, ny=16, nz=36, ntr=3),
+    "mixed_4tr_precursor": lambda: cases.small_mixed(nx=32, ny=16, nz=24, ntr=4, bc_x="precursor"),
+    "odd_nx_no_tma": lambda: cases.small_mixed(nx=18, ny=10, nz=20),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_tma_staging_equals_thread_loads(name, gpu_lib):
+    case = CASES[name]()
+    runs = []
+    for thread_loads in (False, True):
+        st, tr, g = gpu_run(case, "f32", 0, 1.0, thread_loads=thread_loads)
+        dt = g.compute_time_step()
+        g.advance(dt, 3)
+        g.synchronize()
+        st, tr = g.get_conserved()
+        rd, u, v, w, T, trc = [np.ascontiguousarray(np.array(a)) for a in case.coupler_arrays(perturbed=True)]
+        trs = [np.ascontiguousarray(x) for x in trc]
+        n = g.time_step(rd, u, v, w, T, trs, 2.5 * dt)
+        g.close()
+        assert n == 3
+        runs.append((st, tr, [rd, u, v, w, T] + trs))
+    (a_st, a_tr, a_cpl), (b_st, b_tr, b_cpl) = runs
+    assert np.array_equal(a_st, b_st), np.abs(a_st - b_st).max()
+    assert np.array_equal(a_tr, b_tr)
+    for x, y in zip(a_cpl, b_cpl):
+        assert np.array_equal(x, y)

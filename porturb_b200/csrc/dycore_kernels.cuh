@@ -144,28 +144,41 @@ __device__ __forceinline__ R pow1pm1(const Grid<R> &G, R x) {
   return pu_expm1(G.gamma * pu_log1p(x));
 }
 
-// Primitive perturbation fields of one cell (dynamics_rk.h:550-558):
-// rho', u, v, w, theta', p', tracer mixing ratios.  theta' and p' are formed
-// from the perturbation storage without cancellation:
+template <class R, int NTR>
+__device__ __forceinline__ void load_cell(const Grid<R> &G, const R *__restrict__ s, size_t idx, R (&q)[5 + NTR]) {
+#pragma unroll
+  for (int v = 0; v < 5 + NTR; v++) q[v] = __ldg(s + v * G.N + idx);
+}
+
+// Primitive perturbation fields of one cell (dynamics_rk.h:550-558) from its
+// S raw fields q at level k: rho', u, v, w, theta', p', tracer mixing
+// ratios.  theta' and p' are formed from the perturbation storage without
+// cancellation:
 //   theta' = (q4 - theta_h q0)/rho,   p' = P0_h*((1 + q4/(rho theta)_h)^gamma - 1) + (P0_h - p_h).
-// s holds the S raw fields N elements apart (the resident arrays, N = nz*ny*nx,
-// or a halo slab).
+template <class R, int NTR>
+__device__ __forceinline__ void prims_of(const Grid<R> &G, const R (&q)[5 + NTR], int k, R (&w)[6 + NTR]) {
+  const int kh = k + HS;
+  R rho = __ldg(G.rho_h + kh) + q[0];
+  R rr = R(1) / rho;
+  w[0] = q[0];
+  w[1] = q[1] * rr;
+  w[2] = q[2] * rr;
+  w[3] = q[3] * rr;
+  w[4] = (q[4] - __ldg(G.theta_h + kh) * q[0]) * rr;
+  w[5] = fma(__ldg(G.p0_h + kh), pow1pm1(G, q[4] * __ldg(G.rt_inv + kh)), __ldg(G.dp_h + kh));
+#pragma unroll
+  for (int t = 0; t < NTR; t++) w[6 + t] = q[5 + t] * rr;
+}
+
+// The same from a state whose S fields lie N elements apart (the resident
+// arrays, N = nz*ny*nx, or a halo slab).
 template <class R, int NTR>
 __device__ __forceinline__ void prims_s(const Grid<R> &G, const R *__restrict__ s, size_t N, size_t idx, int k,
                                         R (&w)[6 + NTR]) {
-  const int kh = k + HS;
-  R q0 = __ldg(s + idx), q1 = __ldg(s + N + idx), q2 = __ldg(s + 2 * N + idx), q3 = __ldg(s + 3 * N + idx),
-    q4 = __ldg(s + 4 * N + idx);
-  R rho = __ldg(G.rho_h + kh) + q0;
-  R rr = R(1) / rho;
-  w[0] = q0;
-  w[1] = q1 * rr;
-  w[2] = q2 * rr;
-  w[3] = q3 * rr;
-  w[4] = (q4 - __ldg(G.theta_h + kh) * q0) * rr;
-  w[5] = fma(__ldg(G.p0_h + kh), pow1pm1(G, q4 * __ldg(G.rt_inv + kh)), __ldg(G.dp_h + kh));
+  R q[5 + NTR];
 #pragma unroll
-  for (int t = 0; t < NTR; t++) w[6 + t] = __ldg(s + (5 + t) * N + idx) * rr;
+  for (int v = 0; v < 5 + NTR; v++) q[v] = __ldg(s + v * N + idx);
+  prims_of<R, NTR>(G, q, k, w);
 }
 
 template <class R, int NTR>
@@ -284,10 +297,42 @@ struct XYShape {
   // fallback queue (16-bit stencil indices) lives in the flux buffer, which
   // is idle while edges are reconstructed.
   static constexpr size_t learned_bytes = LEARNED ? size_t(NT / 32) * mlp::WARP_SMEM_BYTES + 16 : 0;
-  static constexpr size_t bytes = sizeof(R) * (size_t(F) * HY * HX + 2 * size_t(F) * EN + size_t(S) * FN + YON) +
-                                  (IMM ? MB + MASKB : 0) + learned_bytes;
+  static constexpr size_t layout_bytes = sizeof(R) * (size_t(F) * HY * HX + 2 * size_t(F) * EN + size_t(S) * FN + YON) +
+                                         (IMM ? MB + MASKB : 0) + learned_bytes;
+  // TMA staging of the 16x16 tile (FP32): the raw stage input of the tile's
+  // cross -- the 16x16 interior, 5 rows above and below, 5 columns left and
+  // right, the latter in 8-column boxes -- and, on immersed domains, its
+  // flag bytes (16-byte-wide boxes), land in the edge and flux buffers, idle
+  // until the primitive fields are formed; one mbarrier after the layout.
+  // The kernel rounds its dynamic shared memory up to 128 bytes (PAD).
+  static constexpr size_t PAD = 128;
+  static constexpr size_t al(size_t b) { return (b + 127) / 128 * 128; }
+  static constexpr size_t h_bytes = sizeof(R) * size_t(F) * HY * HX;
+  static constexpr size_t st_in = al(h_bytes);                      // [S][16][16]
+  static constexpr size_t st_top = al(st_in + sizeof(R) * S * 256);  // [S][5][16]
+  static constexpr size_t st_bot = al(st_top + sizeof(R) * S * 80);  // [S][5][16]
+  static constexpr size_t st_west = al(st_bot + sizeof(R) * S * 80); // [S][16][8]
+  static constexpr size_t st_east = al(st_west + sizeof(R) * S * 128);
+  static constexpr size_t fl_in = al(st_east + sizeof(R) * S * 128);  // [16][16] flag bytes
+  static constexpr size_t fl_top = fl_in + 256;                       // [5][16]
+  static constexpr size_t fl_bot = fl_top + 128;                      // [5][16]
+  static constexpr size_t fl_west = fl_bot + 128;                     // [16][16], columns i0-16 ..
+  static constexpr size_t fl_east = fl_west + 256;                    // [16][16]
+  static constexpr size_t stage_end = fl_east + 256;
+  static constexpr size_t yo_off = h_bytes + sizeof(R) * (2 * size_t(F) * EN + size_t(S) * FN);
+  static constexpr bool TMA_FITS = TX == 16 && TY == 16 && sizeof(R) == 4 && !LEARNED && stage_end <= yo_off;
+  static constexpr size_t bar_off = al(layout_bytes);
+  static constexpr size_t bytes = bar_off + 16 + PAD;
   static_assert(!LEARNED || size_t(F) * EN * 2 <= sizeof(R) * S * FN, "fallback queue exceeds the flux buffer");
   static_assert(NT % 32 == 0, "whole warps");
+};
+
+// Tensor maps of one k_xy launch (TMA staging, 16x16 tiles): the stage input
+// with the boxes (16, 16, 1, S) interior, (16, 5, 1, S) halo rows and
+// (8, 16, 1, S) halo columns; the immersed flags with (16, 16, 1) and
+// (16, 5, 1).
+struct XyMaps {
+  CUtensorMap in, ns, ew, fin, fns;
 };
 
 // Edge reconstruction of `total` stencils with learned weights by the NT
@@ -447,11 +492,17 @@ __device__ __forceinline__ void recon_outer_pair(int f, int line, Load load, Sto
 // x/y fluxes and their divergence for one (x,y) tile of one level.
 // LEARNED (FP32, weno_all only): edges from the network's weights, with the
 // plain limiter as the fallback.
+// use_tma (16x16 FP32 tiles of an undecomposed plain domain): a tile that
+// lies whole in the domain takes its cross from TMA copies (maps: tensor maps
+// of sin and of the flags), the halo rows and columns wrapping periodically
+// box by box; tiles at a precursor edge, partial tiles and halo boxes that
+// would straddle the domain's edge are loaded by the threads.
 template <class R, int NTR, int TX, int TY, bool IMM, bool LEARNED = false, bool DECOMP = false>
-__global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (sizeof(R) == 4 ? PU_XY_MIN_BLOCKS : 1)) k_xy(const Grid<R> G, const R *__restrict__ sin, R *__restrict__ txy) {
+__global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (sizeof(R) == 4 ? PU_XY_MIN_BLOCKS : 1)) k_xy(const Grid<R> G, const R *__restrict__ sin, R *__restrict__ txy, const __grid_constant__ XyMaps maps, int use_tma) {
   using Sh = XYShape<R, NTR, TX, TY, IMM, LEARNED>;
   constexpr int F = Sh::F, S = Sh::S, NT = Sh::NT, HX = Sh::HX, HY = Sh::HY, EN = Sh::EN, FN = Sh::FN;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_xy[];
+  unsigned char *smem_raw = smem_xy + ((128u - (tma::saddr(smem_xy) & 127u)) & 127u);
   R *H = reinterpret_cast<R *>(smem_raw);
   R *EL = H + F * HY * HX;
   R *ER = EL + F * EN;
@@ -472,6 +523,54 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
   const bool sim2d = G.sim2d != 0;
   if (LEARNED && tid < 2) qn[tid] = 0;
 
+  // 0. TMA staging of the tile's cross (block-uniform decision).  Box origins:
+  // the interior at (i0, j0); the 5 rows above at j0-5 (ny-5 for the first
+  // tile row), below at j0+16 (0 for the last); the 8 columns left at i0-8
+  // (nx-8), right at i0+16 (0); the flags' 16-wide side boxes at i0-16 (nx-16)
+  // and i0+16 (0).  Every x origin is a multiple of 8 (16 for the flags).
+  bool staged = false;
+  if constexpr (Sh::TMA_FITS && !DECOMP) {
+    if (use_tma && !sim2d && i0 + TX <= nx && j0 + TY <= ny) {
+      const bool px = G.bc_x != BC_PRECURSOR, py = G.bc_y != BC_PRECURSOR;
+      const int xw = i0 > 0 ? i0 - 8 : (px ? nx - 8 : -1);
+      const int xe = i0 + TX < nx ? (i0 + TX + 8 <= nx ? i0 + TX : -1) : (px ? 0 : -1);
+      const int yn = j0 > 0 ? j0 - 5 : (py ? ny - 5 : -1);
+      const int ys = j0 + TY < ny ? (j0 + TY + 5 <= ny ? j0 + TY : -1) : (py ? 0 : -1);
+      const int fw = i0 > 0 ? i0 - 16 : nx - 16;
+      const int fe = i0 + TX < nx ? (i0 + TX + 16 <= nx ? i0 + TX : -1) : 0;
+      const int fn = j0 > 0 ? j0 - 5 : ny - 5, fs = j0 + TY < ny ? (j0 + TY + 5 <= ny ? j0 + TY : -1) : 0;
+      staged = xw >= 0 && xe >= 0 && yn >= 0 && ys >= 0 && (!IMM || (fw >= 0 && fe >= 0 && fn >= 0 && fs >= 0));
+      if (staged) {
+        uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + Sh::bar_off);
+        if (tid == 0) {
+          tma::mbar_init(bar);
+          tma::mbar_expect(bar, uint32_t(sizeof(R) * S * (256 + 80 + 80 + 128 + 128) +
+                                         (IMM ? 256 + 80 + 80 + 256 + 256 : 0)));
+          tma::load_4d(smem_raw + Sh::st_in, &maps.in, i0, j0, k, 0, bar);
+          tma::load_4d(smem_raw + Sh::st_top, &maps.ns, i0, yn, k, 0, bar);
+          tma::load_4d(smem_raw + Sh::st_bot, &maps.ns, i0, ys, k, 0, bar);
+          tma::load_4d(smem_raw + Sh::st_west, &maps.ew, xw, j0, k, 0, bar);
+          tma::load_4d(smem_raw + Sh::st_east, &maps.ew, xe, j0, k, 0, bar);
+          if (IMM) {
+            tma::load_3d(smem_raw + Sh::fl_in, &maps.fin, i0, j0, k, bar);
+            tma::load_3d(smem_raw + Sh::fl_top, &maps.fns, i0, fn, k, bar);
+            tma::load_3d(smem_raw + Sh::fl_bot, &maps.fns, i0, fs, k, bar);
+            tma::load_3d(smem_raw + Sh::fl_west, &maps.fin, fw, j0, k, bar);
+            tma::load_3d(smem_raw + Sh::fl_east, &maps.fin, fe, j0, k, bar);
+          }
+        }
+        __syncthreads();
+        if (!__syncthreads_and(tma::mbar_wait(bar, 0))) {
+          // The copies did not complete: report it, give them a last bounded
+          // wait, and give up the tile.
+          if (tid == 0) atomicOr(G.err, ERR_TMA);
+          tma::mbar_wait(bar, 0);
+          return;
+        }
+      }
+    }
+  }
+
   // 1. Primitive fields of the tile, its x halo rows and its y halo columns.
   constexpr int NA = TY * HX, NB = 10 * TX;
   for (int it = tid; it < NA + (sim2d ? 0 : NB); it += NT) {
@@ -486,7 +585,38 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
     }
     const int gi = i0 - 5 + c, gj = j0 - 5 + r;
     R w[F];
-    if constexpr (DECOMP) {
+    if (Sh::TMA_FITS && !DECOMP && staged) {
+      // The cell's place in the staged boxes ([S][rows][cols]) and its flag.
+      const R *src;
+      int fstride;
+      const uint8_t *fb;
+      if (r < 5) {
+        src = reinterpret_cast<const R *>(smem_raw + Sh::st_top) + r * 16 + (c - 5);
+        fstride = 80;
+        fb = smem_raw + Sh::fl_top + r * 16 + (c - 5);
+      } else if (r >= 5 + TY) {
+        src = reinterpret_cast<const R *>(smem_raw + Sh::st_bot) + (r - 5 - TY) * 16 + (c - 5);
+        fstride = 80;
+        fb = smem_raw + Sh::fl_bot + (r - 5 - TY) * 16 + (c - 5);
+      } else if (c < 5) {
+        src = reinterpret_cast<const R *>(smem_raw + Sh::st_west) + (r - 5) * 8 + (c + 3);
+        fstride = 128;
+        fb = smem_raw + Sh::fl_west + (r - 5) * 16 + (c + 11);
+      } else if (c >= 5 + TX) {
+        src = reinterpret_cast<const R *>(smem_raw + Sh::st_east) + (r - 5) * 8 + (c - 5 - TX);
+        fstride = 128;
+        fb = smem_raw + Sh::fl_east + (r - 5) * 16 + (c - 5 - TX);
+      } else {
+        src = reinterpret_cast<const R *>(smem_raw + Sh::st_in) + (r - 5) * 16 + (c - 5);
+        fstride = 256;
+        fb = smem_raw + Sh::fl_in + (r - 5) * 16 + (c - 5);
+      }
+      R q[S];
+#pragma unroll
+      for (int s2 = 0; s2 < S; s2++) q[s2] = src[s2 * fstride];
+      prims_of<R, NTR>(G, q, k, w);
+      if (IMM) M[r * HX + c] = *fb;
+    } else if constexpr (DECOMP) {
       const R *src;
       size_t fs, q;
       const uint8_t *fl;
@@ -767,27 +897,6 @@ struct ZShape {
 };
 
 // Raw state of one cell (S values) for a later conversion to primitive fields.
-template <class R, int NTR>
-__device__ __forceinline__ void load_cell(const Grid<R> &G, const R *__restrict__ s, size_t idx, R (&q)[5 + NTR]) {
-#pragma unroll
-  for (int v = 0; v < 5 + NTR; v++) q[v] = __ldg(s + v * G.N + idx);
-}
-
-template <class R, int NTR>
-__device__ __forceinline__ void prims_of(const Grid<R> &G, const R (&q)[5 + NTR], int k, R (&w)[6 + NTR]) {
-  const int kh = k + HS;
-  R rho = __ldg(G.rho_h + kh) + q[0];
-  R rr = R(1) / rho;
-  w[0] = q[0];
-  w[1] = q[1] * rr;
-  w[2] = q[2] * rr;
-  w[3] = q[3] * rr;
-  w[4] = (q[4] - __ldg(G.theta_h + kh) * q[0]) * rr;
-  w[5] = fma(__ldg(G.p0_h + kh), pow1pm1(G, q[4] * __ldg(G.rt_inv + kh)), __ldg(G.dp_h + kh));
-#pragma unroll
-  for (int t = 0; t < NTR; t++) w[6 + t] = q[5 + t] * rr;
-}
-
 // The end of one cell's stage in both z kernels: tend = txy - dF/dz plus
 // gravity and Coriolis, the combination a_n*sn + (1-a_n)*sin + a_dt*tend
 // (sn null: sin + a_dt*tend), n_enforce applications of the immersed and

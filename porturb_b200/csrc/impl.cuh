@@ -556,6 +556,10 @@ struct Impl : ImplBase {
   // (halo and cell boxes of s[b], the cell boxes of s[0] and txy).
   ZtMaps zt_maps[3];
   bool zt_tma = false;
+  // TMA staging of the 16x16 x/y kernel: per stage-input buffer s[b] the
+  // interior, halo-row and halo-column boxes, and the flags' boxes.
+  XyMaps xy_maps[3];
+  bool xy_tma = false, xy_tma_flags = false;
 
   // Tensor maps of the state buffers for the tiled z kernel (host-side
   // encoding only, no allocation).  Off when the config asks for thread
@@ -573,6 +577,19 @@ struct Impl : ImplBase {
              tma::encode_state(&zt_maps[b].txy, txy, nx, ny, nz, S, ZT_X, 1, ZT_Z, S);
       }
       zt_tma = ok;
+      ok = XTX_BIG == 16 && XTY_BIG == 16;
+      for (int b = 0; b < 3 && ok; b++) {
+        ok = tma::encode_state(&xy_maps[b].in, s[b], nx, ny, nz, S, 16, 16, 1, S) &&
+             tma::encode_state(&xy_maps[b].ns, s[b], nx, ny, nz, S, 16, 5, 1, S) &&
+             tma::encode_state(&xy_maps[b].ew, s[b], nx, ny, nz, S, 8, 16, 1, S);
+      }
+      xy_tma = ok;
+      xy_tma_flags = ok && flags && tma::encode_bytes3(&xy_maps[0].fin, flags, nx, ny, nz, 16, 16, 1) &&
+                     tma::encode_bytes3(&xy_maps[0].fns, flags, nx, ny, nz, 16, 5, 1);
+      for (int b = 1; b < 3 && xy_tma_flags; b++) {
+        xy_maps[b].fin = xy_maps[0].fin;
+        xy_maps[b].fns = xy_maps[0].fns;
+      }
     }
   }
 
@@ -882,6 +899,7 @@ struct Impl : ImplBase {
     k_imm_finish<R><<<blocks(N, 256), 256, 0, st>>>(dprop, a, dzero, cfg.immersed_power, N, flags,
                                                     static_cast<R *>(imm_mult));
     PU_LAUNCHED();
+    make_maps();   // the flags' maps, now that the flags exist
     // has_imm: any flag set (a cell with prop > 0 has distance 0 in `a`).
     std::vector<uint8_t> hf(N);
     PU_CK(cudaMemcpyAsync(hf.data(), flags, N, cudaMemcpyDeviceToHost, st));
@@ -946,18 +964,22 @@ struct Impl : ImplBase {
     constexpr bool L = LRN && std::is_same<R, float>::value && !DEC;
     R *t = static_cast<R *>(txy);
     cudaEvent_t e0 = prof_begin();
+    int b = 0;   // sin is s[b]: the tensor maps of that buffer
+    while (b < 2 && static_cast<const void *>(sin) != s[b]) b++;
     if (small_tile) {
       using Sh = XYShape<R, NTR, XTX_SM, XTY_SM, IMM, L>;
       dim3 g(blocks(cfg.nx, XTX_SM), blocks(cfg.ny, XTY_SM), cfg.nz);
-      k_xy<R, NTR, XTX_SM, XTY_SM, IMM, L, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
+      k_xy<R, NTR, XTX_SM, XTY_SM, IMM, L, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b], 0);
     } else if (L) {
       using Sh = XYShape<R, NTR, LTX, LTY, IMM, L>;
       dim3 g(blocks(cfg.nx, LTX), blocks(cfg.ny, LTY), cfg.nz);
-      k_xy<R, NTR, LTX, LTY, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
+      k_xy<R, NTR, LTX, LTY, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b], 0);
     } else {
       using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM, false>;
       dim3 g(blocks(cfg.nx, XTX_BIG), blocks(cfg.ny, XTY_BIG), cfg.nz);
-      k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t);
+      const bool use_tma = !DEC && xy_tma && (!IMM || xy_tma_flags) && static_cast<const void *>(sin) == s[b];
+      k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b],
+                                                                                     use_tma ? 1 : 0);
     }
     PU_LAUNCHED();
     prof_end(0, e0);
@@ -970,8 +992,6 @@ struct Impl : ImplBase {
         dim3 gt(blocks(cfg.nx, ZT_X), cfg.ny, blocks(cfg.nz, ZT_Z));
         // The maps of this stage input (s[b]); the cell maps of sn and txy
         // are the same for every b.
-        int b = 0;
-        while (b < 2 && static_cast<const void *>(sin) != s[b]) b++;
         const bool use_tma = zt_tma && static_cast<const void *>(sin) == s[b];
         k_zt<NTR, ZT_X, ZT_Z, IMM><<<gt, ZT_X * ZT_Z, use_tma ? Zs::tma_bytes : Zs::bytes, st>>>(
             G, sin, sn, sout, t, a_n, a_dt, n_enforce, zt_maps[b], use_tma ? 1 : 0);

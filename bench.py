@@ -237,46 +237,6 @@ def run_reference_arm(args, world, rank):
 # ---------------------------------------------------------------------------
 # GPU pieces
 # ---------------------------------------------------------------------------
-def snapshot(g, S, shape, device):
-    """The handle's conserved variables (rho, rho*u, rho*v, rho*w, rho*theta,
-    tracers) as one FP64 device tensor (S, nz, ny, nx)."""
-    import torch
-    from porturb_b200 import capi
-    t = torch.empty((S,) + shape, dtype=torch.float64, device=device)
-    capi.check(g.lib.pu_dycore_get_conserved(g.h, t.data_ptr(), t[5].data_ptr() if S > 5 else None,
-                                             capi.PU_MEM_DEVICE))
-    return t
-
-
-def field_errors(X, D, cells, nz):
-    """Per prognostic: (L2, Linf) of X - D relative to D's departure from the
-    hydrostatic background (rho_h, 0, 0, 0, rho_h*theta_h, 0 for tracers).
-    A field that is zero in D and in X reports 0."""
-    import torch
-    hs = 4
-    r = torch.tensor(np.asarray(cells[0][hs:hs + nz]), dtype=torch.float64, device=D.device)
-    t = torch.tensor(np.asarray(cells[1][hs:hs + nz]), dtype=torch.float64, device=D.device)
-    names = ["rho", "rho_u", "rho_v", "rho_w", "rho_theta"] + ["tracer%d" % q for q in range(D.shape[0] - 5)]
-    out = {}
-    for f in range(D.shape[0]):
-        d = D[f]
-        if f == 0:
-            dep = d - r[:, None, None]
-        elif f == 4:
-            dep = d - (r * t)[:, None, None]
-        else:
-            dep = d
-        diff = X[f] - d
-        dl2 = float(torch.sqrt(torch.mean(diff * diff)))
-        dli = float(diff.abs().max())
-        pl2 = float(torch.sqrt(torch.mean(dep * dep)))
-        pli = float(dep.abs().max())
-        out[names[f]] = {"l2": dl2 / pl2 if pl2 > 0 else (0.0 if dl2 == 0 else None),
-                         "linf": dli / pli if pli > 0 else (0.0 if dli == 0 else None)}
-        del dep, diff
-    return out
-
-
 def timed_steps(g, dt, steps, stream, world):
     import torch
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -444,6 +404,7 @@ def main():
     import torch.distributed as dist
     from porturb_b200 import Dycore, build
     build.build()
+    from porturb_b200.run_case import _snapshot as snapshot, field_errors
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
@@ -451,7 +412,6 @@ def main():
     t_setup = time.perf_counter()
     case = build_case(seed=rank)
     stream = torch.cuda.Stream(device=local)
-    dev = torch.device("cuda", local)
     N = case.ncells
     S = 5 + len(case.tracers)
     shape = (case.nz, case.ny, case.nx)
@@ -477,7 +437,7 @@ def main():
     launches = g.kernel_launches() - launches0
     clk = clocks.stop()
     value = aggregate_value(N, args.steps, ms / 1e3, world)
-    P = None if args.no_f64 else snapshot(g, S, shape, dev)   # after W+K steps
+    P = None if args.no_f64 else snapshot(g, S, shape)   # after W+K steps
     kern = kernel_pass(g, dt, args.steps)
 
     # e2e through the C-ABI with pinned host coupler arrays.
@@ -514,7 +474,7 @@ def main():
         ms_l = timed_steps(g, dt, args.steps, stream, world)
         nl, nf = g.learned_counts()
         if not args.no_f64:
-            L = snapshot(g, S, shape, dev)
+            L = snapshot(g, S, shape)
         lkern = kernel_pass(g, dt, min(args.steps, 3))
         g.set_weno_mode("plain")
         learned = {"value": aggregate_value(N, args.steps, ms_l / 1e3, world), "unit": "cell-steps/s",
@@ -537,7 +497,7 @@ def main():
         for _ in range(args.warmup):
             h.advance(dt, 1)
         ms_64 = timed_steps(h, dt, args.steps, stream, world)
-        D = snapshot(h, S, shape, dev)
+        D = snapshot(h, S, shape)
         cells, _ = h.get_hydrostasis()
         h.close()
         del h

@@ -36,6 +36,11 @@ namespace pu {
 
 // Packed FP32 limiter (two stencils per FFMA2/FADD2/FMUL2) in the plain x/y
 // kernel; 0 keeps the scalar limiter (results are identical).
+// 1: the x/y kernel stages the immersed flags of its tile through TMA with
+// the state; 0: the threads load them.
+#ifndef PU_XY_TMA_FLAGS
+#define PU_XY_TMA_FLAGS 1
+#endif
 #ifndef PU_PACKED_LIMITER
 #define PU_PACKED_LIMITER 1
 #endif
@@ -539,19 +544,20 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
       const int fw = i0 > 0 ? i0 - 16 : nx - 16;
       const int fe = i0 + TX < nx ? (i0 + TX + 16 <= nx ? i0 + TX : -1) : 0;
       const int fn = j0 > 0 ? j0 - 5 : ny - 5, fs = j0 + TY < ny ? (j0 + TY + 5 <= ny ? j0 + TY : -1) : 0;
-      staged = xw >= 0 && xe >= 0 && yn >= 0 && ys >= 0 && (!IMM || (fw >= 0 && fe >= 0 && fn >= 0 && fs >= 0));
+      constexpr bool TF = IMM && PU_XY_TMA_FLAGS;
+      staged = xw >= 0 && xe >= 0 && yn >= 0 && ys >= 0 && (!TF || (fw >= 0 && fe >= 0 && fn >= 0 && fs >= 0));
       if (staged) {
         uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + Sh::bar_off);
         if (tid == 0) {
           tma::mbar_init(bar);
           tma::mbar_expect(bar, uint32_t(sizeof(R) * S * (256 + 80 + 80 + 128 + 128) +
-                                         (IMM ? 256 + 80 + 80 + 256 + 256 : 0)));
+                                         (TF ? 256 + 80 + 80 + 256 + 256 : 0)));
           tma::load_4d(smem_raw + Sh::st_in, &maps.in, i0, j0, k, 0, bar);
           tma::load_4d(smem_raw + Sh::st_top, &maps.ns, i0, yn, k, 0, bar);
           tma::load_4d(smem_raw + Sh::st_bot, &maps.ns, i0, ys, k, 0, bar);
           tma::load_4d(smem_raw + Sh::st_west, &maps.ew, xw, j0, k, 0, bar);
           tma::load_4d(smem_raw + Sh::st_east, &maps.ew, xe, j0, k, 0, bar);
-          if (IMM) {
+          if (TF) {
             tma::load_3d(smem_raw + Sh::fl_in, &maps.fin, i0, j0, k, bar);
             tma::load_3d(smem_raw + Sh::fl_top, &maps.fns, i0, fn, k, bar);
             tma::load_3d(smem_raw + Sh::fl_bot, &maps.fns, i0, fs, k, bar);
@@ -615,7 +621,7 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
 #pragma unroll
       for (int s2 = 0; s2 < S; s2++) q[s2] = src[s2 * fstride];
       prims_of<R, NTR>(G, q, k, w);
-      if (IMM) M[r * HX + c] = *fb;
+      if (IMM) M[r * HX + c] = PU_XY_TMA_FLAGS ? *fb : __ldg(G.flags + plane + size_t(wrapi(gj, ny)) * nx + wrapi(gi, nx));
     } else if constexpr (DECOMP) {
       const R *src;
       size_t fs, q;

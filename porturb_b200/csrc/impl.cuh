@@ -977,7 +977,8 @@ struct Impl : ImplBase {
     } else {
       using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM, false>;
       dim3 g(blocks(cfg.nx, XTX_BIG), blocks(cfg.ny, XTY_BIG), cfg.nz);
-      const bool use_tma = !DEC && xy_tma && (!IMM || xy_tma_flags) && static_cast<const void *>(sin) == s[b];
+      const bool use_tma = !DEC && xy_tma && (!IMM || !PU_XY_TMA_FLAGS || xy_tma_flags) &&
+                           static_cast<const void *>(sin) == s[b];
       k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b],
                                                                                      use_tma ? 1 : 0);
     }

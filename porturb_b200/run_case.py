@@ -3,6 +3,7 @@
     python -m porturb_b200.run_case abl_neutral --nx 256 --ny 256 --nz 64 --steps 3
     python -m porturb_b200.run_case abl_neutral --nz 64 --learned --train-steps 300
     python -m porturb_b200.run_case urban_canopy --nx 1024 --ny 1024 --nz 256 --dx 1 --steps 300 --diag-every 50
+    python -m porturb_b200.run_case abl_neutral --nx 512 --ny 512 --nz 256 --steps 500 --compare
 
 Plain mode advances the FP32 (or --precision f64) dycore; --learned first
 harvests stencils from the initial state, trains the network on the GPU and
@@ -10,7 +11,11 @@ then advances with learned weights; --modules times the physics modules
 (LES closure, sponge, geostrophic forcing, surface fluxes) instead; --driver
 runs the reference driver's whole chain of modules per dt_phys.  Prints
 one JSON line with the per-kernel CUDA-event times and, in learned mode, the
-fallback fraction.
+fallback fraction.  --compare runs the plain FP32 form, the learned form
+(trained on stencils harvested from the initial state) and the FP64 build
+from the same initial state for `steps` steps each and reports their rates
+and, per prognostic, the L2 and Linf error of the FP32 forms against the
+FP64 build relative to its departure from the hydrostatic background.
 """
 from __future__ import annotations
 
@@ -115,6 +120,93 @@ def run_driver(case, a):
             "note": "cell-steps/s of the whole driver step: the dycore's 10 steps and the modules beside it"}
 
 
+def _snapshot(g, S, shape):
+    """Conserved variables of a handle as one FP64 device tensor (S, nz, ny, nx)."""
+    import torch
+    from . import capi
+    t = torch.empty((S,) + tuple(shape), dtype=torch.float64, device="cuda:%d" % g.cfg.device)
+    capi.check(g.lib.pu_dycore_get_conserved(g.h, t.data_ptr(), t[5].data_ptr() if S > 5 else None,
+                                             capi.PU_MEM_DEVICE))
+    return t
+
+
+def field_errors(X, D, cells, nz):
+    """Per prognostic: L2 and Linf of X - D over D's departure from the
+    hydrostatic background (rho_h, 0, 0, 0, rho_h*theta_h, 0 for tracers),
+    computed on the GPU in FP64.  A field that is zero in D and in X reports 0;
+    one that is zero only in D reports None."""
+    import torch
+    hs = 4
+    r = torch.tensor(np.asarray(cells[0][hs:hs + nz]), dtype=torch.float64, device=D.device)
+    t = torch.tensor(np.asarray(cells[1][hs:hs + nz]), dtype=torch.float64, device=D.device)
+    names = ["rho", "rho_u", "rho_v", "rho_w", "rho_theta"] + ["tracer%d" % q for q in range(D.shape[0] - 5)]
+    out = {}
+    for f in range(D.shape[0]):
+        d = D[f]
+        dep = d - r[:, None, None] if f == 0 else (d - (r * t)[:, None, None] if f == 4 else d)
+        diff = X[f] - d
+        dl2, dli = float(torch.sqrt(torch.mean(diff * diff))), float(diff.abs().max())
+        pl2, pli = float(torch.sqrt(torch.mean(dep * dep))), float(dep.abs().max())
+        out[names[f]] = {"l2": dl2 / pl2 if pl2 > 0 else (0.0 if dl2 == 0 else None),
+                         "linf": dli / pli if pli > 0 else (0.0 if dli == 0 else None)}
+        del dep, diff
+    return out
+
+
+def run_compare(case, a):
+    """Plain FP32, learned and FP64 from the same initial state: rates and
+    errors against FP64 after `steps` steps."""
+    import torch
+    N, S, shape = case.ncells, 5 + len(case.tracers), (case.nz, case.ny, case.nx)
+    base = [np.ascontiguousarray(x) for x in case.coupler_arrays(perturbed=False)]
+    pert = [np.ascontiguousarray(x) for x in case.coupler_arrays(perturbed=True)]
+    prop = np.ascontiguousarray(case.immersed_proportion)
+    prop = prop if prop.any() else None
+    out = {"case": a.case, "grid": [case.nx, case.ny, case.nz], "steps": a.steps, "mode": "compare"}
+
+    def timed(g, dt, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        g.advance(dt, n)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    g = Dycore.from_case(case, precision="f32")
+    g.init(*base[:5], list(base[5]), prop)
+    g.load_state(*pert[:5], list(pert[5]))
+    dt = g.compute_time_step()
+    g.learned_harvest(a.harvest, seed=1)
+    tr = g.learned_train(a.train_steps, batch=a.batch, lr=2e-3, seed=3)
+    ms = timed(g, dt, a.steps)
+    P = _snapshot(g, S, shape)
+    out["plain"] = {"cell_steps_per_s": N * a.steps / (ms / 1e3), "ms_per_step": ms / a.steps}
+    g.load_state(*pert[:5], list(pert[5]))
+    g.set_weno_mode("learned")
+    g.learned_set_threshold(a.threshold)
+    g.learned_counts()
+    ms = timed(g, dt, a.steps)
+    nl, nf = g.learned_counts()
+    L = _snapshot(g, S, shape)
+    out["learned"] = {"cell_steps_per_s": N * a.steps / (ms / 1e3), "ms_per_step": ms / a.steps,
+                      "threshold": a.threshold, "fallback_frac": nf / max(1, nl + nf),
+                      "training": dict(tr, batch=a.batch)}
+    g.close()
+    h = Dycore.from_case(case, precision="f64")
+    h.init(*base[:5], list(base[5]), prop)
+    h.load_state(*pert[:5], list(pert[5]))
+    ms = timed(h, dt, a.steps)
+    D = _snapshot(h, S, shape)
+    cells, _ = h.get_hydrostasis()
+    h.close()
+    out["f64"] = {"cell_steps_per_s": N * a.steps / (ms / 1e3), "ms_per_step": ms / a.steps}
+    out["plain_vs_f64"] = field_errors(P, D, cells, case.nz)
+    out["learned_vs_f64"] = field_errors(L, D, cells, case.nz)
+    out["error_norm"] = "L2 and Linf of (X - FP64) over the FP64 field's departure from the hydrostatic background"
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=sorted(CASES))
@@ -130,6 +222,9 @@ def main(argv=None):
     ap.add_argument("--harvest", type=int, default=1 << 18)
     ap.add_argument("--train-steps", type=int, default=300)
     ap.add_argument("--threshold", type=float, default=0.5)
+    ap.add_argument("--batch", type=int, default=16384, help="training batch (--learned, --compare)")
+    ap.add_argument("--compare", action="store_true",
+                    help="plain FP32, learned and FP64 from the same initial state: rates and errors against FP64")
     ap.add_argument("--driver", action="store_true",
                     help="run the reference driver's module chain per dt_phys (boundary layer or urban) on device "
                          "coupler arrays")
@@ -139,6 +234,9 @@ def main(argv=None):
     a = ap.parse_args(argv)
 
     case = CASES[a.case](a)
+    if a.compare:
+        print(json.dumps(run_compare(case, a)), flush=True)
+        return
     if a.modules:
         print(json.dumps(run_modules(case, a)), flush=True)
         return
@@ -154,7 +252,7 @@ def main(argv=None):
            "weno": "learned" if a.learned else "plain"}
     if a.learned:
         g.learned_harvest(a.harvest, seed=1)
-        out["training"] = g.learned_train(a.train_steps, batch=16384, lr=2e-3, seed=3)
+        out["training"] = g.learned_train(a.train_steps, batch=a.batch, lr=2e-3, seed=3)
         g.set_weno_mode("learned")
         g.learned_set_threshold(a.threshold)
         g.learned_counts()

@@ -36,11 +36,6 @@ namespace pu {
 
 // Packed FP32 limiter (two stencils per FFMA2/FADD2/FMUL2) in the plain x/y
 // kernel; 0 keeps the scalar limiter (results are identical).
-// 1: the x/y kernel stages the immersed flags of its tile through TMA with
-// the state; 0: the threads load them.
-#ifndef PU_XY_TMA_FLAGS
-#define PU_XY_TMA_FLAGS 1
-#endif
 #ifndef PU_PACKED_LIMITER
 #define PU_PACKED_LIMITER 1
 #endif
@@ -304,12 +299,13 @@ struct XYShape {
   static constexpr size_t learned_bytes = LEARNED ? size_t(NT / 32) * mlp::WARP_SMEM_BYTES + 16 : 0;
   static constexpr size_t layout_bytes = sizeof(R) * (size_t(F) * HY * HX + 2 * size_t(F) * EN + size_t(S) * FN + YON) +
                                          (IMM ? MB + MASKB : 0) + learned_bytes;
-  // TMA staging of the 16x16 tile (FP32): the raw stage input of the tile's
-  // cross -- the 16x16 interior, 5 rows above and below, 5 columns left and
-  // right, the latter in 8-column boxes -- and, on immersed domains, its
-  // flag bytes (16-byte-wide boxes), land in the edge and flux buffers, idle
-  // until the primitive fields are formed; one mbarrier after the layout.
-  // The kernel rounds its dynamic shared memory up to 128 bytes (PAD).
+  static constexpr size_t bytes = layout_bytes;
+  // TMA staging of the 16x16 tile (FP32, the TMA instantiation): the raw
+  // stage input of the tile's cross -- the 16x16 interior, 5 rows above and
+  // below, 5 columns left and right, the latter in 8-column boxes -- lands in
+  // the edge and flux buffers, idle until the primitive fields are formed;
+  // one mbarrier after the layout.  That kernel rounds its dynamic shared
+  // memory up to 128 bytes (PAD).
   static constexpr size_t PAD = 128;
   static constexpr size_t al(size_t b) { return (b + 127) / 128 * 128; }
   static constexpr size_t h_bytes = sizeof(R) * size_t(F) * HY * HX;
@@ -318,26 +314,20 @@ struct XYShape {
   static constexpr size_t st_bot = al(st_top + sizeof(R) * S * 80);  // [S][5][16]
   static constexpr size_t st_west = al(st_bot + sizeof(R) * S * 80); // [S][16][8]
   static constexpr size_t st_east = al(st_west + sizeof(R) * S * 128);
-  static constexpr size_t fl_in = al(st_east + sizeof(R) * S * 128);  // [16][16] flag bytes
-  static constexpr size_t fl_top = fl_in + 256;                       // [5][16]
-  static constexpr size_t fl_bot = fl_top + 128;                      // [5][16]
-  static constexpr size_t fl_west = fl_bot + 128;                     // [16][16], columns i0-16 ..
-  static constexpr size_t fl_east = fl_west + 256;                    // [16][16]
-  static constexpr size_t stage_end = fl_east + 256;
+  static constexpr size_t stage_end = st_east + sizeof(R) * S * 128;
   static constexpr size_t yo_off = h_bytes + sizeof(R) * (2 * size_t(F) * EN + size_t(S) * FN);
   static constexpr bool TMA_FITS = TX == 16 && TY == 16 && sizeof(R) == 4 && !LEARNED && stage_end <= yo_off;
   static constexpr size_t bar_off = al(layout_bytes);
-  static constexpr size_t bytes = bar_off + 16 + PAD;
+  static constexpr size_t tma_bytes = bar_off + 16 + PAD;
   static_assert(!LEARNED || size_t(F) * EN * 2 <= sizeof(R) * S * FN, "fallback queue exceeds the flux buffer");
   static_assert(NT % 32 == 0, "whole warps");
 };
 
 // Tensor maps of one k_xy launch (TMA staging, 16x16 tiles): the stage input
 // with the boxes (16, 16, 1, S) interior, (16, 5, 1, S) halo rows and
-// (8, 16, 1, S) halo columns; the immersed flags with (16, 16, 1) and
-// (16, 5, 1).
+// (8, 16, 1, S) halo columns.
 struct XyMaps {
-  CUtensorMap in, ns, ew, fin, fns;
+  CUtensorMap in, ns, ew;
 };
 
 // Edge reconstruction of `total` stencils with learned weights by the NT
@@ -497,17 +487,18 @@ __device__ __forceinline__ void recon_outer_pair(int f, int line, Load load, Sto
 // x/y fluxes and their divergence for one (x,y) tile of one level.
 // LEARNED (FP32, weno_all only): edges from the network's weights, with the
 // plain limiter as the fallback.
-// use_tma (16x16 FP32 tiles of an undecomposed plain domain): a tile that
-// lies whole in the domain takes its cross from TMA copies (maps: tensor maps
-// of sin and of the flags), the halo rows and columns wrapping periodically
-// box by box; tiles at a precursor edge, partial tiles and halo boxes that
-// would straddle the domain's edge are loaded by the threads.
-template <class R, int NTR, int TX, int TY, bool IMM, bool LEARNED = false, bool DECOMP = false>
-__global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (sizeof(R) == 4 ? PU_XY_MIN_BLOCKS : 1)) k_xy(const Grid<R> G, const R *__restrict__ sin, R *__restrict__ txy, const __grid_constant__ XyMaps maps, int use_tma) {
+// TMA (16x16 FP32 tiles of an undecomposed plain domain): a tile that lies
+// whole in the domain takes its cross from TMA copies (maps: tensor maps of
+// sin), the halo rows and columns wrapping periodically box by box; tiles at
+// a precursor edge, partial tiles and halo boxes that would straddle the
+// domain's edge are loaded by the threads.
+template <class R, int NTR, int TX, int TY, bool IMM, bool LEARNED = false, bool DECOMP = false, bool TMA = false>
+__global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (sizeof(R) == 4 ? PU_XY_MIN_BLOCKS : 1)) k_xy(const Grid<R> G, const R *__restrict__ sin, R *__restrict__ txy, const __grid_constant__ XyMaps maps) {
   using Sh = XYShape<R, NTR, TX, TY, IMM, LEARNED>;
   constexpr int F = Sh::F, S = Sh::S, NT = Sh::NT, HX = Sh::HX, HY = Sh::HY, EN = Sh::EN, FN = Sh::FN;
-  extern __shared__ __align__(128) unsigned char smem_xy[];
-  unsigned char *smem_raw = smem_xy + ((128u - (tma::saddr(smem_xy) & 127u)) & 127u);
+  static_assert(!TMA || (Sh::TMA_FITS && !DECOMP && !IMM), "TMA staging: 16x16 FP32 tiles, plain domains");
+  extern __shared__ __align__(16) unsigned char smem_xy[];
+  unsigned char *smem_raw = TMA ? smem_xy + ((128u - (tma::saddr(smem_xy) & 127u)) & 127u) : smem_xy;
   R *H = reinterpret_cast<R *>(smem_raw);
   R *EL = H + F * HY * HX;
   R *ER = EL + F * EN;
@@ -531,39 +522,26 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
   // 0. TMA staging of the tile's cross (block-uniform decision).  Box origins:
   // the interior at (i0, j0); the 5 rows above at j0-5 (ny-5 for the first
   // tile row), below at j0+16 (0 for the last); the 8 columns left at i0-8
-  // (nx-8), right at i0+16 (0); the flags' 16-wide side boxes at i0-16 (nx-16)
-  // and i0+16 (0).  Every x origin is a multiple of 8 (16 for the flags).
+  // (nx-8), right at i0+16 (0).  Every x origin is a multiple of 8.
   bool staged = false;
-  if constexpr (Sh::TMA_FITS && !DECOMP) {
-    if (use_tma && !sim2d && i0 + TX <= nx && j0 + TY <= ny) {
+  if constexpr (TMA) {
+    if (!sim2d && i0 + TX <= nx && j0 + TY <= ny) {
       const bool px = G.bc_x != BC_PRECURSOR, py = G.bc_y != BC_PRECURSOR;
       const int xw = i0 > 0 ? i0 - 8 : (px ? nx - 8 : -1);
       const int xe = i0 + TX < nx ? (i0 + TX + 8 <= nx ? i0 + TX : -1) : (px ? 0 : -1);
       const int yn = j0 > 0 ? j0 - 5 : (py ? ny - 5 : -1);
       const int ys = j0 + TY < ny ? (j0 + TY + 5 <= ny ? j0 + TY : -1) : (py ? 0 : -1);
-      const int fw = i0 > 0 ? i0 - 16 : nx - 16;
-      const int fe = i0 + TX < nx ? (i0 + TX + 16 <= nx ? i0 + TX : -1) : 0;
-      const int fn = j0 > 0 ? j0 - 5 : ny - 5, fs = j0 + TY < ny ? (j0 + TY + 5 <= ny ? j0 + TY : -1) : 0;
-      constexpr bool TF = IMM && PU_XY_TMA_FLAGS;
-      staged = xw >= 0 && xe >= 0 && yn >= 0 && ys >= 0 && (!TF || (fw >= 0 && fe >= 0 && fn >= 0 && fs >= 0));
+      staged = xw >= 0 && xe >= 0 && yn >= 0 && ys >= 0;
       if (staged) {
         uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + Sh::bar_off);
         if (tid == 0) {
           tma::mbar_init(bar);
-          tma::mbar_expect(bar, uint32_t(sizeof(R) * S * (256 + 80 + 80 + 128 + 128) +
-                                         (TF ? 256 + 80 + 80 + 256 + 256 : 0)));
+          tma::mbar_expect(bar, uint32_t(sizeof(R) * S * (256 + 80 + 80 + 128 + 128)));
           tma::load_4d(smem_raw + Sh::st_in, &maps.in, i0, j0, k, 0, bar);
           tma::load_4d(smem_raw + Sh::st_top, &maps.ns, i0, yn, k, 0, bar);
           tma::load_4d(smem_raw + Sh::st_bot, &maps.ns, i0, ys, k, 0, bar);
           tma::load_4d(smem_raw + Sh::st_west, &maps.ew, xw, j0, k, 0, bar);
           tma::load_4d(smem_raw + Sh::st_east, &maps.ew, xe, j0, k, 0, bar);
-          if (TF) {
-            tma::load_3d(smem_raw + Sh::fl_in, &maps.fin, i0, j0, k, bar);
-            tma::load_3d(smem_raw + Sh::fl_top, &maps.fns, i0, fn, k, bar);
-            tma::load_3d(smem_raw + Sh::fl_bot, &maps.fns, i0, fs, k, bar);
-            tma::load_3d(smem_raw + Sh::fl_west, &maps.fin, fw, j0, k, bar);
-            tma::load_3d(smem_raw + Sh::fl_east, &maps.fin, fe, j0, k, bar);
-          }
         }
         __syncthreads();
         if (!__syncthreads_and(tma::mbar_wait(bar, 0))) {
@@ -591,37 +569,30 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
     }
     const int gi = i0 - 5 + c, gj = j0 - 5 + r;
     R w[F];
-    if (Sh::TMA_FITS && !DECOMP && staged) {
-      // The cell's place in the staged boxes ([S][rows][cols]) and its flag.
+    if (TMA && staged) {
+      // The cell's place in the staged boxes ([S][rows][cols]).
       const R *src;
       int fstride;
-      const uint8_t *fb;
       if (r < 5) {
         src = reinterpret_cast<const R *>(smem_raw + Sh::st_top) + r * 16 + (c - 5);
         fstride = 80;
-        fb = smem_raw + Sh::fl_top + r * 16 + (c - 5);
       } else if (r >= 5 + TY) {
         src = reinterpret_cast<const R *>(smem_raw + Sh::st_bot) + (r - 5 - TY) * 16 + (c - 5);
         fstride = 80;
-        fb = smem_raw + Sh::fl_bot + (r - 5 - TY) * 16 + (c - 5);
       } else if (c < 5) {
         src = reinterpret_cast<const R *>(smem_raw + Sh::st_west) + (r - 5) * 8 + (c + 3);
         fstride = 128;
-        fb = smem_raw + Sh::fl_west + (r - 5) * 16 + (c + 11);
       } else if (c >= 5 + TX) {
         src = reinterpret_cast<const R *>(smem_raw + Sh::st_east) + (r - 5) * 8 + (c - 5 - TX);
         fstride = 128;
-        fb = smem_raw + Sh::fl_east + (r - 5) * 16 + (c - 5 - TX);
       } else {
         src = reinterpret_cast<const R *>(smem_raw + Sh::st_in) + (r - 5) * 16 + (c - 5);
         fstride = 256;
-        fb = smem_raw + Sh::fl_in + (r - 5) * 16 + (c - 5);
       }
       R q[S];
 #pragma unroll
       for (int s2 = 0; s2 < S; s2++) q[s2] = src[s2 * fstride];
       prims_of<R, NTR>(G, q, k, w);
-      if (IMM) M[r * HX + c] = PU_XY_TMA_FLAGS ? *fb : __ldg(G.flags + plane + size_t(wrapi(gj, ny)) * nx + wrapi(gi, nx));
     } else if constexpr (DECOMP) {
       const R *src;
       size_t fs, q;
@@ -1205,10 +1176,10 @@ struct ZTShape {
   // bit 1 an immersed cell within 10).
   static constexpr size_t base_bytes = sizeof(float) * (size_t(F) * HZ * TX + 2 * size_t(F) * EN) +
                                        (IMM ? (size_t(HZ) * TX + 15) / 16 * 16 : 0);
-  // The kernel rounds the start of its dynamic shared memory up to 128 bytes
-  // (the alignment of the TMA destinations): PAD bytes more than the layout.
+  static constexpr size_t bytes = base_bytes;
+  // The TMA instantiation rounds the start of its dynamic shared memory up to
+  // 128 bytes (the alignment of the TMA destinations): PAD bytes more.
   static constexpr size_t PAD = 128;
-  static constexpr size_t bytes = base_bytes + PAD;
   // TMA staging (byte offsets from the start of shared memory).
   static constexpr size_t el_off = sizeof(float) * size_t(F) * HZ * TX;
   static constexpr size_t raw_off = al(el_off);
@@ -1243,23 +1214,22 @@ struct ZtMaps {
 // with weno_all (IMM: domains with immersed cells, whose level flags go to
 // shared memory with the fields); every other form keeps the march.
 //
-// use_tma: the raw tile and the finalisation's cell inputs come from TMA
-// copies (maps: tensor maps of sin, sn and txy); rows the halo box does not
-// hold (the wrapped levels of a periodic z) and, when the cell buffers do
-// not fit, the cell inputs are read per thread as without it.  Columns
-// beyond the domain read zero there instead of the last column; their
-// results are discarded either way.
-template <int NTR, int TX, int TZ, bool IMM>
+// TMA: the raw tile and the finalisation's cell inputs come from TMA copies
+// (maps: tensor maps of sin, sn and txy); rows the halo box does not hold
+// (the wrapped levels of a periodic z) and, when the cell buffers do not
+// fit, the cell inputs are read per thread as without it.  Columns beyond
+// the domain read zero there instead of the last column; their results are
+// discarded either way.
+template <int NTR, int TX, int TZ, bool IMM, bool TMA = false>
 __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<float> G, const float *__restrict__ sin,
                                                                const float *sn, float *sout,
                                                                const float *__restrict__ txy, float a_n, float a_dt,
-                                                               int n_enforce, const __grid_constant__ ZtMaps maps,
-                                                               int use_tma) {
+                                                               int n_enforce, const __grid_constant__ ZtMaps maps) {
   using R = float;
   using Sh = ZTShape<NTR, TX, TZ, IMM>;
   constexpr int F = Sh::F, S = Sh::S, NT = Sh::NT, HZ = Sh::HZ;
-  extern __shared__ __align__(128) unsigned char smem_zt[];
-  unsigned char *smem_raw = smem_zt + ((128u - (tma::saddr(smem_zt) & 127u)) & 127u);
+  extern __shared__ __align__(16) unsigned char smem_zt[];
+  unsigned char *smem_raw = TMA ? smem_zt + ((128u - (tma::saddr(smem_zt) & 127u)) & 127u) : smem_zt;
   R *H = reinterpret_cast<R *>(smem_raw);   // [F][HZ][TX]
   R *EL = H + F * HZ * TX;                   // [F][TZ+2][TX]
   R *ER = EL + F * Sh::EN;
@@ -1274,12 +1244,12 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
   const int nx = G.nx, nz = G.nz;
   const bool wall = G.bc_z == BC_WALL;
   const size_t NP = G.NP, row = size_t(j) * nx;
-  const bool pref = Sh::PREFETCH && use_tma;
+  constexpr bool pref = Sh::PREFETCH && TMA;
   // Level whose state feeds level p (wall halos replicate the boundary cell,
   // periodic halos wrap; dynamics_rk.h:780-797).
   auto src_level = [&](int p) { return (p >= 0 && p < nz) ? p : (wall ? clampi(p, nz) : wrapi(p, nz)); };
 
-  if (use_tma) {
+  if constexpr (TMA) {
     if (tid == 0) {
       tma::mbar_init(bar);
       tma::mbar_init(bar + 1);
@@ -1311,7 +1281,7 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
     const size_t col = row + min(i0 + c, nx - 1);
     R q[S], w[F];
     const int rr = lv - (k0 - 5);   // the halo box's row of level lv
-    if (use_tma && rr >= 0 && rr < HZ) {
+    if (TMA && rr >= 0 && rr < HZ) {
 #pragma unroll
       for (int s2 = 0; s2 < S; s2++) q[s2] = RAW[(s2 * HZ + rr) * TX + c];
     } else {

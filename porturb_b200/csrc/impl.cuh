@@ -556,10 +556,10 @@ struct Impl : ImplBase {
   // (halo and cell boxes of s[b], the cell boxes of s[0] and txy).
   ZtMaps zt_maps[3];
   bool zt_tma = false;
-  // TMA staging of the 16x16 x/y kernel: per stage-input buffer s[b] the
-  // interior, halo-row and halo-column boxes, and the flags' boxes.
+  // TMA staging of the 16x16 x/y kernel (domains without immersed cells):
+  // per stage-input buffer s[b] the interior, halo-row and halo-column boxes.
   XyMaps xy_maps[3];
-  bool xy_tma = false, xy_tma_flags = false;
+  bool xy_tma = false;
 
   // Tensor maps of the state buffers for the tiled z kernel (host-side
   // encoding only, no allocation).  Off when the config asks for thread
@@ -584,12 +584,6 @@ struct Impl : ImplBase {
              tma::encode_state(&xy_maps[b].ew, s[b], nx, ny, nz, S, 8, 16, 1, S);
       }
       xy_tma = ok;
-      xy_tma_flags = ok && flags && tma::encode_bytes3(&xy_maps[0].fin, flags, nx, ny, nz, 16, 16, 1) &&
-                     tma::encode_bytes3(&xy_maps[0].fns, flags, nx, ny, nz, 16, 5, 1);
-      for (int b = 1; b < 3 && xy_tma_flags; b++) {
-        xy_maps[b].fin = xy_maps[0].fin;
-        xy_maps[b].fns = xy_maps[0].fns;
-      }
     }
   }
 
@@ -685,9 +679,17 @@ struct Impl : ImplBase {
                                int(ZShape<R, NTR, ZTX, ZTY>::bytes)));
     if constexpr (std::is_same<R, float>::value) {
       PU_CK(cudaFuncSetAttribute(k_zt<NTR, ZT_X, ZT_Z, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(ZTShape<NTR, ZT_X, ZT_Z, false>::tma_bytes)));
+                                 int(ZTShape<NTR, ZT_X, ZT_Z, false>::bytes)));
       PU_CK(cudaFuncSetAttribute(k_zt<NTR, ZT_X, ZT_Z, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(ZTShape<NTR, ZT_X, ZT_Z, true>::bytes)));
+      PU_CK(cudaFuncSetAttribute(k_zt<NTR, ZT_X, ZT_Z, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(ZTShape<NTR, ZT_X, ZT_Z, false>::tma_bytes)));
+      PU_CK(cudaFuncSetAttribute(k_zt<NTR, ZT_X, ZT_Z, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(ZTShape<NTR, ZT_X, ZT_Z, true>::tma_bytes)));
+      if constexpr (XYShape<R, NTR, XTX_BIG, XTY_BIG, false>::TMA_FITS)
+        PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, XTX_BIG, XTY_BIG, false, false, false, true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(XYShape<R, NTR, XTX_BIG, XTY_BIG, false>::tma_bytes)));
       PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, LTX, LTY, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(XYShape<R, NTR, LTX, LTY, false, true>::bytes)));
       PU_CK(cudaFuncSetAttribute(k_xy<R, NTR, LTX, LTY, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -899,7 +901,6 @@ struct Impl : ImplBase {
     k_imm_finish<R><<<blocks(N, 256), 256, 0, st>>>(dprop, a, dzero, cfg.immersed_power, N, flags,
                                                     static_cast<R *>(imm_mult));
     PU_LAUNCHED();
-    make_maps();   // the flags' maps, now that the flags exist
     // has_imm: any flag set (a cell with prop > 0 has distance 0 in `a`).
     std::vector<uint8_t> hf(N);
     PU_CK(cudaMemcpyAsync(hf.data(), flags, N, cudaMemcpyDeviceToHost, st));
@@ -969,18 +970,27 @@ struct Impl : ImplBase {
     if (small_tile) {
       using Sh = XYShape<R, NTR, XTX_SM, XTY_SM, IMM, L>;
       dim3 g(blocks(cfg.nx, XTX_SM), blocks(cfg.ny, XTY_SM), cfg.nz);
-      k_xy<R, NTR, XTX_SM, XTY_SM, IMM, L, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b], 0);
+      k_xy<R, NTR, XTX_SM, XTY_SM, IMM, L, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b]);
     } else if (L) {
       using Sh = XYShape<R, NTR, LTX, LTY, IMM, L>;
       dim3 g(blocks(cfg.nx, LTX), blocks(cfg.ny, LTY), cfg.nz);
-      k_xy<R, NTR, LTX, LTY, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b], 0);
+      k_xy<R, NTR, LTX, LTY, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b]);
     } else {
       using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM, false>;
       dim3 g(blocks(cfg.nx, XTX_BIG), blocks(cfg.ny, XTY_BIG), cfg.nz);
-      const bool use_tma = !DEC && xy_tma && (!IMM || !PU_XY_TMA_FLAGS || xy_tma_flags) &&
-                           static_cast<const void *>(sin) == s[b];
-      k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b],
-                                                                                     use_tma ? 1 : 0);
+      // Domains without immersed cells stage their tiles through TMA (the
+      // immersed kernel is faster with its threads' loads: 44.2 against
+      // 44.9 ms per launch on the 1024x1024x256 urban canopy).
+      bool staged = false;
+      if constexpr (!IMM && !DEC && Sh::TMA_FITS) {
+        if (xy_tma && static_cast<const void *>(sin) == s[b]) {
+          k_xy<R, NTR, XTX_BIG, XTY_BIG, false, false, false, true><<<g, Sh::NT, Sh::tma_bytes, st>>>(G, sin, t,
+                                                                                                    xy_maps[b]);
+          staged = true;
+        }
+      }
+      if (!staged)
+        k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b]);
     }
     PU_LAUNCHED();
     prof_end(0, e0);
@@ -993,9 +1003,12 @@ struct Impl : ImplBase {
         dim3 gt(blocks(cfg.nx, ZT_X), cfg.ny, blocks(cfg.nz, ZT_Z));
         // The maps of this stage input (s[b]); the cell maps of sn and txy
         // are the same for every b.
-        const bool use_tma = zt_tma && static_cast<const void *>(sin) == s[b];
-        k_zt<NTR, ZT_X, ZT_Z, IMM><<<gt, ZT_X * ZT_Z, use_tma ? Zs::tma_bytes : Zs::bytes, st>>>(
-            G, sin, sn, sout, t, a_n, a_dt, n_enforce, zt_maps[b], use_tma ? 1 : 0);
+        if (zt_tma && static_cast<const void *>(sin) == s[b])
+          k_zt<NTR, ZT_X, ZT_Z, IMM, true><<<gt, ZT_X * ZT_Z, Zs::tma_bytes, st>>>(G, sin, sn, sout, t, a_n, a_dt,
+                                                                                 n_enforce, zt_maps[b]);
+        else
+          k_zt<NTR, ZT_X, ZT_Z, IMM><<<gt, ZT_X * ZT_Z, Zs::bytes, st>>>(G, sin, sn, sout, t, a_n, a_dt, n_enforce,
+                                                                          zt_maps[b]);
         PU_LAUNCHED();
         prof_end(1, e1);
         return PU_OK;

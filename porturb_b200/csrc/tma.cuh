@@ -61,23 +61,6 @@ inline bool encode_state(CUtensorMap *m, const void *base, int nx, int ny, int n
   return r == CUDA_SUCCESS;
 }
 
-// A map of a byte array (nz, ny, nx), x fastest -- the immersed flags -- with
-// box (bx, by, bz).  False when it breaks a TMA rule (nx % 16 != 0, ...).
-inline bool encode_bytes3(CUtensorMap *m, const void *base, int nx, int ny, int nz, uint32_t bx, uint32_t by,
-                          uint32_t bz) {
-  auto enc = encoder();
-  if (!enc || !base || nx % 16 != 0 || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
-  if (bx % 16 != 0 || bx > 256 || by > 256 || bz > 256 || !bx || !by || !bz) return false;
-  const cuuint64_t dims[3] = {cuuint64_t(nx), cuuint64_t(ny), cuuint64_t(nz)};
-  const cuuint64_t strides[2] = {cuuint64_t(nx), cuuint64_t(nx) * ny};
-  const cuuint32_t box[3] = {bx, by, bz};
-  const cuuint32_t estr[3] = {1, 1, 1};
-  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void *>(base), dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  return r == CUDA_SUCCESS;
-}
-
 // ---- device --------------------------------------------------------------
 
 __device__ __forceinline__ uint32_t saddr(const void *p) {
@@ -103,15 +86,6 @@ __device__ __forceinline__ void load_4d(void *dst, const CUtensorMap *map, int x
       "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
       "[%6];" ::"r"(saddr(dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(f), "r"(saddr(bar))
-      : "memory");
-}
-
-// A box of the 3-D `map` at (x, y, z) (x a multiple of 16 bytes).
-__device__ __forceinline__ void load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
-          "r"(saddr(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(saddr(bar))
       : "memory");
 }
 

@@ -1,12 +1,12 @@
 """TMA staging of the stage kernels' tiles gives the same bits as the
 threads' own loads (pu_config.thread_loads = 1).
 
-The x/y kernel stages the cross of every 16x16 tile that lies whole in the
-domain in five boxes (interior, 5 rows above and below, 5 columns left and
-right in 8-wide boxes; the immersed flags in 16-wide boxes when nx % 16 ==
-0), each wrapping periodically on its own; tiles at a precursor edge,
-partial tiles and halo boxes that would straddle the domain's edge keep the
-thread loads.
+On domains without immersed cells the x/y kernel stages the cross of every
+16x16 tile that lies whole in the domain in five boxes (interior, 5 rows
+above and below, 5 columns left and right in 8-wide boxes), each wrapping
+periodically on its own; tiles at a precursor edge, partial tiles and halo
+boxes that would straddle the domain's edge keep the thread loads, as does
+the immersed x/y kernel.
 
 The tiled z kernel copies its raw tile (levels k0-5 .. k0+36) and, where
 the buffers fit beside four blocks per SM (up to three tracers), the cell
@@ -16,8 +16,8 @@ periodic z from the threads, columns beyond the domain read zero (their
 results are discarded).  Cases: walls and periodic z, immersed cells, one to
 four tracers (with and without the prefetched cell inputs), partial tiles in
 x (nx = 20, 52), y (ny = 37) and z (nz = 40), precursor x and y (only the
-inner tiles staged), flags that cannot be staged (nx = 52), and a grid whose
-nx breaks the TMA stride rule (nx % 4 != 0: thread loads everywhere).
+inner tiles staged), and a grid whose nx breaks the TMA stride rule
+(nx % 4 != 0: thread loads everywhere).
 """
 import numpy as np
 import pytest
@@ -31,11 +31,11 @@ CASES = {
     "abl_64x48x40": lambda: cases.abl_neutral(nx=64, ny=48, nz=40),
     "abl_80x37x40_partial_y": lambda: cases.abl_neutral(nx=80, ny=37, nz=40),
     "urban_64x48x48": lambda: cases.urban_canopy(nx=64, ny=48, nz=48, dx=2.0),
-    "urban_52x40x48_flags_not_staged": lambda: cases.urban_canopy(nx=52, ny=40, nz=48, dx=2.0),
+    "urban_52x40x48_partial_x": lambda: cases.urban_canopy(nx=52, ny=40, nz=48, dx=2.0),
     "mixed_periodic_z": lambda: cases.small_mixed(nx=20, ny=12, nz=40, bc_z="periodic"),
     "mixed_immersed_3tr": lambda: cases.small_mixed(nx=48, ny=32, nz=36, ntr=3),
     "mixed_4tr_precursor_xy": lambda: cases.small_mixed(nx=48, ny=48, nz=24, ntr=4, bc_x="precursor",
-                                                        bc_y="precursor"),
+                                                        bc_y="precursor", immersed=False),
     "odd_nx_no_tma": lambda: cases.small_mixed(nx=18, ny=10, nz=20),
 }
 

@@ -83,6 +83,10 @@ typedef struct pu_config {
   int thread_loads;                        /* 0: the stage kernels stage their tiles through TMA
                                               where the grid allows it (nx % 4 == 0); 1: every
                                               tile is loaded by the threads (the same results) */
+  int imm_all_levels;                      /* 0: on an immersed domain the stage kernels take the
+                                              immersed code only on the levels (z chunks) that an
+                                              immersed flag reaches; 1: on every level (the same
+                                              results) */
 } pu_config;
 
 /* The coupler-side state: density_dry, uvel, vvel, wvel, temp and the tracer

@@ -111,6 +111,10 @@ struct Grid {
   const R *hxl, *hxr, *hyl, *hyr;
   const uint8_t *fxl, *fxr, *fyl, *fyr;
   int gx0, gx1, gy0, gy1;
+  // First level of a k_xy launch (blockIdx.z counts from it) and first z
+  // chunk of a k_zt launch: a stage can run the immersed kernels on the
+  // levels that need them and the plain ones above.
+  int k_first, c_first;
   // Learned WENO weights (kernels instantiated with LEARNED only).
   const uint32_t *ml_frags;     // per-lane operand fragments of the network
   unsigned long long *ml_counts;  // [0] stencils given learned weights, [1] limiter fallbacks
@@ -513,7 +517,7 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
   uint16_t *queue = reinterpret_cast<uint16_t *>(FL);
 
   const int tid = threadIdx.x;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k = blockIdx.z;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k = G.k_first + int(blockIdx.z);
   const int nx = G.nx, ny = G.ny;
   const size_t plane = size_t(k) * G.NP;
   const bool sim2d = G.sim2d != 0;
@@ -1240,7 +1244,7 @@ __global__ void __launch_bounds__(TX *TZ, PU_ZT_MIN_BLOCKS) k_zt(const Grid<floa
   R *TXY = SN + S * TZ * TX;
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + Sh::tma_bar_off);
   const int tid = threadIdx.x;
-  const int i0 = blockIdx.x * TX, j = blockIdx.y, k0 = blockIdx.z * TZ;
+  const int i0 = blockIdx.x * TX, j = blockIdx.y, k0 = (G.c_first + int(blockIdx.z)) * TZ;
   const int nx = G.nx, nz = G.nz;
   const bool wall = G.bc_z == BC_WALL;
   const size_t NP = G.NP, row = size_t(j) * nx;

@@ -94,6 +94,7 @@ struct ImplBase {
   int ntr = 0, S = 0, F = 0, nzh = 0;
   size_t N = 0, NP = 0;
   bool inited = false, has_imm = false;
+  int imm_kc = 0;   // 1 + the highest level holding an immersed flag (immersed, or one within 10 cells)
   bool owns = true;                           // false: buffers point into caller-provided scratch
   long long launches = 0;
   // Device buffers.
@@ -772,6 +773,8 @@ struct Impl : ImplBase {
     G.gy0 = !dc.on || dc.d.py == 0;
     G.gy1 = !dc.on || dc.d.py == dc.d.nproc_y - 1;
     G.err = err;
+    G.k_first = 0;
+    G.c_first = 0;
     G.ml_frags = ml_frags;
     G.ml_counts = ml_counts;
     G.ml_jump = ml_jump;
@@ -907,6 +910,13 @@ struct Impl : ImplBase {
     PU_CK(cudaStreamSynchronize(st));
     has_imm = false;
     for (size_t q = 0; q < N && !has_imm; q++) has_imm = (hf[q] & FLAG_IMM) != 0;
+    imm_kc = 0;
+    for (int k = cfg.nz - 1; k >= 0 && !imm_kc; k--)
+      for (size_t q = size_t(k) * NP; q < size_t(k + 1) * NP; q++)
+        if (hf[q]) {
+          imm_kc = k + 1;
+          break;
+        }
     return PU_OK;
   }
 
@@ -945,6 +955,12 @@ struct Impl : ImplBase {
     return check_err();
   }
 
+  // Levels from the bottom that take the immersed stage kernels: those an
+  // immersed flag reaches (the levels above hold no immersed cell and none
+  // within 10 cells, where the immersed code gives the plain code's results);
+  // every level for a decomposed tile or when the config asks for it.
+  int imm_levels() const { return (dc.on || cfg.imm_all_levels || !has_imm) ? cfg.nz : imm_kc; }
+
   // The tiled z kernel (k_zt) takes the plain FP32 limiter with weno_all,
   // unless a z chunk was asked for (the march, which gives the same bits).  Its grid has one y row per block
   // row, so ny is held to the grid's y limit.
@@ -976,21 +992,32 @@ struct Impl : ImplBase {
       dim3 g(blocks(cfg.nx, LTX), blocks(cfg.ny, LTY), cfg.nz);
       k_xy<R, NTR, LTX, LTY, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b]);
     } else {
+      // Levels [0, kl) take the immersed kernel, [kl, nz) the plain one --
+      // through TMA where the tiles allow it.
       using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM, false>;
-      dim3 g(blocks(cfg.nx, XTX_BIG), blocks(cfg.ny, XTY_BIG), cfg.nz);
-      // Domains without immersed cells stage their tiles through TMA (the
-      // immersed kernel is faster with its threads' loads: 44.2 against
-      // 44.9 ms per launch on the 1024x1024x256 urban canopy).
-      bool staged = false;
-      if constexpr (!IMM && !DEC && Sh::TMA_FITS) {
-        if (xy_tma && static_cast<const void *>(sin) == s[b]) {
-          k_xy<R, NTR, XTX_BIG, XTY_BIG, false, false, false, true><<<g, Sh::NT, Sh::tma_bytes, st>>>(G, sin, t,
-                                                                                                    xy_maps[b]);
-          staged = true;
-        }
+      using Sp = XYShape<R, NTR, XTX_BIG, XTY_BIG, false, false>;
+      const int kl = IMM ? imm_levels() : 0;
+      const unsigned bx = blocks(cfg.nx, XTX_BIG), by = blocks(cfg.ny, XTY_BIG);
+      if (kl > 0) {
+        k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false, DEC><<<dim3(bx, by, kl), Sh::NT, Sh::bytes, st>>>(G, sin, t,
+                                                                                                   xy_maps[b]);
+        if (kl < cfg.nz) PU_LAUNCHED();
       }
-      if (!staged)
-        k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b]);
+      if (kl < cfg.nz) {
+        Grid<R> Gp = G;
+        Gp.k_first = kl;
+        const dim3 g(bx, by, cfg.nz - kl);
+        bool staged = false;
+        if constexpr (!DEC && Sp::TMA_FITS) {
+          if (xy_tma && static_cast<const void *>(sin) == s[b]) {
+            k_xy<R, NTR, XTX_BIG, XTY_BIG, false, false, false, true><<<g, Sp::NT, Sp::tma_bytes, st>>>(Gp, sin, t,
+                                                                                                      xy_maps[b]);
+            staged = true;
+          }
+        }
+        if (!staged)
+          k_xy<R, NTR, XTX_BIG, XTY_BIG, false, false, DEC><<<g, Sp::NT, Sp::bytes, st>>>(Gp, sin, t, xy_maps[b]);
+      }
     }
     PU_LAUNCHED();
     prof_end(0, e0);
@@ -999,16 +1026,38 @@ struct Impl : ImplBase {
     cudaEvent_t e1 = prof_begin();
     if constexpr (std::is_same<R, float>::value) {
       if (z_tiled(L)) {
+        // z chunks [0, ci) take the immersed kernel: chunk c reads levels
+        // 32c-5 .. 32c+36, so it is plain once 32c-5 reaches the first level
+        // no flag holds.  A periodic z wraps flagged levels into the top
+        // chunk: every chunk stays immersed there.  The maps of this stage
+        // input (s[b]); the cell maps of sn and txy are the same for every b.
         using Zs = ZTShape<NTR, ZT_X, ZT_Z, IMM>;
-        dim3 gt(blocks(cfg.nx, ZT_X), cfg.ny, blocks(cfg.nz, ZT_Z));
-        // The maps of this stage input (s[b]); the cell maps of sn and txy
-        // are the same for every b.
-        if (zt_tma && static_cast<const void *>(sin) == s[b])
-          k_zt<NTR, ZT_X, ZT_Z, IMM, true><<<gt, ZT_X * ZT_Z, Zs::tma_bytes, st>>>(G, sin, sn, sout, t, a_n, a_dt,
-                                                                                 n_enforce, zt_maps[b]);
-        else
-          k_zt<NTR, ZT_X, ZT_Z, IMM><<<gt, ZT_X * ZT_Z, Zs::bytes, st>>>(G, sin, sn, sout, t, a_n, a_dt, n_enforce,
-                                                                          zt_maps[b]);
+        using Zp = ZTShape<NTR, ZT_X, ZT_Z, false>;
+        const int nch = int(blocks(cfg.nz, ZT_Z));
+        const int ci = !IMM ? 0 : (cfg.bc_z == PU_BC_WALL ? std::min(nch, (imm_levels() + 5 + ZT_Z - 1) / ZT_Z) : nch);
+        const bool tma = zt_tma && static_cast<const void *>(sin) == s[b];
+        const unsigned bx = blocks(cfg.nx, ZT_X), by = unsigned(cfg.ny);
+        if (ci > 0) {
+          const dim3 gt(bx, by, ci);
+          if (tma)
+            k_zt<NTR, ZT_X, ZT_Z, IMM, true><<<gt, ZT_X * ZT_Z, Zs::tma_bytes, st>>>(G, sin, sn, sout, t, a_n, a_dt,
+                                                                                   n_enforce, zt_maps[b]);
+          else
+            k_zt<NTR, ZT_X, ZT_Z, IMM><<<gt, ZT_X * ZT_Z, Zs::bytes, st>>>(G, sin, sn, sout, t, a_n, a_dt,
+                                                                            n_enforce, zt_maps[b]);
+          if (ci < nch) PU_LAUNCHED();
+        }
+        if (ci < nch) {
+          Grid<R> Gp = G;
+          Gp.c_first = ci;
+          const dim3 gt(bx, by, nch - ci);
+          if (tma)
+            k_zt<NTR, ZT_X, ZT_Z, false, true><<<gt, ZT_X * ZT_Z, Zp::tma_bytes, st>>>(Gp, sin, sn, sout, t, a_n,
+                                                                                      a_dt, n_enforce, zt_maps[b]);
+          else
+            k_zt<NTR, ZT_X, ZT_Z, false><<<gt, ZT_X * ZT_Z, Zp::bytes, st>>>(Gp, sin, sn, sout, t, a_n, a_dt,
+                                                                              n_enforce, zt_maps[b]);
+        }
         PU_LAUNCHED();
         prof_end(1, e1);
         return PU_OK;

@@ -129,6 +129,7 @@ int check_config(const pu_config *c) {
   if (!(c->gamma_d > 1 && c->C0 > 0 && c->R_d > 0 && c->cfl > 0)) return fail(PU_ERR_INVALID, "bad thermodynamic options");
   if (c->z_chunk < 0) return fail(PU_ERR_INVALID, "z_chunk must be >= 0");
   if (c->thread_loads != 0 && c->thread_loads != 1) return fail(PU_ERR_INVALID, "thread_loads must be 0 or 1");
+  if (c->imm_all_levels != 0 && c->imm_all_levels != 1) return fail(PU_ERR_INVALID, "imm_all_levels must be 0 or 1");
   return PU_OK;
 }
 }  // namespace pu

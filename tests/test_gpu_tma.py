@@ -61,3 +61,46 @@ def test_tma_staging_equals_thread_loads(name, gpu_lib):
     assert np.array_equal(a_tr, b_tr)
     for x, y in zip(a_cpl, b_cpl):
         assert np.array_equal(x, y)
+
+
+SPLIT_CASES = {
+    # buildings up to 30 levels, flags reach ~40 of 96 levels: both kernels split
+    "urban_64x48x96": lambda: cases.urban_canopy(nx=64, ny=48, nz=96, dx=2.0),
+    # cuboid to level 16, flags to ~26 of 48; precursor x keeps the edge tiles on thread loads
+    "mixed_48x32x48_precursor": lambda: cases.small_mixed(nx=48, ny=32, nz=48, bc_x="precursor"),
+    # periodic z: the x/y kernel splits, the z kernel stays immersed in every chunk
+    "mixed_32x32x48_periodic_z": lambda: cases.small_mixed(nx=32, ny=32, nz=48, bc_z="periodic"),
+    # flags reach the top: no split
+    "mixed_32x32x20": lambda: cases.small_mixed(nx=32, ny=32, nz=20),
+}
+
+
+@pytest.mark.parametrize("thread_loads", [False, True])
+@pytest.mark.parametrize("name", sorted(SPLIT_CASES))
+def test_immersed_kernels_only_where_flags_reach(name, thread_loads, gpu_lib):
+    """On an immersed domain the stage kernels take the immersed code on the
+    levels (z chunks) an immersed flag reaches and the plain code above; the
+    same bits as the immersed code on every level (imm_all_levels = 1)."""
+    case = SPLIT_CASES[name]()
+    runs = []
+    for all_levels in (False, True):
+        st, tr, g = gpu_run(case, "f32", 0, 1.0, thread_loads=thread_loads, imm_all_levels=all_levels)
+        dt = g.compute_time_step()
+        n0 = g.kernel_launches()
+        g.advance(dt, 3)
+        g.synchronize()
+        launches = g.kernel_launches() - n0
+        st, tr = g.get_conserved()
+        rd, u, v, w, T, trc = [np.ascontiguousarray(np.array(a)) for a in case.coupler_arrays(perturbed=True)]
+        trs = [np.ascontiguousarray(x) for x in trc]
+        assert g.time_step(rd, u, v, w, T, trs, 2.5 * dt) == 3
+        g.close()
+        runs.append((st, tr, [rd, u, v, w, T] + trs, launches))
+    (a_st, a_tr, a_cpl, a_n), (b_st, b_tr, b_cpl, b_n) = runs
+    print(name, "launches in 3 steps: split", a_n, "all levels", b_n)
+    if name != "mixed_32x32x20":
+        assert a_n > b_n          # the split ran extra launches
+    assert np.array_equal(a_st, b_st), np.abs(a_st - b_st).max()
+    assert np.array_equal(a_tr, b_tr)
+    for x, y in zip(a_cpl, b_cpl):
+        assert np.array_equal(x, y)

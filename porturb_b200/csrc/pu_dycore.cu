@@ -95,17 +95,28 @@ int fail(int code, const std::string &msg) {
 
 // Every entry point runs with the handle's device current and restores the
 // caller's device afterwards.
+// Makes a handle's device current for one call and restores the caller's
+// device afterwards; `status` is the switch's result (nothing may run on the
+// device when it failed).
 struct DeviceGuard {
   int prev = -1;
+  cudaError_t status = cudaSuccess;
   explicit DeviceGuard(int dev) {
     if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != dev) cudaSetDevice(dev);
+    if (prev != dev) status = cudaSetDevice(dev);
   }
   ~DeviceGuard() {
     int cur = -1;
     if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
   }
 };
+
+// Declares the guard of a call and returns PU_ERR_CUDA from it when the device
+// cannot be made current.
+#define PU_DEVICE_GUARD(dev)                                                                 \
+  DeviceGuard g(dev);                                                                        \
+  if (g.status != cudaSuccess)                                                               \
+  return fail(PU_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(g.status))
 
 }  // namespace
 
@@ -544,7 +555,7 @@ int pu_dycore_create(const pu_config *cfg, pu_dycore **out) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PU_ERR_CUDA, "no CUDA device");
   if (cfg->device < 0 || cfg->device >= ndev) return fail(PU_ERR_INVALID, "bad device ordinal");
-  DeviceGuard g(cfg->device);
+  PU_DEVICE_GUARD(cfg->device);
   std::unique_ptr<pu_dycore> h(new pu_dycore);
   h->device = cfg->device;
   h->impl.reset(pu::make_impl(cfg->precision, cfg->ntracers));
@@ -576,7 +587,7 @@ int pu_dycore_destroy(pu_dycore *h) {
 
 int pu_dycore_init(pu_dycore *h, const pu_state_view *coupler, const double *immersed_proportion, int mem) {
   if (!h || !coupler) return fail(PU_ERR_INVALID, "null argument");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->init(coupler, immersed_proportion, mem);
 }
 
@@ -585,7 +596,7 @@ int pu_dycore_init_windmill(pu_dycore *h, const pu_state_view *coupler, const do
   if (!h || !coupler) return fail(PU_ERR_INVALID, "null argument");
   if (windmill_proj_weight && !immersed_proportion)
     return fail(PU_ERR_INVALID, "windmill_proj_weight needs immersed_proportion");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->init(coupler, immersed_proportion, mem, windmill_proj_weight);
 }
 
@@ -600,14 +611,14 @@ int pu_dycore_compute_time_step(const pu_dycore *h, double *dt) {
 int pu_dycore_load_state(pu_dycore *h, const pu_state_view *coupler) {
   if (!h || !coupler) return fail(PU_ERR_INVALID, "null argument");
   if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->load_state(coupler);
 }
 
 int pu_dycore_store_state(pu_dycore *h, pu_state_view *coupler) {
   if (!h || !coupler) return fail(PU_ERR_INVALID, "null argument");
   if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->store_state(coupler);
 }
 
@@ -615,7 +626,7 @@ int pu_dycore_advance(pu_dycore *h, double dt_dyn, int nsteps) {
   if (!h) return fail(PU_ERR_INVALID, "null handle");
   if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
   if (!(dt_dyn > 0) || nsteps < 0) return fail(PU_ERR_INVALID, "dt must be positive and nsteps non-negative");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->advance(dt_dyn, nsteps);
 }
 
@@ -623,7 +634,7 @@ int pu_dycore_time_step(pu_dycore *h, pu_state_view *coupler, double dt_phys, in
   if (!h || !coupler) return fail(PU_ERR_INVALID, "null argument");
   if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
   if (!(dt_phys > 0)) return fail(PU_ERR_INVALID, "dt_phys must be positive");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   double dt_dyn;
   pu_dycore_compute_time_step(h, &dt_dyn);
   const int n = (int)std::ceil(dt_phys / dt_dyn);
@@ -638,21 +649,21 @@ int pu_dycore_time_step(pu_dycore *h, pu_state_view *coupler, double dt_phys, in
 int pu_dycore_get_conserved(pu_dycore *h, double *state, double *tracers, int mem) {
   if (!h || !state) return fail(PU_ERR_INVALID, "null argument");
   if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->get_conserved(state, tracers, mem);
 }
 
 int pu_dycore_set_conserved(pu_dycore *h, const double *state, const double *tracers, int mem) {
   if (!h || !state || !tracers) return fail(PU_ERR_INVALID, "null argument");
   if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->set_conserved(state, tracers, mem);
 }
 
 int pu_dycore_get_hydrostasis(pu_dycore *h, double *dc, double *tc, double *pc, double *de, double *te, double *pe) {
   if (!h) return fail(PU_ERR_INVALID, "null handle");
   if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   auto &I = *h->impl;
   const int nzh = I.nzh, ne = I.cfg.nz + 1;
   double *dst_c[3] = {dc, tc, pc}, *dst_e[3] = {de, te, pe};
@@ -669,14 +680,14 @@ int pu_dycore_get_hydrostasis(pu_dycore *h, double *dc, double *tc, double *pc, 
 int pu_dycore_set_hydrostasis(pu_dycore *h, const double *dens, const double *theta, const double *pressure) {
   if (!h || !dens || !theta || !pressure) return fail(PU_ERR_INVALID, "null argument");
   if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->set_hydrostasis(dens, theta, pressure);
 }
 
 int pu_dycore_diagnostics(pu_dycore *h, pu_diag *out) {
   if (!h || !out) return fail(PU_ERR_INVALID, "null argument");
   if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->diagnostics(out);
 }
 
@@ -684,13 +695,13 @@ int pu_dycore_perturbations(pu_dycore *h, const pu_state_view *v, double *densit
                             double *pressure_pert, int mem) {
   if (!h || !v || !density_pert || !theta_pert || !pressure_pert) return fail(PU_ERR_INVALID, "null argument");
   if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->perturbations(v, density_pert, theta_pert, pressure_pert, mem);
 }
 
 int pu_dycore_synchronize(pu_dycore *h) {
   if (!h) return fail(PU_ERR_INVALID, "null handle");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->check_err();
 }
 
@@ -699,14 +710,14 @@ long long pu_dycore_kernel_launches(const pu_dycore *h) { return h ? h->impl->la
 int pu_dycore_learned_harvest(pu_dycore *h, long long n, unsigned long long seed) {
   if (!h || n <= 0) return fail(PU_ERR_INVALID, "bad argument");
   if (!h->impl->inited) return fail(PU_ERR_STATE, "pu_dycore_init has not been called");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->ml_harvest(long(n), seed);
 }
 
 int pu_dycore_learned_train(pu_dycore *h, int steps, int batch, double lr, unsigned long long seed,
                             pu_learn_stats *out) {
   if (!h || steps < 0 || batch <= 0 || !(lr > 0)) return fail(PU_ERR_INVALID, "bad argument");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   int rc = h->impl->ml_alloc();
   if (rc) return rc;
   return h->impl->ml_train(steps, batch, lr, seed, out);
@@ -714,7 +725,7 @@ int pu_dycore_learned_train(pu_dycore *h, int steps, int batch, double lr, unsig
 
 int pu_dycore_learned_get_weights(pu_dycore *h, float *theta) {
   if (!h || !theta) return fail(PU_ERR_INVALID, "null argument");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   int rc = h->impl->ml_alloc();
   if (rc) return rc;
   return h->impl->ml_get(theta);
@@ -722,7 +733,7 @@ int pu_dycore_learned_get_weights(pu_dycore *h, float *theta) {
 
 int pu_dycore_learned_set_weights(pu_dycore *h, const float *theta) {
   if (!h || !theta) return fail(PU_ERR_INVALID, "null argument");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   int rc = h->impl->ml_alloc();
   if (rc) return rc;
   return h->impl->ml_set(theta);
@@ -730,7 +741,7 @@ int pu_dycore_learned_set_weights(pu_dycore *h, const float *theta) {
 
 int pu_dycore_learned_eval(pu_dycore *h, const float *x, long long n, float *wl, float *wr, int use_mma) {
   if (!h || !x || !wl || n <= 0) return fail(PU_ERR_INVALID, "bad argument");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   int rc = h->impl->ml_alloc();
   if (rc) return rc;
   return h->impl->ml_eval(x, long(n), wl, wr, use_mma);
@@ -739,7 +750,7 @@ int pu_dycore_learned_eval(pu_dycore *h, const float *x, long long n, float *wl,
 int pu_dycore_learned_gradient(pu_dycore *h, const float *x, const float *t, long long n, float *grad,
                                double *loss) {
   if (!h || !x || !t || !grad || n <= 0 || n > (1 << 20)) return fail(PU_ERR_INVALID, "bad argument");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   int rc = h->impl->ml_alloc();
   if (rc) return rc;
   return h->impl->ml_gradient(x, t, long(n), grad, loss);
@@ -768,7 +779,7 @@ int pu_dycore_learned_set_threshold(pu_dycore *h, double max_jump) {
 
 int pu_dycore_learned_counts(pu_dycore *h, long long *learned, long long *fallback) {
   if (!h) return fail(PU_ERR_INVALID, "null handle");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   unsigned long long c[2] = {0, 0};
   auto &I = *h->impl;
   if (I.ml_counts) {
@@ -783,7 +794,7 @@ int pu_dycore_learned_counts(pu_dycore *h, long long *learned, long long *fallba
 
 int pu_dycore_profile(pu_dycore *h, int enable) {
   if (!h) return fail(PU_ERR_INVALID, "null handle");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   if (cudaStreamSynchronize(h->impl->st) != cudaSuccess) return fail(PU_ERR_CUDA, "stream synchronize failed");
   h->impl->prof_reset();
   h->impl->profiling = enable != 0;
@@ -792,7 +803,7 @@ int pu_dycore_profile(pu_dycore *h, int enable) {
 
 int pu_dycore_profile_read(pu_dycore *h, pu_profile *out) {
   if (!h || !out) return fail(PU_ERR_INVALID, "null argument");
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   return h->impl->prof_read(out);
 }
 
@@ -834,7 +845,7 @@ int pu_dycore_set_decomposition(pu_dycore *h, const pu_decomp *d, const unsigned
   if (I.weno_mode == PU_WENO_LEARNED) return fail(PU_ERR_UNSUPPORTED, "learned weights do not run on decomposed tiles");
   int rc = check_decomp(d, I.cfg);
   if (rc) return rc;
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   rc = set_decomposition(I, *d, nccl_id);
   if (rc) I.dec_release();
   return rc;
@@ -850,7 +861,7 @@ int pu_dycore_set_decomposition_host(pu_dycore *h, const pu_decomp *d, const pu_
   if (I.weno_mode == PU_WENO_LEARNED) return fail(PU_ERR_UNSUPPORTED, "learned weights do not run on decomposed tiles");
   int rc = check_decomp(d, I.cfg);
   if (rc) return rc;
-  DeviceGuard g(h->device);
+  PU_DEVICE_GUARD(h->device);
   rc = set_decomposition(I, *d, nullptr);
   if (!rc) {
     // Every rank checks the whole table of tiles before any halo moves.
@@ -877,7 +888,7 @@ int pu_dycore_group_init(pu_dycore *const *hs, int n, const pu_state_view *views
   int rc = group_tiles(hs, n, t, false);
   if (rc) return rc;
   if (!views) return fail(PU_ERR_INVALID, "null views");
-  DeviceGuard g(hs[0]->device);
+  PU_DEVICE_GUARD(hs[0]->device);
   for (int i = 0; i < n; i++) {
     rc = hs[i]->impl->dinit_begin(&views[i], props ? props[i] : nullptr, projs ? projs[i] : nullptr, mem);
     if (rc) return rc;
@@ -914,7 +925,7 @@ int pu_dycore_group_advance(pu_dycore *const *hs, int n, double dt, int nsteps) 
   if (rc) return rc;
   if (!(dt > 0)) return fail(PU_ERR_INVALID, "dt must be positive");
   if (nsteps <= 0) return PU_OK;
-  DeviceGuard g(hs[0]->device);
+  PU_DEVICE_GUARD(hs[0]->device);
   for (pu::ImplBase *a : t)
     if ((rc = a->dec_enforce())) return rc;
   for (int s = 0; s < nsteps; s++)
@@ -934,7 +945,7 @@ int pu_dycore_group_time_step(pu_dycore *const *hs, int n, pu_state_view *views,
   if (rc) return rc;
   if (!views) return fail(PU_ERR_INVALID, "null views");
   if (!(dt_phys > 0)) return fail(PU_ERR_INVALID, "dt_phys must be positive");
-  DeviceGuard g(hs[0]->device);
+  PU_DEVICE_GUARD(hs[0]->device);
   double dt_dyn;
   pu_dycore_compute_time_step(hs[0], &dt_dyn);
   const int nc = (int)std::ceil(dt_phys / dt_dyn);

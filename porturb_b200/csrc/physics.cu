@@ -553,17 +553,26 @@ int fail(int code, const std::string &msg) {
     if (e_ != cudaSuccess) return fail(PU_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+// Makes the handle's device current for one call and restores the caller's
+// device afterwards; `status` is the switch's result.
 struct Dev {
   int prev = -1;
+  cudaError_t status = cudaSuccess;
   explicit Dev(int d) {
     if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != d) cudaSetDevice(d);
+    if (prev != d) status = cudaSetDevice(d);
   }
   ~Dev() {
     int cur = -1;
     if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
   }
 };
+
+// The guard of a call; returns PU_ERR_CUDA from it when the device cannot be
+// made current.
+#define PH_DEVICE(dev)  \
+  Dev g(dev);           \
+  if (g.status != cudaSuccess) return fail(PU_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(g.status))
 
 bool on_device(int mem, const void *p) {
   if (mem == PU_MEM_DEVICE) return true;
@@ -724,7 +733,7 @@ int pu_physics_create(const pu_physics_config *cfg, const double *imm_prop_h, co
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PU_ERR_CUDA, "no CUDA device");
   if (cfg->device < 0 || cfg->device >= ndev) return fail(PU_ERR_INVALID, "bad device ordinal");
-  Dev g(cfg->device);
+  PH_DEVICE(cfg->device);
   pu_physics *h = new pu_physics;
   h->cfg = *cfg;
   h->st = static_cast<cudaStream_t>(cfg->stream);
@@ -789,7 +798,7 @@ int pu_les_apply(pu_physics *h, pu_state_view *v, double dt) {
   if (!h || !v) return fail(PU_ERR_INVALID, "null argument");
   if (h->cfg.idTKE < 0) return fail(PU_ERR_INVALID, "the LES closure needs the TKE tracer (les_closure.h:24-25)");
   if (!(dt > 0)) return fail(PU_ERR_INVALID, "dt must be positive");
-  Dev g(h->cfg.device);
+  PH_DEVICE(h->cfg.device);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -823,7 +832,7 @@ int pu_les_apply_to(pu_physics *h, const pu_state_view *in, pu_state_view *out, 
   if (!h || !in || !out) return fail(PU_ERR_INVALID, "null argument");
   if (h->cfg.idTKE < 0) return fail(PU_ERR_INVALID, "the LES closure needs the TKE tracer (les_closure.h:24-25)");
   if (!(dt > 0)) return fail(PU_ERR_INVALID, "dt must be positive");
-  Dev g(h->cfg.device);
+  PH_DEVICE(h->cfg.device);
   if (!in->rho_d || !out->uvel) return fail(PU_ERR_INVALID, "state view has a null array");
   if (!on_device(in->mem, in->rho_d) || !on_device(out->mem, out->uvel))
     return fail(PU_ERR_INVALID, "pu_les_apply_to takes device arrays");
@@ -845,7 +854,7 @@ int pu_les_apply_to(pu_physics *h, const pu_state_view *in, pu_state_view *out, 
 int pu_sponge_layer(pu_physics *h, pu_state_view *v, double dt, double time_scale, double top_prop) {
   if (!h || !v) return fail(PU_ERR_INVALID, "null argument");
   if (!(time_scale > 0) || !(top_prop > 0 && top_prop <= 1)) return fail(PU_ERR_INVALID, "bad sponge parameters");
-  Dev g(h->cfg.device);
+  PH_DEVICE(h->cfg.device);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -870,7 +879,7 @@ int pu_sponge_layer(pu_physics *h, pu_state_view *v, double dt, double time_scal
 
 int pu_geostrophic_forcing(pu_physics *h, pu_state_view *v, double dt, double lat_g, double u_g, double v_g) {
   if (!h || !v) return fail(PU_ERR_INVALID, "null argument");
-  Dev g(h->cfg.device);
+  PH_DEVICE(h->cfg.device);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -890,7 +899,7 @@ int pu_geostrophic_forcing(pu_physics *h, pu_state_view *v, double dt, double la
 
 int pu_surface_fluxes(pu_physics *h, pu_state_view *v, double dt) {
   if (!h || !v) return fail(PU_ERR_INVALID, "null argument");
-  Dev g(h->cfg.device);
+  PH_DEVICE(h->cfg.device);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -910,7 +919,7 @@ int pu_uniform_pg_wind_forcing(pu_physics *h, pu_state_view *v, double dt, doubl
                                unsigned long long update_cycles, pu_uniform_pg_state *state) {
   if (!h || !v || !state) return fail(PU_ERR_INVALID, "null argument");
   if (update_cycles == 0 || !(tau > 0)) return fail(PU_ERR_INVALID, "bad uniform_pg_wind_forcing parameters");
-  Dev g(h->cfg.device);
+  PH_DEVICE(h->cfg.device);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -963,7 +972,7 @@ int pu_uniform_pg_wind_forcing_height(pu_physics *h, pu_state_view *v, double dt
     }
   if (k1 < 0) return fail(PU_ERR_INVALID, "uniform_pg_wind_forcing_height: height below the first level centre");
   if (k1 + 1 >= nz) return fail(PU_ERR_INVALID, "uniform_pg_wind_forcing_height needs nz >= 2");
-  Dev g(h->cfg.device);
+  PH_DEVICE(h->cfg.device);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -990,7 +999,7 @@ int pu_time_averager_accumulate(pu_physics *h, const pu_state_view *v, pu_time_a
                       a->long_avg_u, a->long_avg_v, a->long_avg_w};
   for (double *p : host)
     if (!p) return fail(PU_ERR_INVALID, "null time-average array");
-  Dev g(h->cfg.device);
+  PH_DEVICE(h->cfg.device);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -1028,7 +1037,7 @@ int pu_edge_sponge_set_column(pu_physics *h, const pu_state_view *v, const int *
   if (nfields < 1 || nfields > 8) return fail(PU_ERR_INVALID, "edge sponge: 1 to 8 fields");
   for (int l = 0; l < nfields; l++)
     if (fields[l] < 0 || fields[l] >= S) return fail(PU_ERR_INVALID, "edge sponge: bad field index");
-  Dev g(h->cfg.device);
+  PH_DEVICE(h->cfg.device);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -1058,7 +1067,7 @@ int pu_edge_sponge_apply(pu_physics *h, pu_state_view *v, const int *fields, int
     if (fields[l] < 0 || fields[l] >= S) return fail(PU_ERR_INVALID, "edge sponge: bad field index");
   if (nx_glob < h->cfg.nx || ny_glob < h->cfg.ny || i_beg < 0 || j_beg < 0)
     return fail(PU_ERR_INVALID, "edge sponge: bad tile placement");
-  Dev g(h->cfg.device);
+  PH_DEVICE(h->cfg.device);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -1090,14 +1099,14 @@ int pu_edge_sponge_apply(pu_physics *h, pu_state_view *v, const int *fields, int
 
 int pu_physics_synchronize(pu_physics *h) {
   if (!h) return fail(PU_ERR_INVALID, "null handle");
-  Dev g(h->cfg.device);
+  PH_DEVICE(h->cfg.device);
   PH_CK(cudaStreamSynchronize(h->st));
   return PU_OK;
 }
 
 int pu_physics_last_les_ms(pu_physics *h, double *ms) {
   if (!h || !ms) return fail(PU_ERR_INVALID, "null argument");
-  Dev g(h->cfg.device);
+  PH_DEVICE(h->cfg.device);
   PH_CK(cudaEventSynchronize(h->e1));
   float f = 0;
   PH_CK(cudaEventElapsedTime(&f, h->e0, h->e1));

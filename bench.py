@@ -31,8 +31,9 @@ the same steps from the same state.  One JSON line on rank 0.
 * abl: the neutral boundary layer (256x256x128, dx = 10 m, water_vapor + TKE)
   as an extra object: the plain dycore rate, the physics modules its driver
   runs beside the dycore (FP64), and the same grid as 2x2 tiles of one GPU.
-* Multi-GPU: N ranks run N independent replicas (ensemble members, each its
-  own seed) with no collective in the data path (weak scaling).
+* Multi-GPU: N ranks run N independent replicas (ensemble members: the same
+  city, each rank its own noise seed) with no collective in the data path
+  (weak scaling).
 """
 from __future__ import annotations
 
@@ -71,9 +72,11 @@ def workload_name():
 
 
 def build_case(seed=0, window=None):
+    """The workload; replicas (ensemble members) share the city (layout seed 1)
+    and differ in their theta noise (seed = rank)."""
     from porturb_b200 import cases
     return cases.urban_canopy(nx=WORKLOAD["nx"], ny=WORKLOAD["ny"], nz=WORKLOAD["nz"], dx=WORKLOAD["dx"],
-                              seed=seed, window=window)
+                              seed=seed, window=window, layout_seed=1)
 
 
 def measured_peaks():

@@ -212,7 +212,8 @@ def abl_neutral(nx=256, ny=256, nz=128, dx=10.0, theta0=300.0, z_inv=500.0, laps
 
 
 def urban_canopy(nx=512, ny=512, nz=128, dx=2.0, theta0=300.0, lot=40.0, foot=(20.0, 32.0), height=(10.0, 60.0),
-                 occupancy=0.7, noise_amp=0.1, seed=0, cfl=0.6, steps=1000, u0=10.0, window=None) -> Case:
+                 occupancy=0.7, noise_amp=0.1, seed=0, cfl=0.6, steps=1000, u0=10.0, window=None,
+                 layout_seed=None) -> Case:
     """Immersed-boundary urban canopy: seeded cuboid buildings, one per
     occupied 40 m lot, footprints U[20,32] m, heights U[10,60] m, 70 % lot
     occupancy, a binary immersed mask, theta = 300 K with seeded +-0.1 K noise
@@ -220,7 +221,9 @@ def urban_canopy(nx=512, ny=512, nz=128, dx=2.0, theta0=300.0, lot=40.0, foot=(2
 
     window = (i0, j0, bx, by) gives only the columns [i0, i0+bx) x [j0, j0+by)
     of the nx x ny domain, as a case of its own (the same buildings and noise,
-    which are keyed by lot and by global cell index), without forming the rest."""
+    which are keyed by lot and by global cell index), without forming the rest.
+    The noise is keyed by `seed`, the buildings by `layout_seed` (seed + 1 by
+    default): ensemble members share a city with layout_seed fixed."""
     i0, j0, bx, by = window if window is not None else (0, 0, nx, ny)
     if not (0 <= i0 and i0 + bx <= nx and 0 <= j0 and j0 + by <= ny and bx > 0 and by > 0):
         raise ValueError("window outside the domain")
@@ -230,7 +233,7 @@ def urban_canopy(nx=512, ny=512, nz=128, dx=2.0, theta0=300.0, lot=40.0, foot=(2
     xlen, ylen = nx * dx, ny * dx
     nlx, nly = int(xlen // lot), int(ylen // lot)
     rng_idx = np.arange(nlx * nly * 5, dtype=np.uint64)
-    r = splitmix64_uniform(seed + 1, rng_idx).reshape(nly, nlx, 5)
+    r = splitmix64_uniform(seed + 1 if layout_seed is None else layout_seed, rng_idx).reshape(nly, nlx, 5)
     xc = (np.arange(i0, i0 + bx) + 0.5) * dx
     yc = (np.arange(j0, j0 + by) + 0.5) * dx
     zc = (np.arange(nz) + 0.5) * dx

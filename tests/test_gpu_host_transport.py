@@ -124,3 +124,106 @@ def test_two_ranks_over_host_transport_equal_undecomposed(name, precision, tmp_p
     assert np.array_equal(cons, cons_ref), np.abs(cons - cons_ref).max()
     assert np.array_equal(ctr, ctr_ref)
     assert np.array_equal(arr, arr_ref), np.abs(arr - arr_ref).max()
+
+
+class _OneRank:
+    """pu_host_transport callbacks for a grid of one tile (the rank is every
+    neighbour of itself); `fail` names a callback that reports failure from
+    its n-th call on."""
+
+    def __init__(self, fail=None, after=0):
+        import ctypes as C
+        from porturb_b200 import capi
+        self.C, self.fail, self.after = C, fail, after
+        self.calls = {"exchange": 0, "allreduce_sum_f64": 0, "allgather": 0}
+        self._fns = (capi.EXCHANGE_FN(self._ex), capi.ALLREDUCE_FN(self._ar), capi.ALLGATHER_FN(self._ag))
+        self.struct = capi.pu_host_transport(self._fns[0], self._fns[1], self._fns[2], None)
+
+    def _bad(self, name):
+        self.calls[name] += 1
+        return self.fail == name and self.calls[name] > self.after
+
+    def _ex(self, user, snd, rcv, nbytes, nbr):
+        if self._bad("exchange"):
+            return 5
+        for d in range(4):
+            if nbytes[d]:
+                assert nbr[d] == 0 and nbytes[d ^ 1] == nbytes[d]
+                self.C.memmove(rcv[d], snd[d ^ 1], nbytes[d])
+        return 0
+
+    def _ar(self, user, buf, n):
+        return 5 if self._bad("allreduce_sum_f64") else 0
+
+    def _ag(self, user, src, out, nbytes):
+        if self._bad("allgather"):
+            return 5
+        self.C.memmove(out, src, nbytes)
+        return 0
+
+
+def _one_tile(case, tr, precision="f32"):
+    t = decomp.tiles(case.nx, case.ny, 1, 1)[0]
+    h = Dycore.from_case(case, precision=precision, device=0)
+    decomp.set_decomposition_host(h, t, case.nx, case.ny, tr)
+    return h
+
+
+def test_one_tile_over_host_transport_equals_undecomposed(gpu_lib):
+    """One tile whose halos come back through the host transport from its own
+    edges (periodic): the library's host exchange, summed profiles and
+    immersed halo gather, bit for bit against the undecomposed run."""
+    case = cases.small_mixed(nx=24, ny=16, nz=12)
+    tr = _OneRank()
+    h = _one_tile(case, tr)
+    g = Dycore.from_case(case, precision="f32", device=0)
+    prop = np.ascontiguousarray(case.immersed_proportion)
+    outs = []
+    for d in (h, g):
+        st, trc = _arrays(case, False)
+        d.init(*st, trc, prop)
+        st, trc = _arrays(case, True)
+        d.load_state(*st, trc)
+        d.advance(d.compute_time_step(), 3)
+        outs.append(d.get_conserved())
+        d.close()
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    assert tr.calls == {"exchange": 2 + 3 * 3, "allreduce_sum_f64": 1, "allgather": 1}
+
+
+@pytest.mark.parametrize("where", ["allgather", "allreduce_sum_f64", "init_exchange", "step_exchange"])
+def test_transport_failure_is_reported(where, gpu_lib):
+    """A callback that returns non-zero makes the call that used it return
+    PU_ERR_TRANSPORT: set-up (allgather; the handle stays undecomposed and can
+    be decomposed again), init (the column sums, the immersed halo exchange)
+    or a step (the halo exchange of a stage)."""
+    from porturb_b200 import PortUrbError, capi
+    case = cases.small_mixed(nx=24, ny=16, nz=12)
+    name = {"init_exchange": "exchange", "step_exchange": "exchange"}.get(where, where)
+    tr = _OneRank(fail=name, after=2 if where == "step_exchange" else 0)
+    t = decomp.tiles(case.nx, case.ny, 1, 1)[0]
+    h = Dycore.from_case(case, precision="f32", device=0)
+    if where == "allgather":
+        with pytest.raises(PortUrbError) as e:
+            decomp.set_decomposition_host(h, t, case.nx, case.ny, tr)
+        assert e.value.status == capi.PU_ERR_TRANSPORT
+        decomp.set_decomposition_host(h, t, case.nx, case.ny, _OneRank())   # not left half decomposed
+        h.close()
+        return
+    decomp.set_decomposition_host(h, t, case.nx, case.ny, tr)
+    st, trc = _arrays(case, False)
+    prop = np.ascontiguousarray(case.immersed_proportion)
+    if where in ("allreduce_sum_f64", "init_exchange"):
+        with pytest.raises(PortUrbError) as e:
+            h.init(*st, trc, prop)
+        assert e.value.status == capi.PU_ERR_TRANSPORT
+        h.close()
+        return
+    h.init(*st, trc, prop)
+    st, trc = _arrays(case, True)
+    h.load_state(*st, trc)
+    with pytest.raises(PortUrbError) as e:
+        h.advance(h.compute_time_step(), 1)
+    assert e.value.status == capi.PU_ERR_TRANSPORT
+    assert b"exchange returned 5" in capi.load().pu_last_error()
+    h.close()

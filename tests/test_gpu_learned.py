@@ -180,11 +180,19 @@ def test_learned_modes_rejected_where_unsupported(gpu_lib):
 
 
 def test_trained_network_gain_vs_fp64(gpu_lib):
-    """Warm bubble 64x4x32, 60 steps: the FP32 run with learned weights stays
-    close to the FP64 build (momentum and rho*theta within 2e-3 of the field
-    scale) and is several times more accurate than the same kernels with the
-    untrained network (measured on a B200: 4x-10x for rho*u, rho*w and
-    rho*theta): the gain of training."""
+    """Warm bubble 64x4x32, 60 steps, errors against the FP64 build.
+
+    * The gain of training: the FP32 run with learned weights stays close to
+      the FP64 build (momentum and rho*theta within 2e-3 of the field scale)
+      and is several times more accurate than the same kernels with the
+      untrained network (measured on a B200: 4x-10x for rho*u, rho*w and
+      rho*theta).
+    * Against the method without the network (the plain limiter) there is no
+      gain: the plain FP32 run is more accurate (measured 1.4e-5 / 4.2e-5 /
+      1.3e-4 for rho*u / rho*w / rho*theta against the learned form's 7.1e-4 /
+      6.5e-4 / 8.5e-4) and faster (the bench's `learned` object).  The
+      learned form's error is bounded here at 100x the plain form's, so that a
+      regression of either shows."""
     case = cases.warm_bubble(nx=64, ny=4, nz=32)
     g = _handle(case)
     dt = g.compute_time_step()
@@ -210,3 +218,4 @@ def test_trained_network_gain_vs_fp64(gpu_lib):
     for q in (1, 3, 4):
         assert e_lrn[q] < 2e-3
         assert e_lrn[q] < 0.35 * e_unt[q]
+        assert e_plain[q] < e_lrn[q] < 100 * e_plain[q]

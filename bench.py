@@ -30,7 +30,8 @@ the same steps from the same state.  One JSON line on rank 0.
   GPU (Adam, batch 65536); kernel times and the fallback fraction.
 * abl: the neutral boundary layer (256x256x128, dx = 10 m, water_vapor + TKE)
   as an extra object: the plain dycore rate, the physics modules its driver
-  runs beside the dycore (FP64), and the same grid as 2x2 tiles of one GPU.
+  runs beside the dycore (FP64), the driver's whole step with the TKE LES
+  closure (driver_chain), and the same grid as 2x2 tiles of one GPU.
 * Multi-GPU: N ranks run N independent replicas (ensemble members: the same
   city, each rank its own noise seed) with no collective in the data path
   (weak scaling).
@@ -293,8 +294,28 @@ def abl_extras(stream, world, steps, warmup, rank, no_physics, no_decomposed):
            "ms_per_step": ms / steps, "kernel_ms": kern}
     if not no_physics:
         out["physics"] = physics_modules(case, stream, world)
+        out["driver_chain"] = driver_chain(world, rank)
     if not no_decomposed:
         out["decomposed"] = decomposed_tiles(case, world, min(steps, 10), warmup)
+    return out
+
+
+def driver_chain(world, rank, calls=5):
+    """The boundary-layer driver's whole step (abl_neutral.cpp:93-108) on
+    device coupler arrays of the same workload, through the module API:
+    geostrophic forcing, the dycore's time_step of dt_phys = 10 dycore steps,
+    sponge, surface fluxes, the TKE LES closure and the time averager; CUDA
+    events over `calls` driver steps after one, cell-steps/s of the dycore
+    steps inside them, the TKE LES closure's cost included."""
+    import types
+    from porturb_b200 import cases
+    from porturb_b200.run_case import run_driver
+    case = cases.abl_neutral(nx=ABL["nx"], ny=ABL["ny"], nz=ABL["nz"], dx=ABL["dx"], seed=rank)
+    a = types.SimpleNamespace(case="abl_neutral", nx=ABL["nx"], ny=ABL["ny"], nz=ABL["nz"], steps=calls,
+                              precision="f32")
+    out = run_driver(case, a)
+    out["ms_per_call"] = reduce_max(out["ms_per_call"], world)
+    out["cell_steps_per_s"] = world * case.ncells * out["dycore_steps_per_call"] / (out["ms_per_call"] / 1e3)
     return out
 
 

@@ -4,12 +4,16 @@
     python -m porturb_b200.run_case abl_neutral --nz 64 --learned --train-steps 300
     python -m porturb_b200.run_case urban_canopy --nx 1024 --ny 1024 --nz 256 --dx 1 --steps 300 --diag-every 50
     python -m porturb_b200.run_case abl_neutral --nx 512 --ny 512 --nz 256 --steps 500 --compare
+    python -m porturb_b200.run_case abl_neutral --driver --compare --steps 50
+    python -m porturb_b200.run_case urban_canopy --driver --chain periodic --compare --steps 100
 
 Plain mode advances the FP32 (or --precision f64) dycore; --learned first
 harvests stencils from the initial state, trains the network on the GPU and
 then advances with learned weights; --modules times the physics modules
 (LES closure, sponge, geostrophic forcing, surface fluxes) instead; --driver
-runs the reference driver's whole chain of modules per dt_phys.  Prints
+runs the reference driver's whole chain of modules per dt_phys (--chain abl,
+city or periodic; with --compare, the FP32 and FP64 dycore in the same chain
+from the same state, with the errors per coupler array).  Prints
 one JSON line with the per-kernel CUDA-event times and, in learned mode, the
 fallback fraction.  --compare runs the plain FP32 form, the learned form
 (trained on stencils harvested from the initial state) and the FP64 build
@@ -68,56 +72,143 @@ def run_modules(case, a):
     return out
 
 
-def run_driver(case, a):
-    """The reference driver's loop with this package's modules on device
-    coupler arrays: per call of dt_phys = 10 dycore steps, the boundary-layer
-    chain (abl_neutral.cpp:93-108: geostrophic forcing, dycore, sponge,
-    surface fluxes, LES closure, time averager) or the urban one
-    (city.cpp:137-142: edge sponge, dycore, sponge, surface fluxes, LES
-    closure, time averager).  CUDA-event time of `steps` calls after one."""
+CHAINS = {
+    "abl": "boundary layer (abl_neutral.cpp:93-108)",
+    "city": "urban with edge sponge (city.cpp:137-142)",
+    "periodic": "periodic urban driven by a pressure gradient (cubes_periodic.cpp:144-156)",
+}
+
+
+def _chain_of(a):
+    chain = getattr(a, "chain", None)
+    if chain:
+        return chain
+    return "city" if a.case == "urban_canopy" else "abl"
+
+
+def _driver_run(case, a, precision, calls, dt=None, warm=1):
+    """One driver run: a coupler of the case on this GPU, the chain's modules
+    initialised as the reference's drivers do (LES closure, dycore, time
+    averager), the perturbed state, then `warm` untimed and `calls` timed
+    calls of dt_phys = 10 dycore steps (or `dt`).  Per call:
+      abl      -- geostrophic forcing, dycore, sponge, surface fluxes, LES
+                  closure, time averager (abl_neutral.cpp:93-108);
+      city     -- edge sponge, dycore, sponge, surface fluxes, LES closure,
+                  time averager (city.cpp:137-142);
+      periodic -- the mean wind at 100 m relaxed to (10, 0) m/s on a time
+                  scale of 100 dt_phys, dycore, LES closure, surface fluxes,
+                  time averager (cubes_periodic.cpp:144-156).
+    Returns the coupler, dt_phys, the ms per timed call (CUDA events) and
+    the dycore steps per call."""
     import torch
     from . import (Dynamics_Euler_Stratified_WenoFV, EdgeSponge, LES_Closure, Time_Averager, apply_surface_fluxes,
                    assign_coupler_state, case_coupler, geostrophic_wind_forcing, sponge_layer)
-    from .physics import register_immersed_halos
+    from .physics import register_immersed_halos, uniform_pg_wind_forcing_height
+    chain = _chain_of(a)
     c = case_coupler(case, device="cuda:%d" % torch.cuda.current_device())
     register_immersed_halos(c, case)
-    les, dyn, tavg, edge = LES_Closure(), Dynamics_Euler_Stratified_WenoFV(precision=a.precision), Time_Averager(), \
+    les, dyn, tavg, edge = LES_Closure(), Dynamics_Euler_Stratified_WenoFV(precision=precision), Time_Averager(), \
         EdgeSponge()
     les.init(c)
     dyn.init(c)
     tavg.init(c)
-    urban = a.case == "urban_canopy"
-    if urban:
+    if chain == "city":
         edge.set_column(c)
     assign_coupler_state(c, case, perturbed=True)
-    dt = 10 * dyn.compute_time_step(c)
+    if dt is None:
+        dt = 10 * dyn.compute_time_step(c)
     sub = []
 
     def call():
-        if urban:
+        if chain == "city":
             edge.apply(c, 0.01, 0.01, 0.01, 0.01)
-        else:
+        elif chain == "abl":
             geostrophic_wind_forcing(c, dt, 43.289340204, 10.0, 0.0)
+        else:
+            uniform_pg_wind_forcing_height(c, dt, 100.0, 10.0, 0.0, dt * 100)
         sub.append(dyn.time_step(c, dt))
-        sponge_layer(c, dt, dt if urban else dt * 100, 0.02 if urban else 0.1)
-        apply_surface_fluxes(c, dt)
-        les.apply(c, dt)
+        if chain == "periodic":
+            les.apply(c, dt)
+            apply_surface_fluxes(c, dt)
+        else:
+            sponge_layer(c, dt, dt if chain == "city" else dt * 100, 0.02 if chain == "city" else 0.1)
+            apply_surface_fluxes(c, dt)
+            les.apply(c, dt)
         tavg.accumulate(c, dt)
         c.set_option("elapsed_time", c.get_option("elapsed_time") + dt)
 
-    call()
+    for _ in range(warm):
+        call()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(a.steps):
+    for _ in range(calls):
         call()
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / a.steps
-    return {"case": a.case, "grid": [a.nx, a.ny, a.nz], "driver": "urban (city.cpp)" if urban else
-            "boundary layer (abl_neutral.cpp)", "calls": a.steps, "dycore_steps_per_call": sub[-1], "ms_per_call": ms,
-            "cell_steps_per_s": case.ncells * sub[-1] / (ms / 1e3),
+    return c, dt, e0.elapsed_time(e1) / max(calls, 1), sub[-1]
+
+
+def _release(c):
+    for h in list(c.module_state.values()):
+        if hasattr(h, "close"):
+            h.close()
+    c.module_state.clear()
+
+
+def run_driver(case, a):
+    """The reference driver's loop with this package's modules on device
+    coupler arrays (the chains of `_driver_run`); CUDA-event time of `steps`
+    calls after one."""
+    c, dt, ms, sub = _driver_run(case, a, a.precision, a.steps)
+    _release(c)
+    return {"case": a.case, "grid": [a.nx, a.ny, a.nz], "driver": CHAINS[_chain_of(a)], "calls": a.steps,
+            "dycore_steps_per_call": sub, "ms_per_call": ms, "cell_steps_per_s": case.ncells * sub / (ms / 1e3),
             "note": "cell-steps/s of the whole driver step: the dycore's 10 steps and the modules beside it"}
+
+
+def coupler_errors(X, D):
+    """Per coupler array (density_dry, uvel, vvel, wvel, temp, tracers): L2
+    and Linf of X - D over D's departure from its level means (FP64 on the
+    GPU)."""
+    import torch
+    out = {}
+    for name, x in X.items():
+        d = D[name].to(torch.float64)
+        diff = x.to(torch.float64) - d
+        dep = d - d.mean(dim=(1, 2), keepdim=True)
+        dl2, dli = float(torch.sqrt(torch.mean(diff * diff))), float(diff.abs().max())
+        pl2, pli = float(torch.sqrt(torch.mean(dep * dep))), float(dep.abs().max())
+        out[name] = {"l2": dl2 / pl2 if pl2 > 0 else (0.0 if dl2 == 0 else None),
+                     "linf": dli / pli if pli > 0 else (0.0 if dli == 0 else None)}
+        del d, diff, dep
+    return out
+
+
+def run_driver_compare(case, a):
+    """The driver chain with the FP32 dycore and with the FP64 build from the
+    same initial state and the same dt_phys, `steps` timed calls each (after
+    none: every dycore step of the run is in the timed calls): rates and, per
+    coupler array, the FP32 run's error against the FP64 run."""
+    import torch
+    names = ["density_dry", "uvel", "vvel", "wvel", "temp"]
+    c, dt, ms32, sub = _driver_run(case, a, "f32", a.steps, warm=0)
+    keep = {n: c.get(n).clone() for n in names + list(c.get_tracer_names())}
+    _release(c)
+    del c
+    torch.cuda.empty_cache()
+    c, _, ms64, _ = _driver_run(case, a, "f64", a.steps, dt=dt, warm=0)
+    ref = {n: c.get(n) for n in keep}
+    errs = coupler_errors(keep, ref)
+    _release(c)
+    n = case.ncells * sub
+    return {"case": a.case, "grid": [a.nx, a.ny, a.nz], "driver": CHAINS[_chain_of(a)], "calls": a.steps,
+            "dycore_steps": a.steps * sub, "dt_phys": dt,
+            "f32": {"ms_per_call": ms32, "cell_steps_per_s": n / (ms32 / 1e3)},
+            "f64": {"ms_per_call": ms64, "cell_steps_per_s": n / (ms64 / 1e3)},
+            "f32_vs_f64": errs,
+            "error_norm": "L2 and Linf of (FP32 run - FP64 run) over the FP64 run's departure from its level means",
+            "note": "the physics modules are FP64 in both runs; only the dycore's precision differs"}
 
 
 def _snapshot(g, S, shape):
@@ -228,12 +319,17 @@ def main(argv=None):
     ap.add_argument("--driver", action="store_true",
                     help="run the reference driver's module chain per dt_phys (boundary layer or urban) on device "
                          "coupler arrays")
+    ap.add_argument("--chain", choices=sorted(CHAINS), default=None,
+                    help="--driver: the module chain (default: city for urban_canopy, abl otherwise)")
     ap.add_argument("--modules", action="store_true",
                     help="time the physics modules (LES closure, sponge, geostrophic forcing, surface fluxes) "
                          "on the case's coupler arrays instead of dycore steps")
     a = ap.parse_args(argv)
 
     case = CASES[a.case](a)
+    if a.driver and a.compare:
+        print(json.dumps(run_driver_compare(case, a)), flush=True)
+        return
     if a.compare:
         print(json.dumps(run_compare(case, a)), flush=True)
         return

@@ -76,6 +76,7 @@ CHAINS = {
     "abl": "boundary layer (abl_neutral.cpp:93-108)",
     "city": "urban with edge sponge (city.cpp:137-142)",
     "periodic": "periodic urban driven by a pressure gradient (cubes_periodic.cpp:144-156)",
+    "dycore": "the dycore's time_step alone (no other module)",
 }
 
 
@@ -97,7 +98,8 @@ def _driver_run(case, a, precision, calls, dt=None, warm=1):
                   time averager (city.cpp:137-142);
       periodic -- the mean wind at 100 m relaxed to (10, 0) m/s on a time
                   scale of 100 dt_phys, dycore, LES closure, surface fluxes,
-                  time averager (cubes_periodic.cpp:144-156).
+                  time averager (cubes_periodic.cpp:144-156);
+      dycore   -- the dycore alone (the same init, no other module applied).
     Returns the coupler, dt_phys, the ms per timed call (CUDA events) and
     the dycore steps per call."""
     import torch
@@ -120,6 +122,10 @@ def _driver_run(case, a, precision, calls, dt=None, warm=1):
     sub = []
 
     def call():
+        if chain == "dycore":
+            sub.append(dyn.time_step(c, dt))
+            c.set_option("elapsed_time", c.get_option("elapsed_time") + dt)
+            return
         if chain == "city":
             edge.apply(c, 0.01, 0.01, 0.01, 0.01)
         elif chain == "abl":

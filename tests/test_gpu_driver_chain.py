@@ -8,12 +8,18 @@ build from the same state and dt_phys:
   with an 8 m/s initial wind (mean wind at 100 m relaxed toward 10 m/s on a
   time scale of 100 dt_phys).
 
-Two calls of dt_phys = 10 dycore steps each.  Every coupler array stays
-finite; the FP32 run is within L2 < 1e-4 and Linf < 1e-3 of the FP64 run's
-departure from its level means (the physics modules are FP64 in both, so the
-difference is the dycore's FP32 state over 20 steps); the LES closure moved
-the TKE off its initial 0.1; in the periodic chain the mean wind at 100 m
-rose by the forcing's 0.01 (10 - u) per call, 0.02 + 0.0198 m/s, to 10 %.
+Two calls of dt_phys = 10 dycore steps each, and the same two calls of the
+dycore alone (chain "dycore": the same init, no other module).  Every coupler
+array stays finite.  The physics modules are FP64 in both runs, so the
+difference between the FP32 and FP64 runs starts in the dycore's FP32 state;
+the modules must not amplify it: per coupler array, the chain's L2 (Linf) of
+FP32 - FP64 over the FP64 run's departure from its level means is within 2x
+(5x) of the dycore-alone difference.  Measured on a B200: 1.0-1.35x (L2) and
+up to 2.1x (Linf); the dycore-alone differences are 1e-5 - 4e-2 of the
+departure (largest for the winds of the boundary layer, whose departures
+from the level means are still small).  The LES closure moved the TKE off
+its initial 0.1; in the periodic chain the mean wind at 100 m rose by the
+forcing's 0.01 (10 - u) per call, 0.02 + 0.0198 m/s (0.0398 measured).
 """
 import types
 
@@ -36,30 +42,42 @@ def _args(case, chain):
     return types.SimpleNamespace(case=case.name, nx=case.nx, ny=case.ny, nz=case.nz, chain=chain)
 
 
+def _f32_vs_f64(case, chain, names):
+    a = _args(case, chain)
+    c, dt, _, sub = _driver_run(case, a, "f32", 2, warm=0)
+    assert sub == 10
+    f32 = {n: c.get(n).clone() for n in names}
+    _release(c)
+    c, _, _, _ = _driver_run(case, a, "f64", 2, dt=dt, warm=0)
+    return f32, c
+
+
 @pytest.mark.parametrize("chain", sorted(CHAIN_CASES))
 def test_driver_chain_f32_against_f64(chain, gpu_lib):
     import torch
     case = CHAIN_CASES[chain]()
-    a = _args(case, chain)
-    c, dt, ms, sub = _driver_run(case, a, "f32", 2, warm=0)
-    assert sub == 10
-    names = ["density_dry", "uvel", "vvel", "wvel", "temp"] + list(c.get_tracer_names())
-    f32 = {n: c.get(n).clone() for n in names}
-    _release(c)
-    c, _, _, _ = _driver_run(case, a, "f64", 2, dt=dt, warm=0)
-    f64 = {n: c.get(n) for n in names}
+    names = ["density_dry", "uvel", "vvel", "wvel", "temp"]
+    f32, c = _f32_vs_f64(case, chain, names + ["water_vapor", "TKE"])
+    f64 = {n: c.get(n) for n in f32}
     for n, x in f32.items():
         assert torch.isfinite(x).all(), (chain, n)
         assert torch.isfinite(f64[n]).all(), (chain, n)
-    errs = coupler_errors({n: f32[n] for n in names[:5]}, f64)
-    for n, e in errs.items():
-        print(chain, n, "FP32 run vs FP64 run (of departure): %.2e / %.2e" % (e["l2"], e["linf"]))
-        assert e["l2"] is not None and e["l2"] < 1e-4 and e["linf"] < 1e-3, (chain, n, e)
+    errs = coupler_errors({n: f32[n] for n in names}, f64)
     assert float((f64["TKE"] - 0.1).abs().max()) > 1e-6, chain
     if chain == "periodic":
         # Levels 49 and 50 (centres 99 m and 101 m) hold the 100 m mean.
         u0 = float(np.asarray(case.uvel)[49:51].mean())
         u1 = float(f64["uvel"][49:51].mean())
         print("mean u at 100 m: %.5f -> %.5f" % (u0, u1))
-        assert abs((u1 - u0) - 0.0398) < 0.004, (u0, u1)
+        assert abs((u1 - u0) - 0.0398) < 0.002, (u0, u1)
     _release(c)
+    del f32, f64
+    d32, c = _f32_vs_f64(case, "dycore", names)
+    base = coupler_errors(d32, {n: c.get(n) for n in names})
+    _release(c)
+    for n in names:
+        e, b = errs[n], base[n]
+        print(chain, n, "FP32 - FP64 (of departure): chain %.2e / %.2e, dycore alone %.2e / %.2e"
+              % (e["l2"], e["linf"], b["l2"], b["linf"]))
+        assert e["l2"] is not None and b["l2"] is not None, (chain, n)
+        assert e["l2"] <= 2 * b["l2"] + 1e-7 and e["linf"] <= 5 * b["linf"] + 1e-6, (chain, n, e, b)

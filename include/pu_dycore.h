@@ -87,6 +87,12 @@ typedef struct pu_config {
                                               immersed code only on the levels (z chunks) that an
                                               immersed flag reaches; 1: on every level (the same
                                               results) */
+  int serial_io;                           /* 0: pu_dycore_time_step on host arrays overlaps the
+                                              copies in with the first stage and the copies out
+                                              with the last, chunk by chunk, where the path allows
+                                              it (FP32, weno_all, plain weights, walls in z,
+                                              nz >= 64); 1: copies in, steps, copies out (the
+                                              same results) */
 } pu_config;
 
 /* The coupler-side state: density_dry, uvel, vvel, wvel, temp and the tracer
@@ -148,7 +154,9 @@ int pu_dycore_compute_time_step(const pu_dycore *h, double *dt);
 /* time_step(coupler, dt_phys), dynamics_rk.h:103-137: converts the coupler
  * state in, runs ncycles = ceil(dt_phys/dt_dyn) SSPRK3 steps of
  * dt_phys/ncycles, converts back into the same arrays.  Synchronous; returns
- * PU_ERR_NONFINITE if the state became non-finite.  ncycles may be NULL. */
+ * PU_ERR_NONFINITE if the state became non-finite.  ncycles may be NULL.
+ * On host arrays the copies overlap the steps chunk by chunk (see
+ * pu_config.serial_io); the results are the same either way. */
 int pu_dycore_time_step(pu_dycore *h, pu_state_view *coupler, double dt_phys, int *ncycles);
 
 /* convert_coupler_to_dynamics (dynamics_rk.h:1304-1352) into the resident

@@ -46,7 +46,8 @@ class pu_config(C.Structure):
                 ("enable_gravity", C.c_int), ("weno_all", C.c_int),
                 ("precision", C.c_int), ("weno_mode", C.c_int), ("device", C.c_int),
                 ("stream", C.c_void_p), ("z_chunk", C.c_int), ("thread_loads", C.c_int),
-                ("imm_all_levels", C.c_int)]
+                ("imm_all_levels", C.c_int),
+                ("serial_io", C.c_int)]
 
 
 class pu_state_view(C.Structure):

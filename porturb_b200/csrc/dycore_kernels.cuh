@@ -1422,10 +1422,11 @@ __global__ void k_add_inplace(T *__restrict__ a, const T *__restrict__ b, size_t
 
 // Enforcement pass on a state in place (the call at the top of
 // time_step_rk_3_3, dynamics_rk.h:301).
+// Cells [e0, e1) of the state (whole levels: e0, e1 multiples of NP).
 template <class R, int NTR, bool IMM>
-__global__ void k_enforce(const Grid<R> G, R *__restrict__ s) {
-  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (idx >= G.N) return;
+__global__ void k_enforce(const Grid<R> G, R *__restrict__ s, size_t e0, size_t e1) {
+  const size_t idx = e0 + size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= e1) return;
   const int k = int(idx / G.NP);
   R q[5 + NTR];
 #pragma unroll
@@ -1452,11 +1453,13 @@ struct Thermo {
   unsigned adds_mass;
 };
 
+// Cells [e0, e1) (whole levels) of the coupler arrays into the state.
 template <class R, int NTR>
 __global__ void k_load_coupler(CouplerPtrs cp, Thermo th, const double *__restrict__ rho_off,
-                               const double *__restrict__ rt_off, size_t N, size_t NP, R *__restrict__ s) {
-  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (idx >= N) return;
+                               const double *__restrict__ rt_off, size_t N, size_t NP, R *__restrict__ s, size_t e0,
+                               size_t e1) {
+  const size_t idx = e0 + size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= e1) return;
   const int k = int(idx / NP);
   const double rd = cp.rho_d[idx], u = cp.u[idx], v = cp.v[idx], w = cp.w[idx], temp = cp.T[idx];
   const double rho_v = cp.tr[th.idWV][idx];
@@ -1475,11 +1478,13 @@ __global__ void k_load_coupler(CouplerPtrs cp, Thermo th, const double *__restri
   for (int t = 0; t < NTR; t++) s[(5 + t) * N + idx] = R(cp.tr[t][idx]);
 }
 
+// Cells [e0, e1) (whole levels) of the state into the coupler arrays.
 template <class R, int NTR>
 __global__ void k_store_coupler(CouplerOut co, Thermo th, const double *__restrict__ rho_off,
-                                const double *__restrict__ rt_off, size_t N, size_t NP, const R *__restrict__ s) {
-  const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (idx >= N) return;
+                                const double *__restrict__ rt_off, size_t N, size_t NP, const R *__restrict__ s,
+                                size_t e0, size_t e1) {
+  const size_t idx = e0 + size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= e1) return;
   const int k = int(idx / NP);
   const double rho = rho_off[k] + double(s[idx]);
   const double u = double(s[1 * N + idx]) / rho, v = double(s[2 * N + idx]) / rho, w = double(s[3 * N + idx]) / rho;

@@ -110,6 +110,10 @@ struct ImplBase {
   double *sums = nullptr;
   double *diag_part = nullptr, *diag_out = nullptr;
   int diag_blocks = 0;
+  // The copy stream and chunk events of the overlapped time_step (created at
+  // its first use).
+  cudaStream_t cs = nullptr;
+  std::vector<cudaEvent_t> io_ev;
   // Event-based per-kernel timing (pu_dycore_profile).
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -494,6 +498,8 @@ struct ImplBase {
   virtual ~ImplBase() {
     dec_release();
     for (auto e : ev_pool) cudaEventDestroy(e);
+    for (auto e : io_ev) cudaEventDestroy(e);
+    if (cs) cudaStreamDestroy(cs);
     if (owns)
       for (void *q : {(void *)ml_theta, (void *)ml_m, (void *)ml_v, (void *)ml_wq, (void *)ml_grad, (void *)ml_partial,
                       (void *)ml_frags, (void *)ml_xs, (void *)ml_ts, (void *)ml_counts})
@@ -504,6 +510,14 @@ struct ImplBase {
   virtual int load_state(const pu_state_view *v) = 0;
   virtual int store_state(pu_state_view *v) = 0;
   virtual int advance(double dt, int nsteps) = 0;
+  // time_step (dynamics_rk.h:103-137) after the sub-step count: coupler
+  // arrays in, nsteps SSPRK3 steps of dt, coupler arrays out.
+  virtual int time_step(pu_state_view *v, double dt, int nsteps) {
+    int rc = load_state(v);
+    if (!rc) rc = advance(dt, nsteps);
+    if (!rc) rc = store_state(v);
+    return rc;
+  }
   virtual int get_conserved(double *st, double *tr, int mem) = 0;
   virtual int set_conserved(const double *st, const double *tr, int mem) = 0;
   virtual int set_hydrostasis(const double *r, const double *t, const double *p) = 0;
@@ -924,7 +938,7 @@ struct Impl : ImplBase {
     CouplerPtrs cp;
     PU_TRY(device_view(v, cp));
     k_load_coupler<R, NTR><<<blocks(N, 256), 256, 0, st>>>(cp, thermo(), rho_off, rt_off, N, NP,
-                                                           static_cast<R *>(s[0]));
+                                                           static_cast<R *>(s[0]), 0, N);
     PU_LAUNCHED();
     return PU_OK;
   }
@@ -945,7 +959,7 @@ struct Impl : ImplBase {
     co.rho_d = d[0]; co.u = d[1]; co.v = d[2]; co.w = d[3]; co.T = d[4];
     for (int t = 0; t < 8; t++) co.tr[t] = t < NTR ? d[5 + t] : nullptr;
     k_store_coupler<R, NTR><<<blocks(N, 256), 256, 0, st>>>(co, thermo(), rho_off, rt_off, N, NP,
-                                                            static_cast<const R *>(s[0]));
+                                                            static_cast<const R *>(s[0]), 0, N);
     PU_LAUNCHED();
     if (!on_device)
       for (int a = 0; a < 5 + NTR; a++) {
@@ -974,6 +988,89 @@ struct Impl : ImplBase {
     return std::is_same<R, float>::value && weno_mode == PU_WENO_LEARNED && ml_ready && cfg.weno_all;
   }
 
+  // The big-tile x/y kernel (no learned weights) on levels [k0, k1): the
+  // levels below imm_levels() take the immersed kernel, the others the plain
+  // one -- through TMA where the tiles allow it.  b: the index of the stage
+  // input among s[] (its tensor maps).
+  template <bool IMM, bool DEC = false>
+  int xy_levels(const Grid<R> &G, const R *sin, int b, int k0, int k1) {
+    using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM, false>;
+    using Sp = XYShape<R, NTR, XTX_BIG, XTY_BIG, false, false>;
+    R *t = static_cast<R *>(txy);
+    const int kl = IMM ? std::min(std::max(imm_levels(), k0), k1) : k0;
+    const unsigned bx = blocks(cfg.nx, XTX_BIG), by = blocks(cfg.ny, XTY_BIG);
+    if (kl > k0) {
+      Grid<R> Gi = G;
+      Gi.k_first = k0;
+      k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false, DEC><<<dim3(bx, by, kl - k0), Sh::NT, Sh::bytes, st>>>(
+          Gi, sin, t, xy_maps[b]);
+      PU_LAUNCHED();
+    }
+    if (kl < k1) {
+      Grid<R> Gp = G;
+      Gp.k_first = kl;
+      const dim3 g(bx, by, k1 - kl);
+      bool staged = false;
+      if constexpr (!DEC && Sp::TMA_FITS) {
+        if (xy_tma && static_cast<const void *>(sin) == s[b]) {
+          k_xy<R, NTR, XTX_BIG, XTY_BIG, false, false, false, true><<<g, Sp::NT, Sp::tma_bytes, st>>>(Gp, sin, t,
+                                                                                                    xy_maps[b]);
+          staged = true;
+        }
+      }
+      if (!staged)
+        k_xy<R, NTR, XTX_BIG, XTY_BIG, false, false, DEC><<<g, Sp::NT, Sp::bytes, st>>>(Gp, sin, t, xy_maps[b]);
+      PU_LAUNCHED();
+    }
+    return PU_OK;
+  }
+
+  // The tiled z kernel (FP32, z_tiled) on z chunks [c0, c1) of ZT_Z levels:
+  // chunks below ci take the immersed kernel.  Chunk c reads levels
+  // 32c-5 .. 32c+36, so it is plain once 32c-5 reaches the first level no
+  // flag holds; a periodic z wraps flagged levels into the top chunk, so every
+  // chunk stays immersed there.  The maps of this stage input (s[b]); the
+  // cell maps of sn and txy are the same for every b.
+  template <bool IMM>
+  int zt_chunks(const Grid<R> &G, const R *sin, const R *sn, R *sout, R a_n, R a_dt, int n_enforce, int b, int c0,
+                int c1) {
+    if constexpr (std::is_same<R, float>::value) {
+      using Zs = ZTShape<NTR, ZT_X, ZT_Z, IMM>;
+      using Zp = ZTShape<NTR, ZT_X, ZT_Z, false>;
+      R *t = static_cast<R *>(txy);
+      const int nch = int(blocks(cfg.nz, ZT_Z));
+      const int ci0 = !IMM ? 0 : (cfg.bc_z == PU_BC_WALL ? std::min(nch, (imm_levels() + 5 + ZT_Z - 1) / ZT_Z) : nch);
+      const int ci = std::min(std::max(ci0, c0), c1);
+      const bool tma = zt_tma && static_cast<const void *>(sin) == s[b];
+      const unsigned bx = blocks(cfg.nx, ZT_X), by = unsigned(cfg.ny);
+      if (ci > c0) {
+        Grid<R> Gi = G;
+        Gi.c_first = c0;
+        const dim3 gt(bx, by, ci - c0);
+        if (tma)
+          k_zt<NTR, ZT_X, ZT_Z, IMM, true><<<gt, ZT_X * ZT_Z, Zs::tma_bytes, st>>>(Gi, sin, sn, sout, t, a_n, a_dt,
+                                                                                 n_enforce, zt_maps[b]);
+        else
+          k_zt<NTR, ZT_X, ZT_Z, IMM><<<gt, ZT_X * ZT_Z, Zs::bytes, st>>>(Gi, sin, sn, sout, t, a_n, a_dt, n_enforce,
+                                                                          zt_maps[b]);
+        PU_LAUNCHED();
+      }
+      if (ci < c1) {
+        Grid<R> Gp = G;
+        Gp.c_first = ci;
+        const dim3 gt(bx, by, c1 - ci);
+        if (tma)
+          k_zt<NTR, ZT_X, ZT_Z, false, true><<<gt, ZT_X * ZT_Z, Zp::tma_bytes, st>>>(Gp, sin, sn, sout, t, a_n, a_dt,
+                                                                                    n_enforce, zt_maps[b]);
+        else
+          k_zt<NTR, ZT_X, ZT_Z, false><<<gt, ZT_X * ZT_Z, Zp::bytes, st>>>(Gp, sin, sn, sout, t, a_n, a_dt,
+                                                                            n_enforce, zt_maps[b]);
+        PU_LAUNCHED();
+      }
+    }
+    return PU_OK;
+  }
+
   // One SSPRK3 stage: the x/y kernel (DEC: a decomposed tile reading its
   // received halo slabs), then the z march with the stage combination.
   template <bool IMM, bool LRN, bool DEC = false>
@@ -987,39 +1084,15 @@ struct Impl : ImplBase {
       using Sh = XYShape<R, NTR, XTX_SM, XTY_SM, IMM, L>;
       dim3 g(blocks(cfg.nx, XTX_SM), blocks(cfg.ny, XTY_SM), cfg.nz);
       k_xy<R, NTR, XTX_SM, XTY_SM, IMM, L, DEC><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b]);
+      PU_LAUNCHED();
     } else if (L) {
       using Sh = XYShape<R, NTR, LTX, LTY, IMM, L>;
       dim3 g(blocks(cfg.nx, LTX), blocks(cfg.ny, LTY), cfg.nz);
       k_xy<R, NTR, LTX, LTY, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b]);
+      PU_LAUNCHED();
     } else {
-      // Levels [0, kl) take the immersed kernel, [kl, nz) the plain one --
-      // through TMA where the tiles allow it.
-      using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM, false>;
-      using Sp = XYShape<R, NTR, XTX_BIG, XTY_BIG, false, false>;
-      const int kl = IMM ? imm_levels() : 0;
-      const unsigned bx = blocks(cfg.nx, XTX_BIG), by = blocks(cfg.ny, XTY_BIG);
-      if (kl > 0) {
-        k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false, DEC><<<dim3(bx, by, kl), Sh::NT, Sh::bytes, st>>>(G, sin, t,
-                                                                                                   xy_maps[b]);
-        if (kl < cfg.nz) PU_LAUNCHED();
-      }
-      if (kl < cfg.nz) {
-        Grid<R> Gp = G;
-        Gp.k_first = kl;
-        const dim3 g(bx, by, cfg.nz - kl);
-        bool staged = false;
-        if constexpr (!DEC && Sp::TMA_FITS) {
-          if (xy_tma && static_cast<const void *>(sin) == s[b]) {
-            k_xy<R, NTR, XTX_BIG, XTY_BIG, false, false, false, true><<<g, Sp::NT, Sp::tma_bytes, st>>>(Gp, sin, t,
-                                                                                                      xy_maps[b]);
-            staged = true;
-          }
-        }
-        if (!staged)
-          k_xy<R, NTR, XTX_BIG, XTY_BIG, false, false, DEC><<<g, Sp::NT, Sp::bytes, st>>>(Gp, sin, t, xy_maps[b]);
-      }
+      PU_TRY((xy_levels<IMM, DEC>(G, sin, b, 0, cfg.nz)));
     }
-    PU_LAUNCHED();
     prof_end(0, e0);
     const int kc = cfg.z_chunk > 0 ? cfg.z_chunk : (cfg.nz < 16 ? cfg.nz : 16);
     dim3 gz(blocks(cfg.nx, ZTX), blocks(cfg.ny, ZTY), blocks(cfg.nz, kc));
@@ -1031,34 +1104,7 @@ struct Impl : ImplBase {
         // no flag holds.  A periodic z wraps flagged levels into the top
         // chunk: every chunk stays immersed there.  The maps of this stage
         // input (s[b]); the cell maps of sn and txy are the same for every b.
-        using Zs = ZTShape<NTR, ZT_X, ZT_Z, IMM>;
-        using Zp = ZTShape<NTR, ZT_X, ZT_Z, false>;
-        const int nch = int(blocks(cfg.nz, ZT_Z));
-        const int ci = !IMM ? 0 : (cfg.bc_z == PU_BC_WALL ? std::min(nch, (imm_levels() + 5 + ZT_Z - 1) / ZT_Z) : nch);
-        const bool tma = zt_tma && static_cast<const void *>(sin) == s[b];
-        const unsigned bx = blocks(cfg.nx, ZT_X), by = unsigned(cfg.ny);
-        if (ci > 0) {
-          const dim3 gt(bx, by, ci);
-          if (tma)
-            k_zt<NTR, ZT_X, ZT_Z, IMM, true><<<gt, ZT_X * ZT_Z, Zs::tma_bytes, st>>>(G, sin, sn, sout, t, a_n, a_dt,
-                                                                                   n_enforce, zt_maps[b]);
-          else
-            k_zt<NTR, ZT_X, ZT_Z, IMM><<<gt, ZT_X * ZT_Z, Zs::bytes, st>>>(G, sin, sn, sout, t, a_n, a_dt,
-                                                                            n_enforce, zt_maps[b]);
-          if (ci < nch) PU_LAUNCHED();
-        }
-        if (ci < nch) {
-          Grid<R> Gp = G;
-          Gp.c_first = ci;
-          const dim3 gt(bx, by, nch - ci);
-          if (tma)
-            k_zt<NTR, ZT_X, ZT_Z, false, true><<<gt, ZT_X * ZT_Z, Zp::tma_bytes, st>>>(Gp, sin, sn, sout, t, a_n,
-                                                                                      a_dt, n_enforce, zt_maps[b]);
-          else
-            k_zt<NTR, ZT_X, ZT_Z, false><<<gt, ZT_X * ZT_Z, Zp::bytes, st>>>(Gp, sin, sn, sout, t, a_n, a_dt,
-                                                                              n_enforce, zt_maps[b]);
-        }
-        PU_LAUNCHED();
+        PU_TRY((zt_chunks<IMM>(G, sin, sn, sout, a_n, a_dt, n_enforce, b, 0, int(blocks(cfg.nz, ZT_Z)))));
         prof_end(1, e1);
         return PU_OK;
       }
@@ -1080,7 +1126,7 @@ struct Impl : ImplBase {
     const Grid<R> G = grid();
     R *s0 = static_cast<R *>(s[0]), *s1 = static_cast<R *>(s[1]), *s2 = static_cast<R *>(s[2]);
     cudaEvent_t e0 = prof_begin();
-    k_enforce<R, NTR, IMM><<<blocks(N, 256), 256, 0, st>>>(G, s0);
+    k_enforce<R, NTR, IMM><<<blocks(N, 256), 256, 0, st>>>(G, s0, 0, N);
     PU_LAUNCHED();
     prof_end(2, e0);
     for (int n = 0; n < nsteps; n++) {
@@ -1111,6 +1157,129 @@ struct Impl : ImplBase {
     }
     if (learned_active()) return has_imm ? advance_t<true, true>(dt, nsteps) : advance_t<false, true>(dt, nsteps);
     return has_imm ? advance_t<true, false>(dt, nsteps) : advance_t<false, false>(dt, nsteps);
+  }
+
+  // ---- time_step with the host copies overlapped ----
+  // On host coupler arrays the copies in and out move 2 x 8 S N bytes over the
+  // host link, as long as several steps on large grids.  Here the call runs
+  // as a wavefront over chunks of ZT_Z levels: the input crosses chunk by
+  // chunk on a copy stream, and stage g (1 .. 3 nsteps; 0 = the chunk's
+  // conversion and enforcement) runs on chunk c once stage g-1 has run on
+  // chunks c-1, c and c+1 (the z stencils reach 5 levels into each
+  // neighbour).  On the one compute stream the launches go in diagonals
+  // w = g + c, each in increasing g: everything in diagonal w waits only for
+  // input chunk w, so the stages of the chunks already there run while the
+  // rest crosses; each chunk's final state is converted back and copied out
+  // while the others finish.  Every write lands after the reads of the old
+  // values it replaces: stage g writes the buffer stage g-3 wrote, whose
+  // readers (stage g-2 on c-1..c+1, and for s0 stages g-2 and g-1 on c) sit in
+  // earlier diagonals or earlier in this one; the x/y tendency of chunk c is
+  // written and read by the two kernels of one (g, c), in stream order.
+  // Every cell gets the kernels and inputs of load_state + advance +
+  // store_state, so the results are the same bits.  FP32 with the tiled z
+  // kernel, walls in z (a periodic z couples the top and bottom chunks), at
+  // least two chunks; the config's serial_io turns it off.
+  bool io_overlap(const pu_state_view *v) const {
+    if constexpr (!std::is_same<R, float>::value) {
+      return false;
+    } else {
+      return !cfg.serial_io && !dc.on && !profiling && !small_tile && z_tiled(false) && !learned_active() &&
+             cfg.bc_z == PU_BC_WALL && cfg.nz >= 2 * ZT_Z && v->rho_d &&
+             resolve_mem(v->mem, v->rho_d) == PU_MEM_HOST;
+    }
+  }
+
+  int time_step(pu_state_view *v, double dt, int nsteps) override {
+    if (nsteps <= 0 || !io_overlap(v)) return ImplBase::time_step(v, dt, nsteps);
+    double *host[5 + NTR] = {v->rho_d, v->uvel, v->vvel, v->wvel, v->temp};
+    for (int t = 0; t < NTR; t++) host[5 + t] = v->tracers[t];
+    for (int a = 0; a < 5 + NTR; a++)
+      if (!host[a]) {
+        set_error("coupler view has a null array");
+        return PU_ERR_INVALID;
+      }
+    if (!cs) PU_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    const int nch = int(blocks(cfg.nz, ZT_Z));
+    while (io_ev.size() < size_t(2 * nch + 1)) {
+      cudaEvent_t e;
+      PU_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      io_ev.push_back(e);
+    }
+    const int rc = has_imm ? time_step_io<true>(host, dt, nsteps, nch) : time_step_io<false>(host, dt, nsteps, nch);
+    // No copy into or out of the caller's arrays outlives the call.
+    const cudaError_t e = cudaStreamSynchronize(cs);
+    if (rc) return rc;
+    if (e != cudaSuccess) {
+      set_error(std::string("copy stream: ") + cudaGetErrorString(e));
+      return PU_ERR_CUDA;
+    }
+    return check_err();
+  }
+
+  template <bool IMM>
+  int time_step_io(double *const *host, double dt, int nsteps, int nch) {
+    const Grid<R> G = grid();
+    R *sb[3] = {static_cast<R *>(s[0]), static_cast<R *>(s[1]), static_cast<R *>(s[2])};
+    CouplerPtrs cp;
+    CouplerOut co;
+    cp.rho_d = co.rho_d = staging;
+    cp.u = co.u = staging + N;
+    cp.v = co.v = staging + 2 * N;
+    cp.w = co.w = staging + 3 * N;
+    cp.T = co.T = staging + 4 * N;
+    for (int t = 0; t < 8; t++) cp.tr[t] = co.tr[t] = t < NTR ? staging + size_t(5 + t) * N : nullptr;
+    cudaEvent_t *ein = io_ev.data(), *eout = ein + nch, start = ein[2 * nch];
+    auto lev = [&](int c) { return std::min(cfg.nz, c * ZT_Z); };
+    const int last = 3 * nsteps;
+    // The copy stream starts after the work queued so far (the staging
+    // buffer is free then).
+    PU_CK(cudaEventRecord(start, st));
+    PU_CK(cudaStreamWaitEvent(cs, start, 0));
+    // Stage g on chunk c: g = 0 brings the chunk in; g = 3n+1, 3n+2, 3n+3 are
+    // the stages of step n as advance_t runs them (Shu-Osher SSPRK(3,3),
+    // dynamics_rk.h:308-360); the last one also converts the chunk back.
+    auto run = [&](int g, int c) -> int {
+      const size_t e0 = size_t(lev(c)) * NP, e1 = size_t(lev(c + 1)) * NP;
+      const unsigned nb = blocks(e1 - e0, 256);
+      if (g == 0) {
+        for (int a = 0; a < 5 + NTR; a++)
+          PU_CK(cudaMemcpyAsync(staging + size_t(a) * N + e0, host[a] + e0, (e1 - e0) * sizeof(double),
+                                cudaMemcpyHostToDevice, cs));
+        PU_CK(cudaEventRecord(ein[c], cs));
+        PU_CK(cudaStreamWaitEvent(st, ein[c], 0));
+        k_load_coupler<R, NTR><<<nb, 256, 0, st>>>(cp, thermo(), rho_off, rt_off, N, NP, sb[0], e0, e1);
+        PU_LAUNCHED();
+        k_enforce<R, NTR, IMM><<<nb, 256, 0, st>>>(G, sb[0], e0, e1);
+        PU_LAUNCHED();
+        return PU_OK;
+      }
+      const int m = (g - 1) % 3;   // 0: s1 = s0 + dt L(s0); 1: s2 from s1; 2: s0 from s2
+      const R a_n = m == 0 ? R(0) : (m == 1 ? R(3. / 4.) : R(1. / 3.));
+      const R a_dt = m == 0 ? R(dt) : (m == 1 ? R(1. / 4. * dt) : R(2. / 3. * dt));
+      const int n_enforce = (m == 2 && g != last) ? 2 : 1;
+      PU_TRY((xy_levels<IMM>(G, sb[m], m, lev(c), lev(c + 1))));
+      PU_TRY((zt_chunks<IMM>(G, sb[m], m == 0 ? nullptr : sb[0], sb[(m + 1) % 3], a_n, a_dt, n_enforce, m, c,
+                             c + 1)));
+      if (g == last) {
+        k_store_coupler<R, NTR><<<nb, 256, 0, st>>>(co, thermo(), rho_off, rt_off, N, NP, sb[0], e0, e1);
+        PU_LAUNCHED();
+        PU_CK(cudaEventRecord(eout[c], st));
+      }
+      return PU_OK;
+    };
+    for (int w = 0; w <= last + nch - 1; w++)
+      for (int g = std::max(0, w - (nch - 1)); g <= std::min(w, last); g++) PU_TRY(run(g, w - g));
+    // The output copies, queued after all the compute so that a pageable
+    // destination (whose copies hold the host thread) does not hold back the
+    // launches.
+    for (int c = 0; c < nch; c++) {
+      const size_t e0 = size_t(lev(c)) * NP, e1 = size_t(lev(c + 1)) * NP;
+      PU_CK(cudaStreamWaitEvent(cs, eout[c], 0));
+      for (int a = 0; a < 5 + NTR; a++)
+        PU_CK(cudaMemcpyAsync(host[a] + e0, staging + size_t(a) * N + e0, (e1 - e0) * sizeof(double),
+                              cudaMemcpyDeviceToHost, cs));
+    }
+    return PU_OK;
   }
 
   // ---- decomposed tiles ----
@@ -1156,8 +1325,8 @@ struct Impl : ImplBase {
   int dec_enforce() override {
     const Grid<R> G = grid();
     R *s0 = static_cast<R *>(s[0]);
-    if (has_imm) k_enforce<R, NTR, true><<<blocks(N, 256), 256, 0, st>>>(G, s0);
-    else k_enforce<R, NTR, false><<<blocks(N, 256), 256, 0, st>>>(G, s0);
+    if (has_imm) k_enforce<R, NTR, true><<<blocks(N, 256), 256, 0, st>>>(G, s0, 0, N);
+    else k_enforce<R, NTR, false><<<blocks(N, 256), 256, 0, st>>>(G, s0, 0, N);
     PU_LAUNCHED();
     return PU_OK;
   }

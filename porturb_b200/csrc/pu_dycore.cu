@@ -141,6 +141,7 @@ int check_config(const pu_config *c) {
   if (c->z_chunk < 0) return fail(PU_ERR_INVALID, "z_chunk must be >= 0");
   if (c->thread_loads != 0 && c->thread_loads != 1) return fail(PU_ERR_INVALID, "thread_loads must be 0 or 1");
   if (c->imm_all_levels != 0 && c->imm_all_levels != 1) return fail(PU_ERR_INVALID, "imm_all_levels must be 0 or 1");
+  if (c->serial_io != 0 && c->serial_io != 1) return fail(PU_ERR_INVALID, "serial_io must be 0 or 1");
   return PU_OK;
 }
 }  // namespace pu
@@ -639,9 +640,7 @@ int pu_dycore_time_step(pu_dycore *h, pu_state_view *coupler, double dt_phys, in
   pu_dycore_compute_time_step(h, &dt_dyn);
   const int n = (int)std::ceil(dt_phys / dt_dyn);
   dt_dyn = dt_phys / n;
-  int rc = h->impl->load_state(coupler);
-  if (!rc) rc = h->impl->advance(dt_dyn, n);
-  if (!rc) rc = h->impl->store_state(coupler);
+  const int rc = h->impl->time_step(coupler, dt_dyn, n);
   if (ncycles) *ncycles = n;
   return rc;
 }

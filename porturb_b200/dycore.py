@@ -68,7 +68,7 @@ class Dycore:
     """One pu_dycore handle."""
 
     def __init__(self, nx, ny, nz, dx, dy, dz, tracers, options, precision="f32", device=0, stream=None,
-                 z_chunk=0, weno_mode="plain", thread_loads=False, imm_all_levels=False):
+                 z_chunk=0, weno_mode="plain", thread_loads=False, imm_all_levels=False, serial_io=False):
         self.lib = capi.load()
         cfg = capi.pu_config()
         cfg.nx, cfg.ny, cfg.nz = nx, ny, nz
@@ -98,6 +98,7 @@ class Dycore:
         cfg.z_chunk = z_chunk
         cfg.thread_loads = int(bool(thread_loads))
         cfg.imm_all_levels = int(bool(imm_all_levels))
+        cfg.serial_io = int(bool(serial_io))
         self.cfg = cfg
         self.ntr = len(tracers)
         self.shape = (nz, ny, nx)

@@ -67,6 +67,35 @@ def test_nonfinite_input_is_reported_then_cleared(field, value, where, precision
     g2.close()
 
 
+@pytest.mark.parametrize("k", [5, 70])
+def test_nonfinite_input_overlapped_time_step(k):
+    """The same on a grid whose time_step on host arrays overlaps the copies
+    with the steps (nz = 96: three 32-level chunks; the NaN in the first or
+    the last chunk): the call returns PU_ERR_NONFINITE after its copies
+    finished, and the next clean call gives a fresh handle's bits."""
+    case = cases.abl_neutral(nx=32, ny=32, nz=96)
+    g = _handle(case)
+    dt_phys = 2.5 * g.compute_time_step()
+    st, tr = _arrays(case)
+    l0 = g.kernel_launches()
+    st[2][k, 7, 9] = np.nan
+    with pytest.raises(PortUrbError) as e:
+        g.time_step(*st, tr, dt_phys)
+    assert e.value.status == capi.PU_ERR_NONFINITE
+    # The chunked launches (63 here against 21 for the serial form): the
+    # overlapped path ran.
+    assert g.kernel_launches() - l0 > 40
+    st, tr = _arrays(case)
+    assert g.time_step(*st, tr, dt_phys) == 3
+    g2 = _handle(case)
+    st2, tr2 = _arrays(case)
+    g2.time_step(*st2, tr2, dt_phys)
+    for a, b in zip(st + tr, st2 + tr2):
+        assert np.array_equal(a, b)
+    g.close()
+    g2.close()
+
+
 def test_nonfinite_state_through_advance_is_reported_by_synchronize():
     case = cases.small_mixed(immersed=False)
     g = _handle(case)

@@ -44,10 +44,13 @@ def _write_input(path, case, ncalls, dt_phys):
 
 
 @pytest.mark.gpu
-def test_dropin_matches_python_front_end(tmp_path):
+@pytest.mark.parametrize("grid", ["small", "abl_32x32x64"])
+def test_dropin_matches_python_front_end(tmp_path, grid):
+    """abl_32x32x64: two 32-level chunks, so time_step on the drop-in's host
+    arrays takes the overlapped form (and the Python front end's too)."""
     from porturb_b200 import Dycore, cases
     exe = build_driver()
-    case = cases.small_mixed(immersed=False)
+    case = cases.small_mixed(immersed=False) if grid == "small" else cases.abl_neutral(nx=32, ny=32, nz=64)
     g = Dycore.from_case(case, precision="f32")
     dt_phys = 2.5 * g.compute_time_step()
     _write_input(tmp_path / "in.bin", case, 2, dt_phys)

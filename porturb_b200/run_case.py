@@ -93,7 +93,9 @@ def _driver_run(case, a, precision, calls, dt=None, warm=1):
     averager), the perturbed state, then `warm` untimed and `calls` timed
     calls of dt_phys = 10 dycore steps (or `dt`).  Per call:
       abl      -- geostrophic forcing, dycore, sponge, surface fluxes, LES
-                  closure, time averager (abl_neutral.cpp:93-108);
+                  closure, time averager (abl_neutral.cpp:93-108), the sponge
+                  over the top 300 m of the domain (the boundary layer's
+                  damping layer; the reference driver's top_prop is 0.1);
       city     -- edge sponge, dycore, sponge, surface fluxes, LES closure,
                   time averager (city.cpp:137-142);
       periodic -- the mean wind at 100 m relaxed to (10, 0) m/s on a time
@@ -137,7 +139,8 @@ def _driver_run(case, a, precision, calls, dt=None, warm=1):
             les.apply(c, dt)
             apply_surface_fluxes(c, dt)
         else:
-            sponge_layer(c, dt, dt if chain == "city" else dt * 100, 0.02 if chain == "city" else 0.1)
+            sponge_layer(c, dt, dt if chain == "city" else dt * 100,
+                         0.02 if chain == "city" else min(1.0, 300.0 / case.zlen))
             apply_surface_fluxes(c, dt)
             les.apply(c, dt)
         tavg.accumulate(c, dt)

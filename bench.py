@@ -159,10 +159,28 @@ def cpu_info():
     return {"cpu_model": model, "logical_cpus": os.cpu_count()}
 
 
-def cpu_reference_rate(steps=3, warmup=1):
+def cpu_f64_rate(case, steps=2, warmup=1):
+    """Cell-steps/s of the FP64 oracle (the same algorithm with FP64
+    arithmetic throughout) on the host cores, on the same window."""
+    import pyoracle
+    d = pyoracle.Dycore(case, "f64")
+    d.init_case()
+    d.load_coupler(list(case.coupler_arrays(perturbed=True)))
+    dt = d.compute_time_step()
+    for _ in range(warmup):
+        d.advance(dt, 1)
+    t0 = time.perf_counter()
+    d.advance(dt, steps)
+    el = time.perf_counter() - t0
+    return {"value": case.ncells * steps / el, "unit": "cell-steps/s", "ms_per_step": el * 1e3 / steps, "kind": "port",
+            "sample": "%d step(s) after %d warm-up step(s), the same window" % (steps, warmup)}
+
+
+def cpu_reference_rate(steps=3, warmup=1, f64=False):
     """Cell-steps/s of the reference's own dycore code on the host cores
     (oracle/_ref; this project's REF restatement if the reference library was
-    not built), on a window of the benchmark domain."""
+    not built), on a window of the benchmark domain; with f64, also the FP64
+    oracle's rate there."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     kind = "reference" if pyoracle.have_ref() else "ref"
@@ -189,6 +207,8 @@ def cpu_reference_rate(steps=3, warmup=1):
                         el, init_s),
            "threads": threads, "ms_per_step": el * 1e3 / steps}
     out.update(cpu_info())
+    if f64:
+        out["f64_oracle"] = cpu_f64_rate(case)
     return out
 
 
@@ -561,7 +581,7 @@ def main():
         cpu = None
         if not args.no_cpu_baseline:
             try:
-                cpu = cpu_reference_rate(steps=3, warmup=1)
+                cpu = cpu_reference_rate(steps=3, warmup=1, f64=True)
             except Exception as e:  # the baseline is a report, not the product
                 cpu = {"error": str(e)}
         line = {

@@ -334,6 +334,16 @@ int pu_weno9_edges_f32(const float *stencils, const unsigned char *flags, long l
  * the range. */
 int pu_learned_normalize_f32(const float *stencils, long long n, float *x, float *jump);
 
+/* The bounded wait of the stage kernels' TMA staging, made to run out (a
+ * failure-detection check; no reference counterpart): one block waits on an
+ * mbarrier whose announced copies are never issued, for at most limit_us
+ * microseconds (0: the stage kernels' own limit, 20 ms; at most 1 s), and
+ * gives up.  *completed = 1 if the wait saw the copies complete (it cannot;
+ * the stage kernels report such a give-up as PU_ERR_CUDA), *ms the kernel's
+ * time, *cycles thread 0's clock cycles in the wait (ms and cycles may be
+ * NULL).  The context stays usable.  Synchronous, on the current device. */
+int pu_check_bounded_wait(int limit_us, int *completed, double *ms, long long *cycles);
+
 /* ---------------------------------------------------------------------------
  * Domain decomposition across GPUs (coupler.h:132-229): a handle can be one
  * (px, py) tile of an nproc_x x nproc_y grid of tiles over an nx_glob x

@@ -160,6 +160,7 @@ SIGNATURES = {
                                          C.POINTER(_I)]),
     "pu_weno9_edges_f32": (_I, [_P, _P, C.c_longlong, _I, _P, _P, _I]),
     "pu_learned_normalize_f32": (_I, [_P, C.c_longlong, _P, _P]),
+    "pu_check_bounded_wait": (_I, [_I, _P, _P, _P]),
     "pu_decomp_process_grid": (_I, [_I, C.c_longlong, C.c_longlong, C.POINTER(_I), C.POINTER(_I)]),
     "pu_decomp_tile": (_I, [C.c_longlong, _I, _I, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "pu_decomp_neighbors": (_I, [C.POINTER(pu_decomp), C.POINTER(_I)]),

@@ -364,6 +364,29 @@ __global__ void k_normalize9_eval(const float *__restrict__ s, long long n, floa
   jump[i] = j;
 }
 
+// A bounded wait that runs out: thread 0 announces 16 bytes of copies on an
+// mbarrier of the block and issues none, so the barrier's phase never
+// completes; every thread waits on it with the wait of the stage kernels' TMA
+// staging (pu::tma::mbar_wait) for at most limit_ns and gives up.  out[0] = 1
+// if any thread saw the phase complete (none can), out[1] = the clock cycles
+// thread 0 waited.
+__global__ void k_wait_check(unsigned long long limit_ns, long long *out) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    pu::tma::mbar_init(&bar);
+    pu::tma::mbar_expect(&bar, 16u);
+  }
+  __syncthreads();
+  const long long t0 = clock64();
+  const bool ok = pu::tma::mbar_wait(&bar, 0, limit_ns);
+  const long long t1 = clock64();
+  const int any = __syncthreads_or(ok);
+  if (threadIdx.x == 0) {
+    out[0] = any;
+    out[1] = t1 - t0;
+  }
+}
+
 // The FP32 limiter on a batch of stencils: VARIANT 0 the scalar form, 1 the
 // packed form (stencils 2i and 2i+1 in one thread), 4 the packed one-edge
 // form (the right edge of stencil 2i and the left edge of stencil 2i+1; the
@@ -1035,6 +1058,33 @@ int pu_learned_normalize_f32(const float *stencils, long long n, float *x, float
   cudaFree(dx);
   cudaFree(dj);
   if (e != cudaSuccess) return fail(PU_ERR_CUDA, cudaGetErrorString(e));
+  return PU_OK;
+}
+
+int pu_check_bounded_wait(int limit_us, int *completed, double *ms, long long *cycles) {
+  if (limit_us < 0 || limit_us > 1000000 || !completed) return fail(PU_ERR_INVALID, "bad argument");
+  const unsigned long long limit_ns = limit_us ? 1000ull * limit_us : pu::tma::WAIT_LIMIT_NS;
+  long long *d = nullptr, h[2] = {0, 0};
+  if (cudaMalloc(&d, sizeof(h)) != cudaSuccess) return fail(PU_ERR_NOMEM, "cudaMalloc");
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  if (e == cudaSuccess) e = cudaEventRecord(e0);
+  if (e == cudaSuccess) {
+    k_wait_check<<<1, 128>>>(limit_ns, d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(e1);
+  if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  float t = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(PU_ERR_CUDA, cudaGetErrorString(e));
+  *completed = int(h[0]);
+  if (ms) *ms = t;
+  if (cycles) *cycles = h[1];
   return PU_OK;
 }
 

@@ -82,10 +82,14 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Bounded wait for phase `parity` of the barrier; false if it did not come.
-// Polls with test_wait (no suspension of the waiting threads).
+// Bounded wait for phase `parity` of the barrier: at most 20 ms by the GPU's
+// nanosecond timer (and at most 2^26 polls, in case the timer stood still);
+// false if it did not come.  Polls with test_wait (no suspension of the
+// waiting threads).
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (int it = 0; it < (1 << 24); it++) {
+  uint64_t t0, t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (int it = 0; it < (1 << 26); it++) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
@@ -93,6 +97,8 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
         : "r"(mbar), "r"(parity)
         : "memory");
     if (ok) return true;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 > 20000000ull) return false;
   }
   return false;
 }

@@ -89,11 +89,25 @@ __device__ __forceinline__ void load_4d(void *dst, const CUtensorMap *map, int x
       : "memory");
 }
 
-// Waits for phase `parity` of bar, at most `limit` polls; false if it did
-// not complete (the caller reports the error and gives up the tile).
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int limit = 1 << 22) {
+// The GPU's nanosecond timer.
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// How long a wait on a tile copy may take before the block gives up: a copy
+// lands in microseconds even under full load; a poll of try_wait that does
+// not see it suspends the thread for ~4 us (measured on B200).
+constexpr uint64_t WAIT_LIMIT_NS = 20000000ull;   // 20 ms
+
+// Waits for phase `parity` of bar for at most limit_ns; false if it did not
+// complete (the caller reports the error and gives up the tile).  The poll
+// count is capped too (2^20 polls, ~4 s), in case the timer stood still.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns = WAIT_LIMIT_NS) {
   const uint32_t a = saddr(bar);
-  for (int it = 0; it < limit; it++) {
+  const uint64_t t0 = globaltimer_ns();
+  for (int it = 0; it < (1 << 20); it++) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
@@ -101,6 +115,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int li
         : "r"(a), "r"(parity)
         : "memory");
     if (ok) return true;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
   }
   return false;
 }

@@ -8,7 +8,8 @@ the flag is clear.  The failure is made on the host: a NaN or an Inf written
 into one cell of the coupler arrays the caller passes in (host or device
 memory).  Bad arguments and calls out of order return PU_ERR_INVALID /
 PU_ERR_STATE before any GPU work, where the reference aborts
-(Options.h:122-148, dynamics_rk.h:799).
+(Options.h:122-148, dynamics_rk.h:799).  The stage kernels' bounded wait is
+made to run out on a barrier that nothing completes, and reports it.
 """
 import ctypes as C
 
@@ -149,6 +150,39 @@ def test_bad_arguments_and_calls_out_of_order():
     # The handle still works after all of the above.
     assert g.time_step(*st, tr, 2.5 * g.compute_time_step()) == 3
     g.close()
+
+
+def test_bounded_wait_runs_out_and_the_context_stays_usable(gpu_lib):
+    """The wait of the stage kernels' TMA staging (pu::tma::mbar_wait) made to
+    run out on an mbarrier whose announced copies are never issued
+    (pu_check_bounded_wait): it gives up after its time limit (2 ms here, then
+    the stage kernels' own 20 ms) and reports that it did, the kernel returns
+    within a few ms of the limit, and the context keeps working (a dycore
+    step afterwards matches a fresh handle's)."""
+    lib = capi.load()
+    done = C.c_int(-1)
+    assert lib.pu_check_bounded_wait(100, C.byref(done), None, None) == capi.PU_OK   # loads the kernel
+    assert done.value == 0
+    for limit_us, limit_ms in ((2000, 2.0), (0, 20.0)):
+        done, ms, cyc = C.c_int(-1), C.c_double(), C.c_longlong()
+        assert lib.pu_check_bounded_wait(limit_us, C.byref(done), C.byref(ms), C.byref(cyc)) == capi.PU_OK
+        print("bounded wait with a %.0f ms limit: gave up after %.3f ms (%d cycles)" % (limit_ms, ms.value, cyc.value))
+        assert done.value == 0
+        assert limit_ms <= ms.value < limit_ms + 10.0
+    done = C.c_int(-1)
+    assert lib.pu_check_bounded_wait(-1, C.byref(done), None, None) == capi.PU_ERR_INVALID
+    case = cases.small_mixed()
+    dt_phys = None
+    outs = []
+    for _ in range(2):
+        g = _handle(case)
+        dt_phys = dt_phys or 2.5 * g.compute_time_step()
+        st, tr = _arrays(case)
+        assert g.time_step(*st, tr, dt_phys) == 3
+        outs.append(st + tr)
+        g.close()
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
 
 
 def test_normalize9_matches_oracle(gpu_lib):

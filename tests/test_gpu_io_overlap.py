@@ -10,7 +10,8 @@ finish.  Cases: a plain boundary layer (3 chunks), the urban canopy whose
 immersed levels end inside the second chunk (the immersed/plain split falls
 inside a chunk's range), a last chunk of 16 levels (nz = 80), three tracers
 with immersed cells; each with 1, 2 and 3 SSPRK3 cycles per call, from
-pageable numpy arrays and from pinned torch tensors.  The overlapped call
+pageable numpy arrays and from pinned torch tensors; and the urban canopy at
+its configuration's size (512x512x128).  The overlapped call
 must launch more kernels than the serial one (the chunked stages: the path
 was taken), and a periodic z or nz < 64 must launch the same number (the
 path is not taken).  The launch order itself is checked on the CPU against
@@ -69,6 +70,19 @@ def test_overlapped_time_step_same_bits(name, factor, pinned, gpu_lib):
     assert l0 > l1, (l0, l1)
     for q, (a, b) in enumerate(zip(out0, out1)):
         assert np.array_equal(a, b), (name, q, np.abs(a - b).max())
+    assert np.array_equal(st0, st1) and np.array_equal(tr0, tr1)
+
+
+def test_overlapped_time_step_same_bits_at_config_size(gpu_lib):
+    """The urban canopy at the size of its configuration (512x512x128, 2 m:
+    33.5 M cells, 4 chunks, the immersed levels ending inside chunk 1), 3
+    cycles per call from pinned arrays: the same bits both ways."""
+    case = cases.urban_canopy(nx=512, ny=512, nz=128, dx=2.0)
+    n1, l1, out1, st1, tr1 = _call(case, True, 2.5, True)
+    n0, l0, out0, st0, tr0 = _call(case, False, 2.5, True)
+    assert n0 == n1 == 3 and l0 > l1
+    for q, (a, b) in enumerate(zip(out0, out1)):
+        assert np.array_equal(a, b), (q, np.abs(a - b).max())
     assert np.array_equal(st0, st1) and np.array_equal(tr0, tr1)
 
 

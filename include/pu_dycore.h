@@ -88,11 +88,13 @@ typedef struct pu_config {
                                               immersed flag reaches; 1: on every level (the same
                                               results) */
   int serial_io;                           /* 0: pu_dycore_time_step on host arrays overlaps the
-                                              copies in with the first stage and the copies out
-                                              with the last, chunk by chunk, where the path allows
-                                              it (FP32, weno_all, plain weights, walls in z,
-                                              nz >= 64); 1: copies in, steps, copies out (the
-                                              same results) */
+                                              copies with the steps, chunk by chunk, where the
+                                              path allows it (FP32, weno_all, plain weights, walls
+                                              in z, nz >= 64), and a decomposed tile with a
+                                              transport runs its interior x/y tiles while its
+                                              halos cross; 1: copies in, steps, copies out, and
+                                              every x/y tile after the exchange (the same
+                                              results) */
 } pu_config;
 
 /* The coupler-side state: density_dry, uvel, vvel, wvel, temp and the tracer

@@ -113,8 +113,10 @@ struct Grid {
   int gx0, gx1, gy0, gy1;
   // First level of a k_xy launch (blockIdx.z counts from it) and first z
   // chunk of a k_zt launch: a stage can run the immersed kernels on the
-  // levels that need them and the plain ones above.
-  int k_first, c_first;
+  // levels that need them and the plain ones above.  First column and row of
+  // a k_xy launch (blockIdx.x, .y count tiles from them): a decomposed tile
+  // can run its interior tiles while its halos cross, its edge tiles after.
+  int k_first, c_first, i_first, j_first;
   // Learned WENO weights (kernels instantiated with LEARNED only).
   const uint32_t *ml_frags;     // per-lane operand fragments of the network
   unsigned long long *ml_counts;  // [0] stencils given learned weights, [1] limiter fallbacks
@@ -517,7 +519,8 @@ __global__ void __launch_bounds__(TX *TY, LEARNED ? PU_LEARNED_XY_MIN_BLOCKS : (
   uint16_t *queue = reinterpret_cast<uint16_t *>(FL);
 
   const int tid = threadIdx.x;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, k = G.k_first + int(blockIdx.z);
+  const int i0 = G.i_first + int(blockIdx.x) * TX, j0 = G.j_first + int(blockIdx.y) * TY,
+            k = G.k_first + int(blockIdx.z);
   const int nx = G.nx, ny = G.ny;
   const size_t plane = size_t(k) * G.NP;
   const bool sim2d = G.sim2d != 0;

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -38,6 +39,12 @@ void set_error(const std::string &msg);
       return PU_ERR_CUDA;                                                                 \
     }                                                                                     \
     launches++;                                                                           \
+  } while (0)
+
+#define PU_TRY(x)                 \
+  do {                            \
+    int rc_ = (x);                \
+    if (rc_ != PU_OK) return rc_; \
   } while (0)
 
 // ---------------------------------------------------------------------------
@@ -111,9 +118,14 @@ struct ImplBase {
   double *diag_part = nullptr, *diag_out = nullptr;
   int diag_blocks = 0;
   // The copy stream and chunk events of the overlapped time_step (created at
-  // its first use).
+  // its first use); a decomposed tile's NCCL exchange runs on the same stream
+  // when it overlaps the interior tiles (dec_ev orders it).
   cudaStream_t cs = nullptr;
   std::vector<cudaEvent_t> io_ev;
+  cudaEvent_t dec_ev[2] = {nullptr, nullptr};
+  // A decomposed stage whose interior tiles already ran: the x/y kernel takes
+  // the edge tiles only.
+  bool dec_edges_only = false;
   // Event-based per-kernel timing (pu_dycore_profile).
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -404,7 +416,8 @@ struct ImplBase {
   // two ranks in the order they are posted, so with one or two tiles across a
   // direction (both neighbours the same rank) every rank's first message to
   // the other is its snd[lo], which the other takes into rcv[hi].
-  int nccl_exchange(HaloSet &h, bool x, bool y) {
+  int nccl_exchange(HaloSet &h, bool x, bool y, cudaStream_t on = nullptr) {
+    if (!on) on = st;
     auto &api = nccl();
     if (!api.ok || !dc.comm) {
       set_error("NCCL halo exchange without a communicator");
@@ -419,10 +432,10 @@ struct ImplBase {
     for (int a = 0; a < 2; a++) {
       if ((a == 0 && !x) || (a == 1 && !y)) continue;
       const int lo = 2 * a, hi = lo + 1;
-      note(api.Send(h.snd[lo], h.bytes[lo], ncclUint8, dc.nbr[lo], dc.comm, st));
-      note(api.Recv(h.rcv[hi], h.bytes[hi], ncclUint8, dc.nbr[hi], dc.comm, st));
-      note(api.Send(h.snd[hi], h.bytes[hi], ncclUint8, dc.nbr[hi], dc.comm, st));
-      note(api.Recv(h.rcv[lo], h.bytes[lo], ncclUint8, dc.nbr[lo], dc.comm, st));
+      note(api.Send(h.snd[lo], h.bytes[lo], ncclUint8, dc.nbr[lo], dc.comm, on));
+      note(api.Recv(h.rcv[hi], h.bytes[hi], ncclUint8, dc.nbr[hi], dc.comm, on));
+      note(api.Send(h.snd[hi], h.bytes[hi], ncclUint8, dc.nbr[hi], dc.comm, on));
+      note(api.Recv(h.rcv[lo], h.bytes[lo], ncclUint8, dc.nbr[lo], dc.comm, on));
     }
     r = api.GroupEnd();
     if (first != ncclSuccess) return nccl_fail(first, "ncclSend/ncclRecv");
@@ -431,7 +444,7 @@ struct ImplBase {
   }
   // The exchange through the caller's host transport: the active slabs to
   // pinned host memory, the transport's exchange, the received slabs back.
-  int host_exchange(HaloSet &h, bool x, bool y) {
+  int host_exchange(HaloSet &h, bool x, bool y, const std::function<int()> &interior = nullptr) {
     void *s[4] = {nullptr, nullptr, nullptr, nullptr}, *r[4] = {nullptr, nullptr, nullptr, nullptr};
     size_t b[4] = {0, 0, 0, 0};
     for (int d = 0; d < 4; d++) {
@@ -443,7 +456,15 @@ struct ImplBase {
       r[d] = h.hrcv[d];
       b[d] = h.bytes[d];
     }
-    PU_CK(cudaStreamSynchronize(st));
+    if (interior) {
+      // The interior tiles compute while the host moves the slabs.
+      PU_TRY(dec_events());
+      PU_CK(cudaEventRecord(dec_ev[0], st));
+      PU_TRY(interior());
+      PU_CK(cudaEventSynchronize(dec_ev[0]));
+    } else {
+      PU_CK(cudaStreamSynchronize(st));
+    }
     const int q = dc.ht.exchange(dc.ht.user, s, r, b, dc.nbr);
     if (q != 0) {
       set_error("host transport: exchange returned " + std::to_string(q));
@@ -453,10 +474,29 @@ struct ImplBase {
       if (b[d]) PU_CK(cudaMemcpyAsync(h.rcv[d], h.hrcv[d], b[d], cudaMemcpyHostToDevice, st));
     return PU_OK;
   }
-  // The halo exchange of one HaloSet through this tile's transport.
-  int exchange(HaloSet &h, bool x, bool y) {
-    if (dc.comm) return nccl_exchange(h, x, y);
-    if (dc.host) return host_exchange(h, x, y);
+  int dec_events() {
+    for (auto &e : dec_ev)
+      if (!e) PU_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return PU_OK;
+  }
+  // The halo exchange of one HaloSet through this tile's transport.  With
+  // `interior`, the work that needs no halo is launched while the slabs
+  // cross: NCCL runs on the side stream between two events, the host
+  // transport's callback runs while the device computes.
+  int exchange(HaloSet &h, bool x, bool y, const std::function<int()> &interior = nullptr) {
+    if (dc.comm) {
+      if (!interior) return nccl_exchange(h, x, y);
+      if (!cs) PU_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+      PU_TRY(dec_events());
+      PU_CK(cudaEventRecord(dec_ev[0], st));
+      PU_CK(cudaStreamWaitEvent(cs, dec_ev[0], 0));
+      PU_TRY(nccl_exchange(h, x, y, cs));
+      PU_CK(cudaEventRecord(dec_ev[1], cs));
+      PU_TRY(interior());
+      PU_CK(cudaStreamWaitEvent(st, dec_ev[1], 0));
+      return PU_OK;
+    }
+    if (dc.host) return host_exchange(h, x, y, interior);
     set_error("halo exchange without a transport");
     return PU_ERR_STATE;
   }
@@ -499,6 +539,8 @@ struct ImplBase {
     dec_release();
     for (auto e : ev_pool) cudaEventDestroy(e);
     for (auto e : io_ev) cudaEventDestroy(e);
+    for (auto e : dec_ev)
+      if (e) cudaEventDestroy(e);
     if (cs) cudaStreamDestroy(cs);
     if (owns)
       for (void *q : {(void *)ml_theta, (void *)ml_m, (void *)ml_v, (void *)ml_wq, (void *)ml_grad, (void *)ml_partial,
@@ -621,11 +663,7 @@ struct Impl : ImplBase {
     p = static_cast<T *>(q);
     return PU_OK;
   }
-#define PU_TRY(x)                 \
-  do {                            \
-    int rc_ = (x);                \
-    if (rc_ != PU_OK) return rc_; \
-  } while (0)
+
 
   int alloc() override {
     F = 6 + NTR;
@@ -789,6 +827,8 @@ struct Impl : ImplBase {
     G.err = err;
     G.k_first = 0;
     G.c_first = 0;
+    G.i_first = 0;
+    G.j_first = 0;
     G.ml_frags = ml_frags;
     G.ml_counts = ml_counts;
     G.ml_jump = ml_jump;
@@ -992,22 +1032,30 @@ struct Impl : ImplBase {
   // levels below imm_levels() take the immersed kernel, the others the plain
   // one -- through TMA where the tiles allow it.  b: the index of the stage
   // input among s[] (its tensor maps).
+  // Tiles [tx0, tx1) x [ty0, ty1) (all by default).
   template <bool IMM, bool DEC = false>
-  int xy_levels(const Grid<R> &G, const R *sin, int b, int k0, int k1) {
+  int xy_levels(const Grid<R> &G, const R *sin, int b, int k0, int k1, int tx0 = 0, int tx1 = -1, int ty0 = 0,
+                int ty1 = -1) {
     using Sh = XYShape<R, NTR, XTX_BIG, XTY_BIG, IMM, false>;
     using Sp = XYShape<R, NTR, XTX_BIG, XTY_BIG, false, false>;
     R *t = static_cast<R *>(txy);
+    if (tx1 < 0) tx1 = int(blocks(cfg.nx, XTX_BIG));
+    if (ty1 < 0) ty1 = int(blocks(cfg.ny, XTY_BIG));
+    if (tx1 <= tx0 || ty1 <= ty0 || k1 <= k0) return PU_OK;
     const int kl = IMM ? std::min(std::max(imm_levels(), k0), k1) : k0;
-    const unsigned bx = blocks(cfg.nx, XTX_BIG), by = blocks(cfg.ny, XTY_BIG);
+    const unsigned bx = unsigned(tx1 - tx0), by = unsigned(ty1 - ty0);
+    Grid<R> Gt = G;
+    Gt.i_first = tx0 * XTX_BIG;
+    Gt.j_first = ty0 * XTY_BIG;
     if (kl > k0) {
-      Grid<R> Gi = G;
+      Grid<R> Gi = Gt;
       Gi.k_first = k0;
       k_xy<R, NTR, XTX_BIG, XTY_BIG, IMM, false, DEC><<<dim3(bx, by, kl - k0), Sh::NT, Sh::bytes, st>>>(
           Gi, sin, t, xy_maps[b]);
       PU_LAUNCHED();
     }
     if (kl < k1) {
-      Grid<R> Gp = G;
+      Grid<R> Gp = Gt;
       Gp.k_first = kl;
       const dim3 g(bx, by, k1 - kl);
       bool staged = false;
@@ -1090,6 +1138,15 @@ struct Impl : ImplBase {
       dim3 g(blocks(cfg.nx, LTX), blocks(cfg.ny, LTY), cfg.nz);
       k_xy<R, NTR, LTX, LTY, IMM, L><<<g, Sh::NT, Sh::bytes, st>>>(G, sin, t, xy_maps[b]);
       PU_LAUNCHED();
+    } else if (DEC && dec_edges_only) {
+      // The tiles around the interior ones, which ran while the halos crossed.
+      int tx0, tx1, ty0, ty1;
+      dec_interior(tx0, tx1, ty0, ty1);
+      const int nbx = int(blocks(cfg.nx, XTX_BIG)), nby = int(blocks(cfg.ny, XTY_BIG));
+      PU_TRY((xy_levels<IMM, DEC>(G, sin, b, 0, cfg.nz, 0, nbx, 0, ty0)));
+      PU_TRY((xy_levels<IMM, DEC>(G, sin, b, 0, cfg.nz, 0, nbx, ty1, nby)));
+      PU_TRY((xy_levels<IMM, DEC>(G, sin, b, 0, cfg.nz, 0, tx0, ty0, ty1)));
+      PU_TRY((xy_levels<IMM, DEC>(G, sin, b, 0, cfg.nz, tx1, nbx, ty0, ty1)));
     } else {
       PU_TRY((xy_levels<IMM, DEC>(G, sin, b, 0, cfg.nz)));
     }
@@ -1147,11 +1204,20 @@ struct Impl : ImplBase {
         return PU_ERR_STATE;
       }
       PU_TRY(dec_enforce());
+      const bool split = dec_split();
       for (int n = 0; n < nsteps; n++)
         for (int sg = 0; sg < 3; sg++) {
           PU_TRY(dec_pack(sg));
-          PU_TRY(exchange(dc.state, true, !sim2d()));
-          PU_TRY(dec_compute(sg, dt, n == nsteps - 1));
+          if (!split) {
+            PU_TRY(exchange(dc.state, true, !sim2d()));
+            PU_TRY(dec_compute(sg, dt, n == nsteps - 1));
+            continue;
+          }
+          PU_TRY(exchange(dc.state, true, !sim2d(), [&] { return dec_xy_interior(sg); }));
+          dec_edges_only = true;
+          const int rc = dec_compute(sg, dt, n == nsteps - 1);
+          dec_edges_only = false;
+          PU_TRY(rc);
         }
       return PU_OK;
     }
@@ -1338,6 +1404,35 @@ struct Impl : ImplBase {
     if (sg == 0) return stage<IMM, false, true>(G, s0, nullptr, s1, R(0), R(dt), 1);
     if (sg == 1) return stage<IMM, false, true>(G, s1, s0, s2, R(3. / 4.), R(1. / 4. * dt), 1);
     return stage<IMM, false, true>(G, s2, s0, s0, R(1. / 3.), R(2. / 3. * dt), last ? 1 : 2);
+  }
+  // The tiles of a decomposed tile's x/y kernel whose cross (the 16x16 tile
+  // and 5 cells around it) stays inside the tile and so reads no halo slab:
+  // [tx0, tx1) x [ty0, ty1), empty when the tile is too small.
+  void dec_interior(int &tx0, int &tx1, int &ty0, int &ty1) const {
+    tx0 = 1;
+    ty0 = 1;
+    tx1 = std::max(tx0, (cfg.nx - XTX_BIG - 5) / XTX_BIG + 1);
+    ty1 = std::max(ty0, (cfg.ny - XTY_BIG - 5) / XTY_BIG + 1);
+    if (cfg.nx < XTX_BIG + 5) tx1 = tx0;
+    if (cfg.ny < XTY_BIG + 5) ty1 = ty0;
+  }
+  // Interior tiles run while the halos cross (a transport, the 16x16 x/y
+  // tiles, some interior; the config's serial_io turns it off).
+  bool dec_split() const {
+    if (!dc.on || cfg.serial_io || small_tile || sim2d() || !has_transport()) return false;
+    int tx0, tx1, ty0, ty1;
+    dec_interior(tx0, tx1, ty0, ty1);
+    return tx1 > tx0 && ty1 > ty0;
+  }
+  // The x/y kernel of stage sg on the interior tiles (the stage input is
+  // s[sg]: s0, s1, s2 for the three stages).
+  int dec_xy_interior(int sg) {
+    const Grid<R> G = grid();
+    const R *sin = static_cast<const R *>(s[sg]);
+    int tx0, tx1, ty0, ty1;
+    dec_interior(tx0, tx1, ty0, ty1);
+    return has_imm ? xy_levels<true, true>(G, sin, sg, 0, cfg.nz, tx0, tx1, ty0, ty1)
+                   : xy_levels<false, true>(G, sin, sg, 0, cfg.nz, tx0, tx1, ty0, ty1);
   }
   int dec_compute(int sg, double dt, bool last) override {
     const Grid<R> G = grid();

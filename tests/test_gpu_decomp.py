@@ -132,27 +132,36 @@ import sys
 sys.path[:0] = [%r]
 import numpy as np
 from porturb_b200 import Dycore, cases, decomp
-case = cases.small_mixed(nx=40, ny=32, nz=16, immersed=True)
-g = Dycore.from_case(case)
-dt = g.compute_time_step()
-rd, u, v, w, T, trc = [np.ascontiguousarray(a) for a in case.coupler_arrays(perturbed=False)]
-prop = np.ascontiguousarray(case.immersed_proportion)
-g.init(rd, u, v, w, T, list(trc), prop)
-cells, _ = g.get_hydrostasis()
-h = Dycore.from_case(case)
-t = decomp.tiles(case.nx, case.ny, 1, 1)[0]
-decomp.set_decomposition(h, t, case.nx, case.ny, nccl_id=decomp.nccl_unique_id())
-h.init(rd, u, v, w, T, list(trc), prop)
-c2, _ = h.get_hydrostasis()
-assert all(np.allclose(c2[q], cells[q], rtol=1.2e-7, atol=0) for q in range(3))
-h.set_hydrostasis(*cells)
-for d in (g, h):
-    rd, u, v, w, T, trc = [np.ascontiguousarray(a) for a in case.coupler_arrays(perturbed=True)]
-    d.load_state(rd, u, v, w, T, list(trc))
-    d.advance(dt, 3)
-a, b = g.get_conserved(), h.get_conserved()
-assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
-print("nccl one-rank decomposition ok")
+launches = {}
+for nx, ny, serial in ((40, 32, False), (64, 64, False), (64, 64, True)):
+    case = cases.small_mixed(nx=nx, ny=ny, nz=16, immersed=True)
+    g = Dycore.from_case(case)
+    dt = g.compute_time_step()
+    rd, u, v, w, T, trc = [np.ascontiguousarray(a) for a in case.coupler_arrays(perturbed=False)]
+    prop = np.ascontiguousarray(case.immersed_proportion)
+    g.init(rd, u, v, w, T, list(trc), prop)
+    cells, _ = g.get_hydrostasis()
+    h = Dycore.from_case(case, serial_io=serial)
+    t = decomp.tiles(case.nx, case.ny, 1, 1)[0]
+    decomp.set_decomposition(h, t, case.nx, case.ny, nccl_id=decomp.nccl_unique_id())
+    h.init(rd, u, v, w, T, list(trc), prop)
+    c2, _ = h.get_hydrostasis()
+    assert all(np.allclose(c2[q], cells[q], rtol=1.2e-7, atol=0) for q in range(3))
+    h.set_hydrostasis(*cells)
+    for d in (g, h):
+        rd, u, v, w, T, trc = [np.ascontiguousarray(a) for a in case.coupler_arrays(perturbed=True)]
+        d.load_state(rd, u, v, w, T, list(trc))
+        l0 = d.kernel_launches()
+        d.advance(dt, 3)
+        launches[(nx, serial, d is h)] = d.kernel_launches() - l0
+    a, b = g.get_conserved(), h.get_conserved()
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), (nx, ny, serial)
+    g.close()
+    h.close()
+# 64x64: the interior tiles ran while the halos crossed (more launches than
+# the whole-tile form); 40x32 has no interior tile.
+assert launches[(64, False, True)] > launches[(64, True, True)], launches
+print("nccl one-rank decomposition ok", launches)
 """
 
 

@@ -32,6 +32,9 @@ pytestmark = [pytest.mark.gpu, pytest.mark.timeout(600)]
 CASES = {
     "x_split": lambda: cases.small_mixed(nx=40, ny=24, nz=16),
     "y_split": lambda: cases.small_mixed(nx=24, ny=40, nz=16),
+    # tiles of 64x64 and 64x56: interior 16x16 tiles run while the halos cross
+    "x_split_interior": lambda: cases.small_mixed(nx=128, ny=64, nz=16),
+    "y_split_interior": lambda: cases.small_mixed(nx=64, ny=112, nz=16),
 }
 NSTEPS = 3
 
@@ -104,7 +107,7 @@ def test_two_ranks_over_host_transport_equal_undecomposed(name, precision, tmp_p
     mp.start_processes(_rank, args=(world, _free_port(), name, precision, str(tmp_path)), nprocs=world, join=True,
                        start_method="spawn")
     npx, npy = decomp.process_grid(world, case.nx, case.ny)
-    assert (npx, npy) == ((2, 1) if name == "x_split" else (1, 2))
+    assert (npx, npy) == ((2, 1) if name.startswith("x_split") else (1, 2))
     ts = decomp.tiles(case.nx, case.ny, npx, npy)
     res = [np.load(tmp_path / ("rank%d.npz" % r)) for r in range(world)]
     # The tiles' own profiles: sums over the two ranks against the whole grid's.

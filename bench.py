@@ -18,13 +18,15 @@ the same steps from the same state.  One JSON line on rank 0.
 * e2e: the reference-facing call (pu_dycore_time_step, dt_phys = 10 dycore
   steps as the reference's drivers use, abl_neutral.cpp:25) with the coupler
   arrays in pinned host memory: host->device copy, conversion, 10 SSPRK3
-  steps, conversion back and device->host copy inside every timed call.
+  steps, conversion back and device->host copy inside every timed call (the
+  library overlaps the copies with the steps chunk by chunk).
 * roofline: the x/y flux kernel (the larger share of the step), its
   algorithmic bytes per launch over its CUDA-event duration; traffic from the
   committed ncu capture (profiles/traffic.json).
 * cpu_baseline / --impl reference: the reference's own dycore code
   (oracle/_ref, built from the reference's headers with a single-rank shim)
-  on all host cores, on a 64x64x256 window of the same domain.
+  on all host cores, on a 64x64x256 window of the same domain; beside it the
+  FP64 oracle's rate on that window.
 * learned: the learned-weight form on the same initial state, after
   harvesting 2^24 stencils from the plain run and training the network on the
   GPU (Adam, batch 65536); kernel times and the fallback fraction.

@@ -13,6 +13,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/pu_dycore.h"
 #include "dycore_kernels.cuh"
 #include "learned.cuh"
@@ -40,6 +42,14 @@ void set_error(const std::string &msg);
     }                                                                                     \
     launches++;                                                                           \
   } while (0)
+
+// A named range for profilers (NVTX; a no-op unless a tool is attached).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 #define PU_TRY(x)                 \
   do {                            \
@@ -484,6 +494,7 @@ struct ImplBase {
   // cross: NCCL runs on the side stream between two events, the host
   // transport's callback runs while the device computes.
   int exchange(HaloSet &h, bool x, bool y, const std::function<int()> &interior = nullptr) {
+    NvtxRange range("pu:halo_exchange");
     if (dc.comm) {
       if (!interior) return nccl_exchange(h, x, y);
       if (!cs) PU_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
@@ -975,6 +986,7 @@ struct Impl : ImplBase {
   }
 
   int load_state(const pu_state_view *v) override {
+    NvtxRange range("pu:load_state");
     CouplerPtrs cp;
     PU_TRY(device_view(v, cp));
     k_load_coupler<R, NTR><<<blocks(N, 256), 256, 0, st>>>(cp, thermo(), rho_off, rt_off, N, NP,
@@ -984,6 +996,7 @@ struct Impl : ImplBase {
   }
 
   int store_state(pu_state_view *v) override {
+    NvtxRange range("pu:store_state");
     CouplerOut co;
     double *d[5 + NTR];
     double *dst[5] = {v->rho_d, v->uvel, v->vvel, v->wvel, v->temp};
@@ -1180,6 +1193,7 @@ struct Impl : ImplBase {
 
   template <bool IMM, bool LRN>
   int advance_t(double dt, int nsteps) {
+    NvtxRange range("pu:advance");
     const Grid<R> G = grid();
     R *s0 = static_cast<R *>(s[0]), *s1 = static_cast<R *>(s[1]), *s2 = static_cast<R *>(s[2]);
     cudaEvent_t e0 = prof_begin();
@@ -1284,6 +1298,7 @@ struct Impl : ImplBase {
 
   template <bool IMM>
   int time_step_io(double *const *host, double dt, int nsteps, int nch) {
+    NvtxRange range("pu:time_step_overlapped");
     const Grid<R> G = grid();
     R *sb[3] = {static_cast<R *>(s[0]), static_cast<R *>(s[1]), static_cast<R *>(s[2])};
     CouplerPtrs cp;

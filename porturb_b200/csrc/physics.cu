@@ -23,6 +23,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/pu_physics.h"
 
 namespace pu {
@@ -568,6 +570,14 @@ struct Dev {
   }
 };
 
+// A named range for profilers (NVTX; a no-op unless a tool is attached).
+struct PhRange {
+  explicit PhRange(const char *name) { nvtxRangePushA(name); }
+  ~PhRange() { nvtxRangePop(); }
+  PhRange(const PhRange &) = delete;
+  PhRange &operator=(const PhRange &) = delete;
+};
+
 // The guard of a call; returns PU_ERR_CUDA from it when the device cannot be
 // made current.
 #define PH_DEVICE(dev)  \
@@ -799,6 +809,7 @@ int pu_les_apply(pu_physics *h, pu_state_view *v, double dt) {
   if (h->cfg.idTKE < 0) return fail(PU_ERR_INVALID, "the LES closure needs the TKE tracer (les_closure.h:24-25)");
   if (!(dt > 0)) return fail(PU_ERR_INVALID, "dt must be positive");
   PH_DEVICE(h->cfg.device);
+  PhRange range(__func__);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -833,6 +844,7 @@ int pu_les_apply_to(pu_physics *h, const pu_state_view *in, pu_state_view *out, 
   if (h->cfg.idTKE < 0) return fail(PU_ERR_INVALID, "the LES closure needs the TKE tracer (les_closure.h:24-25)");
   if (!(dt > 0)) return fail(PU_ERR_INVALID, "dt must be positive");
   PH_DEVICE(h->cfg.device);
+  PhRange range(__func__);
   if (!in->rho_d || !out->uvel) return fail(PU_ERR_INVALID, "state view has a null array");
   if (!on_device(in->mem, in->rho_d) || !on_device(out->mem, out->uvel))
     return fail(PU_ERR_INVALID, "pu_les_apply_to takes device arrays");
@@ -855,6 +867,7 @@ int pu_sponge_layer(pu_physics *h, pu_state_view *v, double dt, double time_scal
   if (!h || !v) return fail(PU_ERR_INVALID, "null argument");
   if (!(time_scale > 0) || !(top_prop > 0 && top_prop <= 1)) return fail(PU_ERR_INVALID, "bad sponge parameters");
   PH_DEVICE(h->cfg.device);
+  PhRange range(__func__);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -880,6 +893,7 @@ int pu_sponge_layer(pu_physics *h, pu_state_view *v, double dt, double time_scal
 int pu_geostrophic_forcing(pu_physics *h, pu_state_view *v, double dt, double lat_g, double u_g, double v_g) {
   if (!h || !v) return fail(PU_ERR_INVALID, "null argument");
   PH_DEVICE(h->cfg.device);
+  PhRange range(__func__);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -900,6 +914,7 @@ int pu_geostrophic_forcing(pu_physics *h, pu_state_view *v, double dt, double la
 int pu_surface_fluxes(pu_physics *h, pu_state_view *v, double dt) {
   if (!h || !v) return fail(PU_ERR_INVALID, "null argument");
   PH_DEVICE(h->cfg.device);
+  PhRange range(__func__);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -920,6 +935,7 @@ int pu_uniform_pg_wind_forcing(pu_physics *h, pu_state_view *v, double dt, doubl
   if (!h || !v || !state) return fail(PU_ERR_INVALID, "null argument");
   if (update_cycles == 0 || !(tau > 0)) return fail(PU_ERR_INVALID, "bad uniform_pg_wind_forcing parameters");
   PH_DEVICE(h->cfg.device);
+  PhRange range(__func__);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -973,6 +989,7 @@ int pu_uniform_pg_wind_forcing_height(pu_physics *h, pu_state_view *v, double dt
   if (k1 < 0) return fail(PU_ERR_INVALID, "uniform_pg_wind_forcing_height: height below the first level centre");
   if (k1 + 1 >= nz) return fail(PU_ERR_INVALID, "uniform_pg_wind_forcing_height needs nz >= 2");
   PH_DEVICE(h->cfg.device);
+  PhRange range(__func__);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -1000,6 +1017,7 @@ int pu_time_averager_accumulate(pu_physics *h, const pu_state_view *v, pu_time_a
   for (double *p : host)
     if (!p) return fail(PU_ERR_INVALID, "null time-average array");
   PH_DEVICE(h->cfg.device);
+  PhRange range(__func__);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);
@@ -1068,6 +1086,7 @@ int pu_edge_sponge_apply(pu_physics *h, pu_state_view *v, const int *fields, int
   if (nx_glob < h->cfg.nx || ny_glob < h->cfg.ny || i_beg < 0 || j_beg < 0)
     return fail(PU_ERR_INVALID, "edge sponge: bad tile placement");
   PH_DEVICE(h->cfg.device);
+  PhRange range(__func__);
   double *d[5 + PU_MAX_TRACERS];
   bool staged;
   int rc = device_arrays(*h, v, d, staged);

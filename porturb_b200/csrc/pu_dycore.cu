@@ -18,7 +18,14 @@ namespace pu {
 namespace {
 thread_local std::string g_error;
 }
-void set_error(const std::string &msg) { g_error = msg; }
+// Records the message of a failed call and clears the runtime's last error,
+// so that a failure the caller recovers from (an allocation that did not fit,
+// say) is not reported again by the next launch check.  A sticky error stays
+// with the context whatever is cleared here.
+void set_error(const std::string &msg) {
+  g_error = msg;
+  cudaGetLastError();
+}
 
 NcclApi &nccl() {
   static NcclApi api;
@@ -663,6 +670,7 @@ int pu_dycore_time_step(pu_dycore *h, pu_state_view *coupler, double dt_phys, in
   pu_dycore_compute_time_step(h, &dt_dyn);
   const int n = (int)std::ceil(dt_phys / dt_dyn);
   dt_dyn = dt_phys / n;
+  pu::NvtxRange range("pu_dycore_time_step");
   const int rc = h->impl->time_step(coupler, dt_dyn, n);
   if (ncycles) *ncycles = n;
   return rc;

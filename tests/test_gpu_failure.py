@@ -9,7 +9,9 @@ into one cell of the coupler arrays the caller passes in (host or device
 memory).  Bad arguments and calls out of order return PU_ERR_INVALID /
 PU_ERR_STATE before any GPU work, where the reference aborts
 (Options.h:122-148, dynamics_rk.h:799).  The stage kernels' bounded wait is
-made to run out on a barrier that nothing completes, and reports it.
+made to run out on a barrier that nothing completes, and reports it; a
+device allocation that cannot succeed returns PU_ERR_NOMEM and leaves
+nothing allocated.
 """
 import ctypes as C
 
@@ -183,6 +185,34 @@ def test_bounded_wait_runs_out_and_the_context_stays_usable(gpu_lib):
         g.close()
     for a, b in zip(*outs):
         assert np.array_equal(a, b)
+
+
+def test_allocation_failure_is_reported_and_released(gpu_lib):
+    """A grid larger than the device (2048^3 cells: ~600 GB of state
+    buffers) makes pu_dycore_create return PU_ERR_NOMEM; nothing of it stays
+    allocated (the free device memory is what it was), and handles created
+    afterwards work."""
+    import torch
+    case = cases.small_mixed()
+    g = _handle(case)          # the library's kernels loaded, the context warm
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(0)[0]
+    with pytest.raises(PortUrbError) as e:
+        Dycore(2048, 2048, 2048, 1.0, 1.0, 1.0, case.tracers, case.options, precision="f32", device=0)
+    assert e.value.status == capi.PU_ERR_NOMEM
+    assert b"cudaMalloc" in capi.load().pu_last_error()
+    free1 = torch.cuda.mem_get_info(0)[0]
+    assert abs(free1 - free0) <= 8 << 20, (free0, free1)
+    dt_phys = 2.5 * g.compute_time_step()
+    st, tr = _arrays(case)
+    assert g.time_step(*st, tr, dt_phys) == 3
+    g.close()
+    g2 = _handle(case)
+    st2, tr2 = _arrays(case)
+    assert g2.time_step(*st2, tr2, dt_phys) == 3
+    for a, b in zip(st + tr, st2 + tr2):
+        assert np.array_equal(a, b)
+    g2.close()
 
 
 def test_normalize9_matches_oracle(gpu_lib):
